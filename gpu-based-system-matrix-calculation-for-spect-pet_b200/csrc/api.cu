@@ -1,0 +1,371 @@
+// Host side of libsysmat: parameter decoding, device tables, the native handle API and the
+// reference-compatible entry points.
+//
+// The reference host wrappers (PESysMatGen.cu:1368-1437, scatter.cu:2013-2378) allocate,
+// copy, launch and free on every call.  Here a context holds the uploaded geometry and its
+// derived tables; the reference-compatible entry points keep one cached context per device
+// keyed by the parameter contents, so a rotation loop re-uses the tables and the output
+// buffer.  No function calls exit(); every failure is an error code.
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/sysmat.h"
+#include "geom.cuh"
+#include "pe.cuh"
+#include "scatter.cuh"
+
+using namespace sysmat;
+
+#define CUDA_TRY(expr)                                                                     \
+    do {                                                                                   \
+        cudaError_t _e = (expr);                                                           \
+        if (_e != cudaSuccess) {                                                           \
+            std::fprintf(stderr, "sysmat: %s failed: %s (%s:%d)\n", #expr,                 \
+                         cudaGetErrorString(_e), __FILE__, __LINE__);                      \
+            return SYSMAT_ERR_CUDA;                                                        \
+        }                                                                                  \
+    } while (0)
+
+struct sysmat_ctx {
+    int device = -1;
+    int num_sms = 0;
+    DevGeom g{};
+    int n_holes0_host = 0;
+    // raw parameter arrays on the device (bitmap kernels read them like the reference)
+    float* d_col = nullptr;
+    float* d_det = nullptr;
+    float* d_img = nullptr;
+    float* d_phys = nullptr;
+    std::vector<float> h_phys;
+    std::vector<float> h_img;
+    // derived tables
+    float4* d_tables = nullptr;
+    // launch bookkeeping
+    unsigned long long* d_counter = nullptr;
+    int* d_status = nullptr;
+    // scatter pair tables (built lazily from bitmaps)
+    ScatterScratch scratch{};
+};
+
+namespace {
+
+int floor_count(float v, float bias) { return (int)std::floor(v + bias); }
+
+bool finite_all(const float* p, size_t n)
+{
+    for (size_t i = 0; i < n; ++i)
+        if (!std::isfinite(p[i])) return false;
+    return true;
+}
+
+// Decode counts and sizes exactly as the reference kernels do and check the documented
+// capacities (PESysMatGen.cu:964-1013; the 80000-float tables hold at most 6666 crystals
+// and 8877 holes; layer headers 1..9 sit below the hole table at index 100).
+int decode(const float* pC, const float* pD, const float* pI, DevGeom& g, int& n_holes0)
+{
+    if (!pD || !pI) return SYSMAT_ERR_ARG;
+    std::memset(&g, 0, sizeof(g));
+    g.n_det = floor_count(pD[0], 0.000001f);
+    if (g.n_det < 1 || g.n_det > (kNDetector - 1) / 12) return SYSMAT_ERR_CAPACITY;
+    if (!finite_all(pD, 1 + 12 * (size_t)g.n_det)) return SYSMAT_ERR_ARG;
+    g.nx = (int)std::floor(pI[0]);
+    g.ny = (int)std::floor(pI[1]);
+    g.nz = (int)std::floor(pI[2]);
+    if (g.nx < 1 || g.ny < 1 || g.nz < 1) return SYSMAT_ERR_ARG;
+    g.nvox = (long long)g.nx * g.ny * g.nz;
+    if (!finite_all(pI, 12) || !std::isfinite(pI[20])) return SYSMAT_ERR_ARG;
+    g.wx = pI[3]; g.wy = pI[4]; g.wz = pI[5];
+    g.shx = pI[8]; g.shy = pI[9]; g.shz = pI[10];
+    g.fov = pI[11];
+    g.angle_step = pI[7];
+    g.nonneg_mu = 1;
+    for (int d = 0; d < g.n_det; ++d)
+        for (int k = 7; k <= 9; ++k)
+            if (!(pD[12 * d + k] >= 0.0f)) g.nonneg_mu = 0;
+    n_holes0 = 0;
+    if (pC) {
+        g.n_layers = floor_count(pC[0], 0.000001f);
+        if (g.n_layers < 0 || g.n_layers > kMaxLayers) return SYSMAT_ERR_CAPACITY;
+        int h = 0;
+        for (int m = 0; m < g.n_layers; ++m) {
+            const float* L = pC + (m + 1) * 10;
+            if (!finite_all(L, 8)) return SYSMAT_ERR_ARG;
+            const int nh = (int)std::floor(L[0]);
+            if (nh < 0) return SYSMAT_ERR_ARG;
+            LayerInfo& Ly = g.layer[m];
+            // plate box exactly as PESysMatGen.cu:1242-1249 forms it
+            Ly.x1 = -L[1] / 2.0f;
+            Ly.x2 = L[1] / 2.0f;
+            Ly.y1 = -L[2] / 2.0f + g.fov + L[4];
+            Ly.y2 = L[2] / 2.0f + g.fov + L[4];
+            Ly.z1 = -L[3] / 2.0f;
+            Ly.z2 = L[3] / 2.0f;
+            Ly.thickness = L[2];
+            Ly.mu_total = L[5];
+            if (!(L[5] >= 0.0f)) g.nonneg_mu = 0;
+            Ly.hole_begin = h;
+            Ly.hole_count = nh;
+            h += nh;
+            if (h > (kNCollimator - 100) / 9) return SYSMAT_ERR_CAPACITY;
+        }
+        g.n_holes = h;
+        if (!finite_all(pC + 100, 9 * (size_t)h)) return SYSMAT_ERR_ARG;
+        for (int i = 0; i < h; ++i)
+            if (!(pC[100 + 9 * i + 5] >= 0.0f)) g.nonneg_mu = 0;
+        n_holes0 = floor_count(pC[10], 0.000001f);
+        if (n_holes0 < 0 || n_holes0 > h) n_holes0 = g.n_layers > 0 ? g.layer[0].hole_count : 0;
+        g.n_holes0 = n_holes0;
+    }
+    return SYSMAT_OK;
+}
+
+bool same_device(const sysmat_ctx* ctx)
+{
+    int cur = -1;
+    if (cudaGetDevice(&cur) != cudaSuccess) return false;
+    return cur == ctx->device;
+}
+
+}  // namespace
+
+extern "C" SYSMAT_API const char* sysmat_error_string(int code)
+{
+    switch (code) {
+    case SYSMAT_OK: return "ok";
+    case SYSMAT_ERR_ARG: return "invalid argument or parameter array";
+    case SYSMAT_ERR_CUDA: return "CUDA runtime error";
+    case SYSMAT_ERR_CAPACITY: return "geometry exceeds a documented capacity";
+    case SYSMAT_ERR_IO: return "relationship bitmap file could not be read or written";
+    case SYSMAT_ERR_NOMEM: return "allocation failed";
+    case SYSMAT_ERR_TIMEOUT: return "a bounded device wait gave up";
+    default: return "unknown error";
+    }
+}
+
+extern "C" SYSMAT_API const char* sysmat_version(void) { return "sysmat-b200 0.1 (sm_100a)"; }
+
+extern "C" SYSMAT_API int sysmat_create(sysmat_ctx** out, int device, const float* pC, const float* pD,
+                             const float* pI, const float* pP)
+{
+    if (!out) return SYSMAT_ERR_ARG;
+    *out = nullptr;
+    DevGeom g;
+    int nh0 = 0;
+    int rc = decode(pC, pD, pI, g, nh0);
+    if (rc) return rc;
+    int cur = -1;
+    CUDA_TRY(cudaGetDevice(&cur));
+    if (cur != device) return SYSMAT_ERR_ARG;
+    sysmat_ctx* ctx = new sysmat_ctx();
+    ctx->device = device;
+    ctx->g = g;
+    ctx->n_holes0_host = nh0;
+    ctx->h_img.assign(pI, pI + kNImage);
+    if (pP) ctx->h_phys.assign(pP, pP + kNPhysics);
+    cudaDeviceProp prop;
+    if (cudaGetDeviceProperties(&prop, device) != cudaSuccess) { delete ctx; return SYSMAT_ERR_CUDA; }
+    ctx->num_sms = prop.multiProcessorCount;
+
+    const int D = g.n_det, H = g.n_holes;
+    const size_t n_tables = 4 * (size_t)D + 3 * (size_t)(H > 0 ? H : 1);
+    bool ok = cudaMalloc(&ctx->d_det, sizeof(float) * kNDetector) == cudaSuccess &&
+              cudaMalloc(&ctx->d_col, sizeof(float) * kNCollimator) == cudaSuccess &&
+              cudaMalloc(&ctx->d_img, sizeof(float) * kNImage) == cudaSuccess &&
+              cudaMalloc(&ctx->d_phys, sizeof(float) * kNPhysics) == cudaSuccess &&
+              cudaMalloc(&ctx->d_tables, sizeof(float4) * n_tables) == cudaSuccess &&
+              cudaMalloc(&ctx->d_counter, sizeof(unsigned long long) * 4) == cudaSuccess &&
+              cudaMalloc(&ctx->d_status, sizeof(int) * 4) == cudaSuccess;
+    if (!ok) { sysmat_destroy(ctx); return SYSMAT_ERR_NOMEM; }
+    ok = cudaMemcpy(ctx->d_det, pD, sizeof(float) * kNDetector, cudaMemcpyHostToDevice) == cudaSuccess &&
+         cudaMemset(ctx->d_col, 0, sizeof(float) * kNCollimator) == cudaSuccess &&
+         (!pC || cudaMemcpy(ctx->d_col, pC, sizeof(float) * kNCollimator, cudaMemcpyHostToDevice) == cudaSuccess) &&
+         cudaMemcpy(ctx->d_img, pI, sizeof(float) * kNImage, cudaMemcpyHostToDevice) == cudaSuccess &&
+         cudaMemset(ctx->d_phys, 0, sizeof(float) * kNPhysics) == cudaSuccess &&
+         (!pP || cudaMemcpy(ctx->d_phys, pP, sizeof(float) * kNPhysics, cudaMemcpyHostToDevice) == cudaSuccess);
+    if (!ok) { sysmat_destroy(ctx); return SYSMAT_ERR_CUDA; }
+
+    float4* t = ctx->d_tables;
+    ctx->g.cry.pos = t;
+    ctx->g.cry.size = t + D;
+    ctx->g.cry.mu = t + 2 * D;
+    ctx->g.cry.trig = t + 3 * D;
+    float4* th = t + 4 * D;
+    const int Hs = H > 0 ? H : 1;
+    ctx->g.hole.a = th;
+    ctx->g.hole.b = th + Hs;
+    ctx->g.hole.raw = th + 2 * Hs;
+    derive_crystals<<<(D + 127) / 128, 128>>>(ctx->d_det, g.fov, D, t, t + D, t + 2 * D, t + 3 * D);
+    if (H > 0) derive_holes<<<(H + 127) / 128, 128>>>(ctx->d_col, g.fov, H, th, th + Hs, th + 2 * Hs);
+    if (cudaGetLastError() != cudaSuccess || cudaDeviceSynchronize() != cudaSuccess) {
+        sysmat_destroy(ctx);
+        return SYSMAT_ERR_CUDA;
+    }
+    *out = ctx;
+    return SYSMAT_OK;
+}
+
+extern "C" SYSMAT_API int sysmat_destroy(sysmat_ctx* ctx)
+{
+    if (!ctx) return SYSMAT_OK;
+    scatter_scratch_free(ctx->scratch);
+    cudaFree(ctx->d_det);
+    cudaFree(ctx->d_col);
+    cudaFree(ctx->d_img);
+    cudaFree(ctx->d_phys);
+    cudaFree(ctx->d_tables);
+    cudaFree(ctx->d_counter);
+    cudaFree(ctx->d_status);
+    delete ctx;
+    return SYSMAT_OK;
+}
+
+extern "C" SYSMAT_API int sysmat_dims(const sysmat_ctx* ctx, int* n_det, long long* n_vox, int* n_holes0,
+                           int* n_holes, int* n_layers)
+{
+    if (!ctx) return SYSMAT_ERR_ARG;
+    if (n_det) *n_det = ctx->g.n_det;
+    if (n_vox) *n_vox = ctx->g.nvox;
+    if (n_holes0) *n_holes0 = ctx->g.n_holes0;
+    if (n_holes) *n_holes = ctx->g.n_holes;
+    if (n_layers) *n_layers = ctx->g.n_layers;
+    return SYSMAT_OK;
+}
+
+static int check_block(const sysmat_ctx* ctx, int det_begin, int det_count, long long vox_begin,
+                       long long vox_count, const float* d_out, long long ld)
+{
+    if (!ctx || !d_out) return SYSMAT_ERR_ARG;
+    if (det_begin < 0 || det_count < 0 || det_begin + det_count > ctx->g.n_det) return SYSMAT_ERR_ARG;
+    if (vox_begin < 0 || vox_count < 0 || vox_begin + vox_count > ctx->g.nvox) return SYSMAT_ERR_ARG;
+    if (ld < vox_count) return SYSMAT_ERR_ARG;
+    if (!same_device(ctx)) return SYSMAT_ERR_ARG;
+    return SYSMAT_OK;
+}
+
+extern "C" SYSMAT_API int sysmat_pe(sysmat_ctx* ctx, float rotation, int det_begin, int det_count,
+                         long long vox_begin, long long vox_count, float* d_out, long long ld,
+                         int mode, void* stream)
+{
+    int rc = check_block(ctx, det_begin, det_count, vox_begin, vox_count, d_out, ld);
+    if (rc) return rc;
+    if (mode != SYSMAT_MODE_REFERENCE && mode != SYSMAT_MODE_PRECISE) return SYSMAT_ERR_ARG;
+    if (det_count == 0 || vox_count == 0) return SYSMAT_OK;
+    cudaStream_t s = (cudaStream_t)stream;
+    CUDA_TRY(cudaMemsetAsync(ctx->d_counter, 0, sizeof(unsigned long long), s));
+    CUDA_TRY(cudaMemsetAsync(ctx->d_status, 0, sizeof(int), s));
+    PeLaunch L;
+    L.det_begin = det_begin;
+    L.det_count = det_count;
+    L.vox_begin = vox_begin;
+    L.vox_count = vox_count;
+    L.ld = ld;
+    L.rotation = rotation;
+    L.out = d_out;
+    L.work_counter = ctx->d_counter;
+    L.status = ctx->d_status;
+    if (launch_pe(ctx->g, L, mode, ctx->num_sms, s)) return SYSMAT_ERR_CUDA;
+    int status = 0;
+    CUDA_TRY(cudaMemcpyAsync(&status, ctx->d_status, sizeof(int), cudaMemcpyDeviceToHost, s));
+    CUDA_TRY(cudaStreamSynchronize(s));
+    if (status & kStatusCapacity) return SYSMAT_ERR_CAPACITY;
+    return SYSMAT_OK;
+}
+
+// ------------------------------------------------------------------------------------
+// Reference-compatible entry points.
+
+namespace {
+
+uint64_t fnv1a(uint64_t h, const void* p, size_t n)
+{
+    const unsigned char* b = (const unsigned char*)p;
+    for (size_t i = 0; i < n; ++i) { h ^= b[i]; h *= 1099511628211ull; }
+    return h;
+}
+
+struct LegacySlot {
+    std::mutex mu;
+    uint64_t key = 0;
+    sysmat_ctx* ctx = nullptr;
+    float* d_out = nullptr;
+    size_t out_cap = 0;
+};
+
+LegacySlot& slot_for(int device)
+{
+    static LegacySlot slots[64];
+    return slots[device & 63];
+}
+
+// Context for the given parameter contents (image rotation index excluded), re-used
+// across calls on the same device.
+int legacy_ctx(int device, const float* pC, const float* pD, const float* pI, const float* pP,
+               LegacySlot& slot)
+{
+    float img[kNImage];
+    std::memcpy(img, pI, sizeof(img));
+    img[20] = 0.0f;
+    uint64_t key = 1469598103934665603ull;
+    key = fnv1a(key, pD, sizeof(float) * kNDetector);
+    key = fnv1a(key, img, sizeof(img));
+    if (pC) key = fnv1a(key, pC, sizeof(float) * kNCollimator);
+    else key = fnv1a(key, "noC", 3);
+    if (pP) key = fnv1a(key, pP, sizeof(float) * kNPhysics);
+    else key = fnv1a(key, "noP", 3);
+    if (slot.ctx && slot.key == key) return SYSMAT_OK;
+    if (slot.ctx) { sysmat_destroy(slot.ctx); slot.ctx = nullptr; }
+    int rc = sysmat_create(&slot.ctx, device, pC, pD, pI, pP);
+    if (rc) return rc;
+    slot.key = key;
+    return SYSMAT_OK;
+}
+
+int legacy_out(LegacySlot& slot, size_t n)
+{
+    if (slot.out_cap >= n && slot.d_out) return SYSMAT_OK;
+    cudaFree(slot.d_out);
+    slot.d_out = nullptr;
+    slot.out_cap = 0;
+    if (cudaMalloc(&slot.d_out, sizeof(float) * n) != cudaSuccess) return SYSMAT_ERR_NOMEM;
+    slot.out_cap = n;
+    return SYSMAT_OK;
+}
+
+int select_device(int cuda_id)
+{
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess || n < 1) return SYSMAT_ERR_CUDA;
+    // the reference falls back to the current device when cuda_id is out of range
+    // (scatter.cu:2034-2042)
+    int dev = (cuda_id >= 0 && cuda_id < n) ? cuda_id : 0;
+    if (cudaSetDevice(dev) != cudaSuccess) return SYSMAT_ERR_CUDA;
+    return dev;
+}
+
+}  // namespace
+
+extern "C" SYSMAT_API int PESysMatGen(float* parameter_Collimator, float* parameter_Detector,
+                           float* parameter_Image, float* dst, int cuda_id)
+{
+    if (!parameter_Collimator || !parameter_Detector || !parameter_Image || !dst) return SYSMAT_ERR_ARG;
+    const int dev = select_device(cuda_id);
+    if (dev < 0) return dev;
+    LegacySlot& slot = slot_for(dev);
+    std::lock_guard<std::mutex> lock(slot.mu);
+    int rc = legacy_ctx(dev, parameter_Collimator, parameter_Detector, parameter_Image, nullptr, slot);
+    if (rc) return rc;
+    const int D = slot.ctx->g.n_det;
+    const long long V = slot.ctx->g.nvox;
+    rc = legacy_out(slot, (size_t)D * (size_t)V);
+    if (rc) return rc;
+    rc = sysmat_pe(slot.ctx, parameter_Image[20], 0, D, 0, V, slot.d_out, V, SYSMAT_MODE_REFERENCE,
+                   nullptr);
+    if (rc) return rc;
+    CUDA_TRY(cudaMemcpy(dst, slot.d_out, sizeof(float) * (size_t)D * (size_t)V, cudaMemcpyDeviceToHost));
+    return (int)V;
+}

@@ -1,0 +1,550 @@
+// Photoelectric system-matrix kernel for sm_100a.
+//
+// Computes A[d][v] = sum over the 8x16x8 sub-elements s of crystal d of
+//   Omega_s * exp(-sum mu L) * (1 - exp(-mu_d L_abs,s)) * mu_pe,d / mu_d
+// as the reference kernel photodetectorCudaMe defines it
+// (PEGen_RayTracing_CircularHole/PESysMatGen.cu:951-1364), with a different execution plan:
+//
+//  * a block owns one crystal d and a 4x4x2 brick of voxels (work items handed out by an
+//    atomic counter over a persistent grid); one warp per matrix element; the 32 lanes
+//    take 32 consecutive sub-elements per round, 32 rounds;
+//  * candidate culling runs in three stages.  (1) Block: a conservative superset of the
+//    reference's cone test (:1105-1186) for every voxel of the brick, from the brick's
+//    centre and radius, is compacted into shared memory in the reference's object order.
+//    (2) Warp: the reference cone test itself, with the reference's float formula, on the
+//    superset; a passing object is kept only if its direction-slope rectangle (dx/dy,
+//    dz/dy seen from the voxel) overlaps the one of crystal d.  (3) Lane: an object whose
+//    rectangle does not contain the sub-element ray's slope is skipped.  A skipped object
+//    has an exactly-zero chord in the reference, and adding 0 or fma(mu, 0, x) leaves a
+//    float unchanged, so no stage changes any float result;
+//  * when an element has more kept objects than one shared-memory chunk holds, the warp
+//    walks them chunk by chunk for every round, in the same order, so the attenuation
+//    sums keep the reference's order;
+//  * the plate-bypass penalty (:1240-1254) is skipped for rays whose slope lies inside the
+//    plate's "through both faces" rectangle, where the chord is >= T >= 0.2 mm;
+//  * sub-elements whose plate penalty fired contribute exp(-(>=1e5)) = 0 and stop early
+//    (only when every attenuation coefficient is non-negative);
+//  * the element sum is one float chain in the reference's sub-element order
+//    (SYSMAT_MODE_REFERENCE, the reference's atomicAdd sequence at :1359) or an FP64
+//    accumulation (SYSMAT_MODE_PRECISE); lane 0 writes dst[d][v].
+#include "geom.cuh"
+#include "pe.cuh"
+
+namespace sysmat {
+
+namespace {
+
+constexpr int kWarps = 8;
+constexpr int kThreads = kWarps * 32;
+constexpr int kSuperCap = 1024;         // block superset capacity (objects)
+constexpr int kChunk = 128;             // per-warp kept-object chunk
+constexpr int kBx = 4, kBy = 4, kBz = 2;
+constexpr float kSlopeMargin = 2e-4f;   // slope units; >> FP32 position error / depth
+constexpr float kMinDepth = 1.0f;       // mm; slope rectangles need objects this far behind
+
+struct WarpSmem {
+    float4 rect[kChunk];
+    int id[kChunk];                      // holes: hole index; crystals: n_holes + crystal
+    float4 inner[kMaxLayers];            // plate "through both faces" slope rectangle
+    float chain[32];
+};
+
+struct BlockSmem {
+    float4 sdata[kSuperCap];             // holes: x, (y1+y2)/2, z, crit; crystals: x, y, z, diag
+    int sid[kSuperCap];
+    int warp_cnt[kWarps];
+    int s_count;                         // superset size; -1 = superset overflowed, use all
+    long long item;
+    WarpSmem w[kWarps];
+};
+
+__device__ __forceinline__ bool in_rect(const float4& r, float a, float b)
+{
+    return a >= r.x && a <= r.y && b >= r.z && b <= r.w;
+}
+
+__device__ __forceinline__ bool rects_overlap(const float4& p, const float4& q)
+{
+    return p.x <= q.y && q.x <= p.y && p.z <= q.w && q.z <= p.w;
+}
+
+__device__ __forceinline__ float4 open_rect()
+{
+    return make_float4(-INFINITY, INFINITY, -INFINITY, INFINITY);
+}
+
+// Slope rectangle of a crystal box seen from (px, py, pz), widened by the margin; the open
+// rectangle if any corner is closer than kMinDepth in y.
+__device__ float4 crystal_rect(float4 pos, float4 size, float4 trig, float px, float py, float pz)
+{
+    const float hw = 0.5f * size.x, ht = 0.5f * size.y, hh = 0.5f * size.z;
+    const float y0 = pos.y - ht - py, y1 = pos.y + ht - py;
+    if (!(y0 >= kMinDepth)) return open_rect();
+    const float r0 = 1.0f / y0, r1 = 1.0f / y1;
+    float amin = INFINITY, amax = -INFINITY, bmin = INFINITY, bmax = -INFINITY;
+#pragma unroll
+    for (int c = 0; c < 4; ++c) {
+        const float xs = (c & 1) ? hw : -hw;
+        const float zs = (c & 2) ? hh : -hh;
+        const float x = pos.x + (xs * trig.x - zs * trig.y) - px;
+        const float z = pos.z + (xs * trig.y + zs * trig.x) - pz;
+        amin = fminf(amin, fminf(x * r0, x * r1));
+        amax = fmaxf(amax, fmaxf(x * r0, x * r1));
+        bmin = fminf(bmin, fminf(z * r0, z * r1));
+        bmax = fmaxf(bmax, fmaxf(z * r0, z * r1));
+    }
+    return make_float4(amin - kSlopeMargin, amax + kSlopeMargin, bmin - kSlopeMargin,
+                       bmax + kSlopeMargin);
+}
+
+__device__ float4 hole_rect(float4 ha, float r, float px, float py, float pz)
+{
+    const float y0 = ha.y - py, y1 = ha.z - py;
+    if (!(y0 >= kMinDepth) || !(y1 >= kMinDepth)) return open_rect();
+    const float r0 = 1.0f / y0, r1 = 1.0f / y1;
+    const float xa = ha.x - r - px, xb = ha.x + r - px;
+    const float za = ha.w - r - pz, zb = ha.w + r - pz;
+    const float amin = fminf(fminf(xa * r0, xa * r1), fminf(xb * r0, xb * r1));
+    const float amax = fmaxf(fmaxf(xa * r0, xa * r1), fmaxf(xb * r0, xb * r1));
+    const float bmin = fminf(fminf(za * r0, za * r1), fminf(zb * r0, zb * r1));
+    const float bmax = fmaxf(fmaxf(za * r0, za * r1), fmaxf(zb * r0, zb * r1));
+    return make_float4(amin - kSlopeMargin, amax + kSlopeMargin, bmin - kSlopeMargin,
+                       bmax + kSlopeMargin);
+}
+
+// Object i in the reference's order: holes 0..H-1 (layer by layer), then crystals.
+__device__ __forceinline__ float4 object_data(const DevGeom& g, int i)
+{
+    if (i < g.n_holes) {
+        const float4 a = __ldg(&g.hole.a[i]);
+        const float4 b = __ldg(&g.hole.b[i]);
+        return make_float4(a.x, b.z, a.w, b.w);
+    }
+    const float4 p = __ldg(&g.cry.pos[i - g.n_holes]);
+    return make_float4(p.x, p.y, p.z, __ldg(&g.cry.size[i - g.n_holes].w));
+}
+
+__device__ __forceinline__ int layer_of_hole(const DevGeom& g, int h)
+{
+    int m = 0;
+    while (m + 1 < g.n_layers && h >= g.layer[m + 1].hole_begin) ++m;
+    return m;
+}
+
+// Per-element constants shared by the lanes of a warp.
+struct Elem {
+    float xI, yI, zI;            // voxel centre (rotated)
+    float xIs, yIs, zIs;         // voxel in crystal d's frame
+    float xd, yd, zd, w, t, h;   // crystal d
+    float cosr, sinr;
+    float mu_t, mu_pe;
+    float ux, uy, uz, crit_self; // reference cone test (:1110-1116)
+    float4 rd;                   // slope rectangle of crystal d
+    bool filt;
+};
+
+// Reference cone test of object i against element e (:1120-1184), then the bundle filter.
+// Returns true if the object is kept; rect receives its slope rectangle.
+__device__ __forceinline__ bool keep_object(const DevGeom& g, const Elem& e, int i, float4 od,
+                                            int d, float4& rect)
+{
+    rect = open_rect();
+    bool keep;
+    if (i < g.n_holes) {
+        const float L = sqrtf((e.xI - od.x) * (e.xI - od.x) + (e.yI - od.y) * (e.yI - od.y) +
+                              (e.zI - od.z) * (e.zI - od.z));
+        const float crit = od.w / L;
+        const float vx = (od.x - e.xI) / L, vy = (od.y - e.yI) / L, vz = (od.z - e.zI) / L;
+        keep = sqrtf((vz - e.uz) * (vz - e.uz) + (vy - e.uy) * (vy - e.uy) + (vx - e.ux) * (vx - e.ux)) <=
+               crit + e.crit_self;
+        if (keep && e.filt) {
+            rect = hole_rect(__ldg(&g.hole.a[i]), __ldg(&g.hole.b[i].x), e.xI, e.yI, e.zI);
+            keep = rects_overlap(rect, e.rd);
+        }
+    } else {
+        const int o = i - g.n_holes;
+        if (o == d) return false;
+        const float L = sqrtf((e.xI - od.x) * (e.xI - od.x) + (e.yI - od.y) * (e.yI - od.y) +
+                              (e.zI - od.z) * (e.zI - od.z));
+        const float crit = od.w / L / 2.0f;
+        const float vx = (od.x - e.xI) / L, vy = (od.y - e.yI) / L, vz = (od.z - e.zI) / L;
+        keep = sqrtf((vz - e.uz) * (vz - e.uz) + (vy - e.uy) * (vy - e.uy) + (vx - e.ux) * (vx - e.ux)) <=
+               crit + e.crit_self;
+        if (keep && e.filt) {
+            rect = crystal_rect(__ldg(&g.cry.pos[o]), __ldg(&g.cry.size[o]), __ldg(&g.cry.trig[o]),
+                                e.xI, e.yI, e.zI);
+            keep = rects_overlap(rect, e.rd);
+        }
+    }
+    return keep;
+}
+
+// Fill the warp's chunk with kept objects, scanning source positions [cursor, n_src).
+// Source = block superset (n_src = s_count) or all objects.  Returns the new cursor; the
+// chunk count goes to *count.  Stops early when the chunk could overflow.
+__device__ int build_chunk(const DevGeom& g, const BlockSmem& bs, WarpSmem& ws, const Elem& e,
+                           int d, int cursor, int n_src, bool from_super, int lane, int* count)
+{
+    int n = 0;
+    while (cursor < n_src && n <= kChunk - 32) {
+        const int j = cursor + lane;
+        bool keep = false;
+        float4 rect;
+        int id = 0;
+        if (j < n_src) {
+            id = from_super ? bs.sid[j] : j;
+            const float4 od = from_super ? bs.sdata[j] : object_data(g, j);
+            keep = keep_object(g, e, id, od, d, rect);
+        }
+        const unsigned m = __ballot_sync(0xffffffffu, keep);
+        if (keep) {
+            const int pos = n + __popc(m & ((1u << lane) - 1u));
+            ws.rect[pos] = rect;
+            ws.id[pos] = id;
+        }
+        n += __popc(m);
+        cursor += 32;
+    }
+    __syncwarp();
+    *count = n;
+    return cursor < n_src ? cursor : n_src;
+}
+
+// Attenuation walk state of one lane (one sub-element).
+struct Walk {
+    float att;      // accumulated mu * L
+    float len;      // hole chord sum of the current layer
+    int lay;        // current layer
+};
+
+__device__ __forceinline__ void close_layers(const DevGeom& g, Walk& s, int upto, float cosang)
+{
+    while (s.lay < upto) {                                    // :1281-1284
+        const float lcol = g.layer[s.lay].thickness / cosang;
+        if ((lcol - s.len) >= 0.00001f) s.att = s.att + g.layer[s.lay].mu_total * (lcol - s.len);
+        s.len = 0.0f;
+        ++s.lay;
+    }
+}
+
+// Walk one chunk of kept objects for one sub-element ray (voxel -> (xD, yD, zD)).
+__device__ __forceinline__ void walk_chunk(const DevGeom& g, const WarpSmem& ws, int n, const Elem& e,
+                                           float xD, float yD, float zD, float sa_a, float sa_b,
+                                           float cosang, Walk& s)
+{
+    for (int k = 0; k < n; ++k) {
+        const int id = ws.id[k];
+        if (id < g.n_holes) {
+            const int m = layer_of_hole(g, id);
+            if (m != s.lay) close_layers(g, s, m, cosang);
+            if (!in_rect(ws.rect[k], sa_a, sa_b)) continue;
+            const float4 ha = __ldg(&g.hole.a[id]);
+            const float4 hb = __ldg(&g.hole.b[id]);
+            const float tmp = cyl_chord(e.xI, e.yI, e.zI, xD, yD, zD, ha.x, ha.y, ha.z, ha.w, hb.x);
+            s.len = s.len + tmp;                                 // :1276-1278
+            s.att = s.att + hb.y * tmp;
+        } else {
+            if (s.lay < g.n_layers) close_layers(g, s, g.n_layers, cosang);
+            if (!in_rect(ws.rect[k], sa_a, sa_b)) continue;
+            const int o = id - g.n_holes;
+            const float4 po = __ldg(&g.cry.pos[o]);
+            const float4 so = __ldg(&g.cry.size[o]);
+            const float4 to = __ldg(&g.cry.trig[o]);
+            const float mo = __ldg(&g.cry.mu[o].x);
+            float xa, ya, za, xb, yb, zb;                        // :1295-1323
+            to_crystal_frame(po.x, po.y, po.z, to.z, to.w, e.xI, e.yI, e.zI, xa, ya, za);
+            to_crystal_frame(po.x, po.y, po.z, to.z, to.w, xD, yD, zD, xb, yb, zb);
+            const float la = box_chord(xa, ya, za, xb, yb, zb, -0.5f * so.x, -0.5f * so.y,
+                                       -0.5f * so.z, 0.5f * so.x, 0.5f * so.y, 0.5f * so.z);
+            s.att = s.att + la * mo;
+        }
+    }
+}
+
+struct SubElem {
+    int ix, iy, iz;
+    float xDs, yDs, zDs, xD, yD, zD, dsq, sq, cosang, sa_a, sa_b;
+};
+
+__device__ __forceinline__ SubElem sub_element(const Elem& e, int s)
+{
+    SubElem q;
+    q.iz = s >> 7;
+    q.ix = (s >> 4) & 7;
+    q.iy = s & 15;
+    q.xDs = -e.w / 2.0f + ((float)q.ix + 0.5f) / 8.0f * e.w;   // :1207-1217
+    q.zDs = -e.h / 2.0f + ((float)q.iz + 0.5f) / 8.0f * e.h;
+    q.yDs = -e.t / 2.0f + ((float)q.iy + 0.5f) / 16.0f * e.t;
+    q.xD = e.xd + (q.xDs * e.cosr - q.zDs * e.sinr);
+    q.zD = e.zd + (q.xDs * e.sinr + q.zDs * e.cosr);
+    q.yD = e.yd + q.yDs;
+    q.dsq = (q.yD - e.yI) * (q.yD - e.yI) + (q.xD - e.xI) * (q.xD - e.xI) + (q.zD - e.zI) * (q.zD - e.zI);
+    q.sq = sqrtf(q.dsq);
+    q.cosang = (q.yD - e.yI) / q.sq;
+    if (e.filt) {             // every sub-element lies >= kMinDepth behind the voxel
+        const float rdy = __frcp_rn(q.yD - e.yI);
+        q.sa_a = (q.xD - e.xI) * rdy;
+        q.sa_b = (q.zD - e.zI) * rdy;
+    } else {                  // all rectangles are open: any finite slope passes
+        q.sa_a = 0.0f;
+        q.sa_b = 0.0f;
+    }
+    return q;
+}
+
+// Plate penalty (:1240-1254); true if any layer fired.
+__device__ __forceinline__ bool plate_penalty(const DevGeom& g, const WarpSmem& ws, const Elem& e,
+                                              const SubElem& q, float& att)
+{
+    bool blocked = false;
+    for (int m = 0; m < g.n_layers; ++m) {
+        if (in_rect(ws.inner[m], q.sa_a, q.sa_b)) continue;
+        const LayerInfo& Ly = g.layer[m];
+        const float tl = box_chord(e.xI, e.yI, e.zI, q.xD, q.yD, q.zD, Ly.x1, Ly.y1, Ly.z1, Ly.x2,
+                                   Ly.y2, Ly.z2);
+        if (tl < 0.1f) { att = att + 100000.0f; blocked = true; }
+    }
+    return blocked;
+}
+
+// Self attenuation, absorption and solid angle for a sub-element, given the attenuation
+// accumulated outside crystal d (:1223-1231, :1329-1357).
+__device__ __forceinline__ float finish_sub_element(const Elem& e, const SubElem& q, float att)
+{
+    const float w = e.w, t = e.t, h = e.h;
+    const float ux1 = ((float)q.ix / 8.0f - 0.5f) * w;
+    const float ux2 = (((float)q.ix + 1.0f) / 8.0f - 0.5f) * w;
+    const float uy1 = ((float)q.iy / 16.0f - 0.5f) * t;
+    const float uy2 = (((float)q.iy + 1.0f) / 16.0f - 0.5f) * t;
+    const float uz1 = ((float)q.iz / 8.0f - 0.5f) * h;
+    const float uz2 = (((float)q.iz + 1.0f) / 8.0f - 0.5f) * h;
+    const float l1 = box_chord_inside(e.xIs, e.yIs, e.zIs, q.xDs, q.yDs, q.zDs, -w / 2.0f, -t / 2.0f,
+                                      -h / 2.0f, w / 2.0f, t / 2.0f, h / 2.0f);
+    const float l2 = box_chord_inside(e.xIs, e.yIs, e.zIs, q.xDs, q.yDs, q.zDs, ux1, uy1, uz1, ux2,
+                                      uy2, uz2);
+    att = att + (l1 - l2) * e.mu_t;
+    const float eff = 1.0f * expf(-att);
+    const float xt = q.xDs + 1000.0f * (q.xDs - e.xIs) / q.sq;
+    const float yt = q.yDs + 1000.0f * (q.yDs - e.yIs) / q.sq;
+    const float zt = q.zDs + 1000.0f * (q.zDs - e.zIs) / q.sq;
+    const float labs = box_chord(e.xIs, e.yIs, e.zIs, xt, yt, zt, ux1, uy1, uz1, ux2, uy2, uz2);
+    const float absf = (1.0f - expf(-labs * e.mu_t)) * e.mu_pe / e.mu_t;
+    // solid angle in double, as the reference's 4*M_PI promotion makes it; one shared
+    // reciprocal (the float results round identically except in double-rounding ties)
+    const double rq = 1.0 / ((4.0 * 3.14159265358979323846) * (double)q.dsq * (double)q.sq);
+    const float ax = t * h / 8.0f / 16.0f, az = w * t / 8.0f / 16.0f, ay = w * h / 8.0f / 8.0f;
+    const float sax = (float)((double)ax * (double)fabsf((q.xD - e.xI) * e.cosr - (q.zD - e.zI) * e.sinr) * rq);
+    const float saz = (float)((double)az * (double)fabsf((q.xD - e.xI) * e.sinr + (q.zD - e.zI) * e.cosr) * rq);
+    const float say = (float)((double)ay * (double)fabsf(q.yD - e.yI) * rq);
+    const float sxy = (sax >= say) ? sax : say;
+    const float sa = (sxy >= saz) ? sxy : saz;
+    return eff * sa * absf;
+}
+
+template <int MODE>
+__device__ float pe_element(const DevGeom& g, const BlockSmem& bs, WarpSmem& ws, int d,
+                            long long v, float cr, float sr, int lane)
+{
+    Elem e;
+    voxel_centre(g, v, cr, sr, e.xI, e.yI, e.zI);
+    const float4 P = __ldg(&g.cry.pos[d]);
+    const float4 S = __ldg(&g.cry.size[d]);
+    const float4 M = __ldg(&g.cry.mu[d]);
+    const float4 T = __ldg(&g.cry.trig[d]);
+    e.xd = P.x; e.yd = P.y; e.zd = P.z;
+    e.w = S.x; e.t = S.y; e.h = S.z;
+    e.mu_t = M.x; e.mu_pe = M.y;
+    e.cosr = T.x; e.sinr = T.y;
+    if (!(e.mu_t > 0.01f)) return 0.0f;                    // :1107, :1194
+    to_crystal_frame(e.xd, e.yd, e.zd, T.z, T.w, e.xI, e.yI, e.zI, e.xIs, e.yIs, e.zIs);
+    const float dist = sqrtf((e.yd - e.yI) * (e.yd - e.yI) + (e.xd - e.xI) * (e.xd - e.xI) +
+                             (e.zd - e.zI) * (e.zd - e.zI));
+    e.crit_self = S.w / dist / 2.0f;
+    e.ux = (e.xd - e.xI) / dist;
+    e.uy = (e.yd - e.yI) / dist;
+    e.uz = (e.zd - e.zI) / dist;
+    e.rd = crystal_rect(P, S, T, e.xI, e.yI, e.zI);
+    e.filt = isfinite(e.rd.x);
+
+    if (lane < g.n_layers) {          // plate "through both faces" rectangles
+        const LayerInfo& Ly = g.layer[lane];
+        float4 inner = make_float4(INFINITY, -INFINITY, INFINITY, -INFINITY);   // empty
+        const float f0 = Ly.y1 - e.yI, f1 = Ly.y2 - e.yI;
+        const float behind = e.yd - 0.5f * e.t - Ly.y2;
+        if (e.filt && f0 >= kMinDepth && behind >= kMinDepth && (Ly.y2 - Ly.y1) >= 0.2f) {
+            const float r0 = 1.0f / f0, r1 = 1.0f / f1;
+            inner.x = fmaxf((Ly.x1 - e.xI) * r0, (Ly.x1 - e.xI) * r1) + kSlopeMargin;
+            inner.y = fminf((Ly.x2 - e.xI) * r0, (Ly.x2 - e.xI) * r1) - kSlopeMargin;
+            inner.z = fmaxf((Ly.z1 - e.zI) * r0, (Ly.z1 - e.zI) * r1) + kSlopeMargin;
+            inner.w = fminf((Ly.z2 - e.zI) * r0, (Ly.z2 - e.zI) * r1) - kSlopeMargin;
+        }
+        ws.inner[lane] = inner;
+    }
+
+    const bool from_super = bs.s_count >= 0;
+    const int n_src = from_super ? bs.s_count : g.n_holes + g.n_det;
+    int count = 0;
+    int cursor = build_chunk(g, bs, ws, e, d, 0, n_src, from_super, lane, &count);
+    const bool single = cursor >= n_src;
+
+    float chain = 0.0f;
+    double dacc = 0.0;
+    for (int r = 0; r < 32; ++r) {
+        const SubElem q = sub_element(e, r * 32 + lane);
+        Walk s{0.0f, 0.0f, 0};
+        const bool blocked = plate_penalty(g, ws, e, q, s.att);
+        const bool skip = blocked && g.nonneg_mu;
+        if (single) {
+            if (!skip) walk_chunk(g, ws, count, e, q.xD, q.yD, q.zD, q.sa_a, q.sa_b, q.cosang, s);
+        } else {
+            // chunked walk: rebuild the chunks for this round (the warp stays converged)
+            int cur = 0;
+            while (cur < n_src) {
+                if (r > 0 || cur > 0) cur = build_chunk(g, bs, ws, e, d, cur, n_src, from_super, lane, &count);
+                else cur = cursor;
+                if (!skip) walk_chunk(g, ws, count, e, q.xD, q.yD, q.zD, q.sa_a, q.sa_b, q.cosang, s);
+                __syncwarp();
+            }
+        }
+        float contrib = 0.0f;
+        if (!skip) {
+            if (s.lay < g.n_layers) close_layers(g, s, g.n_layers, q.cosang);
+            contrib = finish_sub_element(e, q, s.att);
+        }
+        if constexpr (MODE == 0) {
+            ws.chain[lane] = contrib;
+            __syncwarp();
+#pragma unroll
+            for (int k = 0; k < 32; ++k) chain = chain + ws.chain[k];
+            __syncwarp();
+        } else {
+            dacc += (double)contrib;
+        }
+    }
+    if constexpr (MODE == 0) return chain;
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) dacc += __shfl_xor_sync(0xffffffffu, dacc, off);
+    return (float)dacc;
+}
+
+// Block superset of the reference cone test over all voxels within radius rho of
+// (cx, cy, cz): keep object o when |u_o - u_d| <= (rho + r_o)/(L_o - rho)
+// + (rho + r_d)/(L_d - rho) + 1e-4 at the centre (each direction moves by at most
+// rho/(L - rho) in chord length, each angular radius r/L grows to at most r/(L - rho)).
+__device__ void build_superset(const DevGeom& g, BlockSmem& bs, int d, float cx, float cy, float cz,
+                               float rho)
+{
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    const float4 P = __ldg(&g.cry.pos[d]);
+    const float rdd = 0.5f * __ldg(&g.cry.size[d].w);
+    const float Ld = sqrtf((P.x - cx) * (P.x - cx) + (P.y - cy) * (P.y - cy) + (P.z - cz) * (P.z - cz));
+    const float uxd = (P.x - cx) / Ld, uyd = (P.y - cy) / Ld, uzd = (P.z - cz) / Ld;
+    const bool near_d = !(Ld - rho > 0.5f);
+    const float td = near_d ? 0.0f : (rho + rdd) / (Ld - rho);
+    const int N = g.n_holes + g.n_det;
+    int running = 0;
+    for (int base = 0; base < N; base += kThreads) {
+        const int i = base + threadIdx.x;
+        bool keep = false;
+        float4 od = make_float4(0.f, 0.f, 0.f, 0.f);
+        if (i < N && !(i >= g.n_holes && i - g.n_holes == d)) {
+            od = object_data(g, i);
+            const float ro = (i < g.n_holes) ? od.w : 0.5f * od.w;
+            const float Lo = sqrtf((od.x - cx) * (od.x - cx) + (od.y - cy) * (od.y - cy) +
+                                   (od.z - cz) * (od.z - cz));
+            if (near_d || !(Lo - rho > 0.5f)) {
+                keep = true;
+            } else {
+                const float dx = (od.x - cx) / Lo - uxd, dy = (od.y - cy) / Lo - uyd,
+                            dz = (od.z - cz) / Lo - uzd;
+                const float thr = (rho + ro) / (Lo - rho) + td + 1e-4f;
+                keep = sqrtf(dx * dx + dy * dy + dz * dz) <= thr;
+            }
+        }
+        const unsigned m = __ballot_sync(0xffffffffu, keep);
+        if (lane == 0) bs.warp_cnt[wid] = __popc(m);
+        __syncthreads();
+        int off = running, tot = 0;
+        for (int k = 0; k < kWarps; ++k) {
+            const int c = bs.warp_cnt[k];
+            if (k < wid) off += c;
+            tot += c;
+        }
+        const int pos = off + __popc(m & ((1u << lane) - 1u));
+        if (keep && pos < kSuperCap) {
+            bs.sdata[pos] = od;
+            bs.sid[pos] = i;
+        }
+        running += tot;
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) bs.s_count = (running <= kSuperCap) ? running : -1;
+    __syncthreads();
+}
+
+template <int MODE>
+__global__ void __launch_bounds__(kThreads, 2) pe_kernel(DevGeom g, PeLaunch L)
+{
+    __shared__ BlockSmem bs;
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    WarpSmem& ws = bs.w[wid];
+    const float ang = L.rotation * g.angle_step;           // :1006
+    const float cr = cosf(ang), sr = sinf(ang);
+    const long long nxy = (long long)g.nx * g.ny;
+    const long long vlast = L.vox_begin + L.vox_count - 1;
+    const int iz0 = (int)(L.vox_begin / nxy), iz1 = (int)(vlast / nxy);
+    const int nbx = (g.nx + kBx - 1) / kBx, nby = (g.ny + kBy - 1) / kBy;
+    const int nbz = (iz1 - iz0 + 1 + kBz - 1) / kBz;
+    const long long n_bricks = (long long)nbx * nby * nbz;
+    const long long total = n_bricks * L.det_count;
+    for (;;) {
+        if (threadIdx.x == 0) bs.item = (long long)atomicAdd(L.work_counter, 1ull);
+        __syncthreads();
+        const long long item = bs.item;
+        __syncthreads();
+        if (item >= total) break;
+        const int di = (int)(item / n_bricks);
+        const long long b = item - (long long)di * n_bricks;
+        const int bz = (int)(b / ((long long)nbx * nby));
+        const int rem = (int)(b - (long long)bz * nbx * nby);
+        const int by = rem / nbx, bx = rem - by * nbx;
+        const int x0 = bx * kBx, y0 = by * kBy, z0 = iz0 + bz * kBz;
+        const int x1 = min(x0 + kBx, g.nx) - 1, y1 = min(y0 + kBy, g.ny) - 1, z1 = min(z0 + kBz, iz1 + 1) - 1;
+        const int d = L.det_begin + di;
+        // brick centre and radius from its extreme voxel centres (rotation about z keeps lengths)
+        float ax, ay, az, bxx, byy, bzz;
+        voxel_centre(g, x0 + g.nx * ((long long)y0 + g.ny * z0), 1.0f, 0.0f, ax, ay, az);
+        voxel_centre(g, x1 + g.nx * ((long long)y1 + g.ny * z1), 1.0f, 0.0f, bxx, byy, bzz);
+        const float mx = 0.5f * (ax + bxx), my = 0.5f * (ay + byy), mz = 0.5f * (az + bzz);
+        const float rho = 0.5f * sqrtf((bxx - ax) * (bxx - ax) + (byy - ay) * (byy - ay) +
+                                       (bzz - az) * (bzz - az)) + 1e-3f;
+        build_superset(g, bs, d, mx * cr - my * sr, mx * sr + my * cr, mz, rho);
+        for (int slot = wid; slot < kBx * kBy * kBz; slot += kWarps) {
+            const int ox = slot % kBx, oy = (slot / kBx) % kBy, oz = slot / (kBx * kBy);
+            const int ix = x0 + ox, iy = y0 + oy, iz = z0 + oz;
+            if (ix >= g.nx || iy >= g.ny || iz > z1) continue;
+            const long long v = ix + g.nx * ((long long)iy + (long long)g.ny * iz);
+            if (v < L.vox_begin || v > vlast) continue;
+            const float val = pe_element<MODE>(g, bs, ws, d, v, cr, sr, lane);
+            if (lane == 0) L.out[(long long)di * L.ld + (v - L.vox_begin)] = val;
+            __syncwarp();
+        }
+        __syncthreads();
+    }
+}
+
+}  // namespace
+
+int launch_pe(const DevGeom& g, const PeLaunch& L, int mode, int num_sms, cudaStream_t stream)
+{
+    int per_sm = 0;
+    if (mode == 0) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, pe_kernel<0>, kThreads, 0);
+    else           cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, pe_kernel<1>, kThreads, 0);
+    if (per_sm < 1) per_sm = 1;
+    const int blocks = num_sms * per_sm;
+    if (mode == 0) pe_kernel<0><<<blocks, kThreads, 0, stream>>>(g, L);
+    else           pe_kernel<1><<<blocks, kThreads, 0, stream>>>(g, L);
+    return cudaGetLastError() == cudaSuccess ? 0 : -1;
+}
+
+}  // namespace sysmat

@@ -1,0 +1,221 @@
+"""Python binding of libsysmat.so (ctypes) — the host-side mirror of the reference API.
+
+`PESysMatGen` and the three `scatter` programs keep the reference's host-buffer calling
+convention (PEGen_RayTracing_CircularHole/PESysMatGen.h:4-5 and the three scatter.h
+headers).  `Context` exposes the native device API on torch CUDA tensors, which is what the
+tests and the benchmark use.  The library must be built (make -C <this directory>); there
+is no CPU fallback: every call fails loudly if the CUDA library is missing.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libsysmat.so")
+
+OK = 0
+ERRORS = {-1: "SYSMAT_ERR_ARG", -2: "SYSMAT_ERR_CUDA", -3: "SYSMAT_ERR_CAPACITY",
+          -4: "SYSMAT_ERR_IO", -5: "SYSMAT_ERR_NOMEM", -6: "SYSMAT_ERR_TIMEOUT"}
+MODE_REFERENCE = 0
+MODE_PRECISE = 1
+SCATTER_CRYSTAL = 1
+SCATTER_COLLIMATOR = 2
+HOLE_MODEL_COMBINED = 0
+HOLE_MODEL_VARIANT = 1
+
+# Every symbol declared in include/sysmat.h.
+EXPORTS = ("PESysMatGen", "scatter", "scatter_collimator", "scatter_crystal", "sysmat_create",
+           "sysmat_destroy", "sysmat_dims", "sysmat_pe", "sysmat_bitmap_crystal_words",
+           "sysmat_bitmap_collimator_words", "sysmat_bitmap_crystal", "sysmat_bitmap_collimator",
+           "sysmat_scatter", "sysmat_error_string", "sysmat_version")
+
+_fp = ctypes.POINTER(ctypes.c_float)
+_vp = ctypes.c_void_p
+_lib = None
+
+
+class SysmatError(RuntimeError):
+    def __init__(self, code, what=""):
+        self.code = code
+        name = ERRORS.get(code, str(code))
+        super().__init__(f"{what}: {name} ({lib().sysmat_error_string(code).decode()})")
+
+
+def lib():
+    """Load libsysmat.so; raises if it has not been built."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError(f"{LIB_PATH} is missing: build it with `make -C {HERE}`")
+        L = ctypes.CDLL(LIB_PATH)
+        sigs = {
+            "PESysMatGen": ([_fp, _fp, _fp, _fp, ctypes.c_int], ctypes.c_int),
+            "scatter": ([_fp, _fp, _fp, _fp, _fp, ctypes.c_char_p, ctypes.c_char_p, _fp, ctypes.c_int],
+                        ctypes.c_int),
+            "scatter_collimator": ([_fp, _fp, _fp, _fp, _fp, ctypes.c_char_p, _fp, ctypes.c_int],
+                                   ctypes.c_int),
+            "scatter_crystal": ([_fp, _fp, _fp, _fp, ctypes.c_char_p, _fp, ctypes.c_int], ctypes.c_int),
+            "sysmat_create": ([ctypes.POINTER(_vp), ctypes.c_int, _fp, _fp, _fp, _fp], ctypes.c_int),
+            "sysmat_destroy": ([_vp], ctypes.c_int),
+            "sysmat_dims": ([_vp, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_longlong),
+                             ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int),
+                             ctypes.POINTER(ctypes.c_int)], ctypes.c_int),
+            "sysmat_pe": ([_vp, ctypes.c_float, ctypes.c_int, ctypes.c_int, ctypes.c_longlong,
+                           ctypes.c_longlong, _vp, ctypes.c_longlong, ctypes.c_int, _vp], ctypes.c_int),
+            "sysmat_bitmap_crystal_words": ([_vp], ctypes.c_longlong),
+            "sysmat_bitmap_collimator_words": ([_vp], ctypes.c_longlong),
+            "sysmat_bitmap_crystal": ([_vp, _vp, _vp], ctypes.c_int),
+            "sysmat_bitmap_collimator": ([_vp, _vp, _vp], ctypes.c_int),
+            "sysmat_scatter": ([_vp, ctypes.c_int, ctypes.c_int, ctypes.c_float, _vp, _vp, _vp,
+                                ctypes.c_int, ctypes.c_int, ctypes.c_longlong, ctypes.c_longlong, _vp,
+                                ctypes.c_longlong, _vp], ctypes.c_int),
+            "sysmat_error_string": ([ctypes.c_int], ctypes.c_char_p),
+            "sysmat_version": ([], ctypes.c_char_p),
+        }
+        for name, (args, res) in sigs.items():
+            if hasattr(L, name):
+                fn = getattr(L, name)
+                fn.argtypes = args
+                fn.restype = res
+        _lib = L
+    return _lib
+
+
+def _check(rc, what):
+    if rc < 0:
+        raise SysmatError(rc, what)
+    return rc
+
+
+def _f32(a):
+    a = np.ascontiguousarray(a, dtype=np.float32)
+    return a, a.ctypes.data_as(_fp)
+
+
+def _ptr(t):
+    return ctypes.c_void_p(t.data_ptr())
+
+
+def _stream(stream):
+    if stream is None:
+        import torch
+        stream = torch.cuda.current_stream()
+    return ctypes.c_void_p(stream.cuda_stream)
+
+
+# ---------------------------------------------------------------------------------------
+# Reference-compatible entry points (host buffers).
+
+def PESysMatGen(collimator, detector, image, dst, cuda_id=0):
+    """dst: float32 numpy array of at least D*V elements (written in place).  Returns V."""
+    c, pc = _f32(collimator)
+    d, pd = _f32(detector)
+    i, pi = _f32(image)
+    if dst.dtype != np.float32 or not dst.flags.c_contiguous:
+        raise ValueError("dst must be a contiguous float32 array")
+    return _check(lib().PESysMatGen(pc, pd, pi, dst.ctypes.data_as(_fp), cuda_id), "PESysMatGen")
+
+
+def scatter(collimator, detector, image, physics, pe, fname_crystal, fname_collimator, dst, cuda_id=0):
+    c, pc = _f32(collimator)
+    d, pd = _f32(detector)
+    i, pi = _f32(image)
+    p, pp = _f32(physics)
+    m, pm = _f32(pe)
+    return _check(lib().scatter(pc, pd, pi, pp, pm, fname_crystal.encode(), fname_collimator.encode(),
+                                dst.ctypes.data_as(_fp), cuda_id), "scatter")
+
+
+def scatter_collimator(collimator, detector, image, physics, pe, fname, dst, cuda_id=0):
+    c, pc = _f32(collimator)
+    d, pd = _f32(detector)
+    i, pi = _f32(image)
+    p, pp = _f32(physics)
+    m, pm = _f32(pe)
+    return _check(lib().scatter_collimator(pc, pd, pi, pp, pm, fname.encode(),
+                                           dst.ctypes.data_as(_fp), cuda_id), "scatter_collimator")
+
+
+def scatter_crystal(detector, image, physics, pe, fname, dst, cuda_id=0):
+    d, pd = _f32(detector)
+    i, pi = _f32(image)
+    p, pp = _f32(physics)
+    m, pm = _f32(pe)
+    return _check(lib().scatter_crystal(pd, pi, pp, pm, fname.encode(), dst.ctypes.data_as(_fp),
+                                        cuda_id), "scatter_crystal")
+
+
+# ---------------------------------------------------------------------------------------
+# Native API on torch CUDA tensors.
+
+class Context:
+    """One uploaded system on one device (sysmat_create / sysmat_destroy)."""
+
+    def __init__(self, geo, device=0):
+        import torch
+        self.device = device
+        torch.cuda.set_device(device)
+        self._arrays = [_f32(geo.collimator), _f32(geo.detector), _f32(geo.image), _f32(geo.physics)]
+        h = ctypes.c_void_p()
+        (c, pc), (d, pd), (i, pi), (p, pp) = self._arrays
+        _check(lib().sysmat_create(ctypes.byref(h), device, pc, pd, pi, pp), "sysmat_create")
+        self.handle = h
+        nd, nv, nh0, nh, nl = (ctypes.c_int(), ctypes.c_longlong(), ctypes.c_int(), ctypes.c_int(),
+                               ctypes.c_int())
+        _check(lib().sysmat_dims(h, ctypes.byref(nd), ctypes.byref(nv), ctypes.byref(nh0),
+                                 ctypes.byref(nh), ctypes.byref(nl)), "sysmat_dims")
+        self.n_det, self.n_vox = nd.value, nv.value
+        self.n_holes0, self.n_holes, self.n_layers = nh0.value, nh.value, nl.value
+
+    def close(self):
+        if self.handle:
+            lib().sysmat_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def pe(self, out, rotation=0.0, det_begin=0, det_count=None, vox_begin=0, vox_count=None,
+           mode=MODE_REFERENCE, stream=None):
+        """Fill `out` (CUDA float32, rows x >=vox_count, row-contiguous) with the PE block."""
+        det_count = self.n_det - det_begin if det_count is None else det_count
+        vox_count = self.n_vox - vox_begin if vox_count is None else vox_count
+        ld = out.stride(0) if out.dim() == 2 else vox_count
+        _check(lib().sysmat_pe(self.handle, float(rotation), det_begin, det_count, vox_begin, vox_count,
+                               _ptr(out), ld, mode, _stream(stream)), "sysmat_pe")
+        return out
+
+    def bitmap_crystal(self, stream=None):
+        import torch
+        n = lib().sysmat_bitmap_crystal_words(self.handle)
+        out = torch.empty(max(n, 1), dtype=torch.int32, device=f"cuda:{self.device}")
+        _check(lib().sysmat_bitmap_crystal(self.handle, _ptr(out), _stream(stream)), "bitmap_crystal")
+        return out[:n]
+
+    def bitmap_collimator(self, stream=None):
+        import torch
+        n = lib().sysmat_bitmap_collimator_words(self.handle)
+        out = torch.empty(max(n, 1), dtype=torch.int32, device=f"cuda:{self.device}")
+        _check(lib().sysmat_bitmap_collimator(self.handle, _ptr(out), _stream(stream)),
+               "bitmap_collimator")
+        return out[:n]
+
+    def scatter(self, out, pe, parts=SCATTER_CRYSTAL | SCATTER_COLLIMATOR,
+                hole_model=HOLE_MODEL_COMBINED, bm_crystal=None, bm_collimator=None, rotation=0.0,
+                det_begin=0, det_count=None, vox_begin=0, vox_count=None, stream=None):
+        det_count = self.n_det - det_begin if det_count is None else det_count
+        vox_count = self.n_vox - vox_begin if vox_count is None else vox_count
+        ld = out.stride(0) if out.dim() == 2 else vox_count
+        nullp = ctypes.c_void_p(0)
+        _check(lib().sysmat_scatter(self.handle, parts, hole_model, float(rotation), _ptr(pe),
+                                    _ptr(bm_crystal) if bm_crystal is not None else nullp,
+                                    _ptr(bm_collimator) if bm_collimator is not None else nullp,
+                                    det_begin, det_count, vox_begin, vox_count, _ptr(out), ld,
+                                    _stream(stream)), "sysmat_scatter")
+        return out

@@ -1,0 +1,135 @@
+/* sysmat: B200-native SPECT system-matrix generator — public C ABI.
+ *
+ * Two layers of entry points:
+ *
+ * 1. Reference-compatible entry points.  Same names (where C allows), same argument
+ *    meaning, same host-buffer ownership and output layout as the reference programs.
+ *    A reference CLI re-linked against libsysmat.so runs unchanged (see
+ *    include/sysmat_compat.hpp for the C++ overloads of `scatter`).
+ *
+ * 2. A native, handle-based API on device pointers and a caller-supplied CUDA stream,
+ *    used by the reference-compatible layer, the tests and the benchmark.  It never
+ *    calls cudaSetDevice behind the caller's back and never exits the process.
+ *
+ * Matrix layout everywhere: float dst[detector][voxel], voxel v = ix + Nx*(iy + Ny*iz)
+ * (reference PESysMatGen.cu:1025, :1031-1034).  Parameter arrays: float32, 80000
+ * (collimator), 80000 (detector), 100 (image), 100 (physics) values, laid out as in the
+ * reference (PESysMatGen.cu:961-1075, scatter.cu:1144-1167).
+ *
+ * Errors: every function returns an int; negative values are SYSMAT_ERR_* codes.
+ */
+#ifndef SYSMAT_H
+#define SYSMAT_H
+
+#if defined(SYSMAT_BUILD)
+#define SYSMAT_API __attribute__((visibility("default")))
+#else
+#define SYSMAT_API
+#endif
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define SYSMAT_OK 0
+#define SYSMAT_ERR_ARG (-1)        /* invalid argument or parameter array */
+#define SYSMAT_ERR_CUDA (-2)       /* a CUDA runtime call failed */
+#define SYSMAT_ERR_CAPACITY (-3)   /* a geometry exceeds a documented capacity */
+#define SYSMAT_ERR_IO (-4)         /* a relationship-bitmap file could not be read/written */
+#define SYSMAT_ERR_NOMEM (-5)      /* device or host allocation failed */
+#define SYSMAT_ERR_TIMEOUT (-6)    /* a bounded device wait gave up */
+
+/* Summation modes of the photoelectric kernel. */
+#define SYSMAT_MODE_REFERENCE 0    /* sub-element sum as one float chain in reference order */
+#define SYSMAT_MODE_PRECISE 1      /* sub-element sum accumulated in FP64 */
+
+/* Scatter parts (bit mask) and collimator solid-angle models. */
+#define SYSMAT_SCATTER_CRYSTAL 1
+#define SYSMAT_SCATTER_COLLIMATOR 2
+#define SYSMAT_HOLE_MODEL_COMBINED 0   /* ScatterGen_RayTracing_CircularHole/scatter.cu:1711-1716 */
+#define SYSMAT_HOLE_MODEL_VARIANT 1    /* ScatterGen_Collimator/scatter.cu:1212-1215 */
+
+/* ---------------------------------------------------------------------------------- */
+/* Reference-compatible entry points (host buffers in, host buffers out, synchronous). */
+
+/* Replaces PESysMatGen (PEGen_RayTracing_CircularHole/PESysMatGen.h:4-5, defined at
+ * PESysMatGen.cu:1368).  Reads 80000/80000/100 floats; writes D*V floats of the rotation
+ * parameter_Image[20] into dst.  Returns V (the number of voxels) or a SYSMAT_ERR_* code.
+ * The reference computes in one float chain per element; so does this entry point. */
+SYSMAT_API int PESysMatGen(float* parameter_Collimator, float* parameter_Detector, float* parameter_Image,
+                float* dst, int cuda_id);
+
+/* Replaces scatter of the combined program (ScatterGen_RayTracing_CircularHole/scatter.h:4-5,
+ * scatter.cu:2013).  PE_SysMat: the D*V photoelectric matrix read from offset 0.  The
+ * bitmaps are computed and written to the named files when parameter_Physics[8] / [9]
+ * equal 1, else read from them (scatter.cu:2116-2164, :2246-2296).  Writes D*V floats =
+ * collimator scatter + crystal scatter.  Returns V or a SYSMAT_ERR_* code. */
+SYSMAT_API int scatter(float* parameter_Collimator, float* parameter_Detector, float* parameter_Image,
+            float* parameter_Physics, float* PE_SysMat, const char* FnameGeoCrystal,
+            const char* FnameGeoCollimator, float* dst, int cuda_id);
+
+/* Replaces scatter of the collimator-only program (ScatterGen_Collimator/scatter.h:4-5,
+ * scatter.cu:1511): collimator scatter with that program's hole solid angle. */
+SYSMAT_API int scatter_collimator(float* parameter_Collimator, float* parameter_Detector,
+                       float* parameter_Image, float* parameter_Physics, float* PE_SysMat,
+                       const char* FnameGeo, float* dst, int cuda_id);
+
+/* Replaces scatter of the crystal-only program (ScatterGen_Crystal/scatter.h:4-5,
+ * scatter.cu:1528): inter-crystal scatter only. */
+SYSMAT_API int scatter_crystal(float* parameter_Detector, float* parameter_Image, float* parameter_Physics,
+                    float* PE_SysMat, const char* FnameGeo, float* dst, int cuda_id);
+
+/* ---------------------------------------------------------------------------------- */
+/* Native API.  The caller makes `device` current before every call that takes a ctx.   */
+
+typedef struct sysmat_ctx sysmat_ctx;
+
+/* Parse and upload one system.  pC/pD/pI/pP are host arrays of 80000/80000/100/100
+ * floats (pC may be NULL for crystal-only use, pP may be NULL for PE-only use).  Derived
+ * per-crystal and per-hole tables are computed on the device. */
+SYSMAT_API int sysmat_create(sysmat_ctx** out, int device, const float* pC, const float* pD,
+                  const float* pI, const float* pP);
+SYSMAT_API int sysmat_destroy(sysmat_ctx* ctx);
+
+/* Geometry sizes: D, V (all voxels), holes of layer 0, total holes, layers. */
+SYSMAT_API int sysmat_dims(const sysmat_ctx* ctx, int* n_det, long long* n_vox, int* n_holes0,
+                int* n_holes, int* n_layers);
+
+/* Photoelectric matrix block for one rotation index: detectors [det_begin,
+ * det_begin+det_count) x voxels [vox_begin, vox_begin+vox_count), written to d_out with
+ * row stride ld (floats).  mode: SYSMAT_MODE_*.  Asynchronous on `stream`
+ * (cudaStream_t; NULL = legacy default stream). */
+SYSMAT_API int sysmat_pe(sysmat_ctx* ctx, float rotation, int det_begin, int det_count, long long vox_begin,
+              long long vox_count, float* d_out, long long ld, int mode, void* stream);
+
+/* Relationship bitmaps in the reference's word layout (scatter.cu:1040-1074).
+ * Word counts: crystal ceil(D(D+1)/2*D/32), collimator ceil(H0*D*D/32). */
+SYSMAT_API long long sysmat_bitmap_crystal_words(const sysmat_ctx* ctx);
+SYSMAT_API long long sysmat_bitmap_collimator_words(const sysmat_ctx* ctx);
+SYSMAT_API int sysmat_bitmap_crystal(sysmat_ctx* ctx, uint32_t* d_words, void* stream);
+SYSMAT_API int sysmat_bitmap_collimator(sysmat_ctx* ctx, uint32_t* d_words, void* stream);
+
+/* Primary-Compton scatter block.  parts: SYSMAT_SCATTER_* mask.  d_pe: the D x V
+ * photoelectric matrix (row stride V) the crystal part reads.  d_bm_crystal /
+ * d_bm_collimator: bitmaps as produced above or loaded from the reference's files.
+ * hole_model: SYSMAT_HOLE_MODEL_*.  With both parts the result is
+ * float(collimator) + float(crystal), as the reference sums on the host. */
+SYSMAT_API int sysmat_scatter(sysmat_ctx* ctx, int parts, int hole_model, float rotation, const float* d_pe,
+                   const uint32_t* d_bm_crystal, const uint32_t* d_bm_collimator, int det_begin,
+                   int det_count, long long vox_begin, long long vox_count, float* d_out,
+                   long long ld, void* stream);
+
+/* Text for a SYSMAT_ERR_* code. */
+SYSMAT_API const char* sysmat_error_string(int code);
+
+/* Library build identification (for logs): returns a static string. */
+SYSMAT_API const char* sysmat_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* SYSMAT_H */

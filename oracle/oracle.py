@@ -1,0 +1,142 @@
+"""Test infrastructure only: ctypes binding of the CPU oracle (liboracle.so).
+
+The oracle restates the reference's algorithm in C (sysmat_oracle.c, oracle_body.h) in
+two precisions: 32 = the reference's float arithmetic, 64 = the same program widened to
+double.  Tests, the smoke check and bench.py's CPU-baseline leg use it as the checker.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "liboracle.so")
+
+_lib = None
+_fp = ctypes.POINTER(ctypes.c_float)
+_dp = ctypes.POINTER(ctypes.c_double)
+_ip = ctypes.POINTER(ctypes.c_int)
+_u32p = ctypes.POINTER(ctypes.c_uint32)
+_i64p = ctypes.POINTER(ctypes.c_longlong)
+
+
+def build() -> None:
+    subprocess.run(["make", "-s", "-C", HERE, "liboracle.so"], check=True)
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            build()
+        L = ctypes.CDLL(LIB_PATH)
+        L.oracle_pe.argtypes = [_fp, _fp, _fp, ctypes.c_int, _ip, ctypes.c_int, ctypes.c_longlong,
+                                ctypes.c_longlong, _dp, _i64p, ctypes.c_int]
+        L.oracle_pe.restype = ctypes.c_int
+        L.oracle_scatter.argtypes = [_fp, _fp, _fp, _fp, _fp, _u32p, ctypes.c_int, ctypes.c_int, _ip,
+                                     ctypes.c_int, ctypes.c_longlong, ctypes.c_longlong, _dp,
+                                     ctypes.c_int]
+        L.oracle_scatter.restype = ctypes.c_int
+        L.oracle_bitmap_crystal_words.argtypes = [_fp]
+        L.oracle_bitmap_crystal_words.restype = ctypes.c_longlong
+        L.oracle_bitmap_collimator_words.argtypes = [_fp, _fp]
+        L.oracle_bitmap_collimator_words.restype = ctypes.c_longlong
+        L.oracle_bitmap_crystal.argtypes = [_fp, _u32p, ctypes.c_int]
+        L.oracle_bitmap_collimator.argtypes = [_fp, _fp, _u32p, ctypes.c_int]
+        for name in ("oracle_box_chord", "oracle_box_chord_inside", "oracle_cyl_chord"):
+            getattr(L, name).argtypes = [ctypes.c_int, _dp]
+            getattr(L, name).restype = ctypes.c_double
+        L.oracle_kn_sum.argtypes = [ctypes.c_int, ctypes.c_double, ctypes.c_double, ctypes.c_double]
+        L.oracle_kn_sum.restype = ctypes.c_double
+        _lib = L
+    return _lib
+
+
+def _f32(a):
+    a = np.ascontiguousarray(a, dtype=np.float32)
+    return a, a.ctypes.data_as(_fp)
+
+
+def _dets(geo, dets):
+    if dets is None:
+        dets = np.arange(geo.n_det)
+    d = np.ascontiguousarray(np.asarray(dets, dtype=np.int32))
+    return d, d.ctypes.data_as(_ip)
+
+
+def pe(geo, prec=64, dets=None, v0=0, nv=None, threads=0, counts=False):
+    """PE elements (len(dets), nv) as float64; with counts=True also the per-element work
+    counts (subelements, hole hits, crystal hits, candidate crystals, candidate holes)."""
+    nv = geo.n_vox - v0 if nv is None else nv
+    c, pc = _f32(geo.collimator)
+    d, pd = _f32(geo.detector)
+    i, pi = _f32(geo.image)
+    dd, pdd = _dets(geo, dets)
+    out = np.zeros((dd.size, nv), dtype=np.float64)
+    cnt = np.zeros((dd.size, nv, 5), dtype=np.int64) if counts else None
+    rc = lib().oracle_pe(pc, pd, pi, prec, pdd, dd.size, v0, nv, out.ctypes.data_as(_dp),
+                         cnt.ctypes.data_as(_i64p) if counts else None, threads)
+    if rc:
+        raise RuntimeError(f"oracle_pe failed ({rc})")
+    return (out, cnt) if counts else out
+
+
+def bitmap_crystal(geo, threads=0):
+    d, pd = _f32(geo.detector)
+    n = lib().oracle_bitmap_crystal_words(pd)
+    out = np.zeros(n, dtype=np.uint32)
+    lib().oracle_bitmap_crystal(pd, out.ctypes.data_as(_u32p), threads)
+    return out
+
+
+def bitmap_collimator(geo, threads=0):
+    c, pc = _f32(geo.collimator)
+    d, pd = _f32(geo.detector)
+    n = lib().oracle_bitmap_collimator_words(pc, pd)
+    out = np.zeros(n, dtype=np.uint32)
+    lib().oracle_bitmap_collimator(pc, pd, out.ctypes.data_as(_u32p), threads)
+    return out
+
+
+PART = {"crystal": 1, "collimator": 2, "collimator_variant": 3}
+
+
+def scatter(geo, pe_matrix, part, bitmap, prec=64, dets=None, v0=0, nv=None, threads=0):
+    """Scatter elements for part 'crystal', 'collimator' (combined program) or
+    'collimator_variant' (collimator-only program); float64 (len(dets), nv)."""
+    nv = geo.n_vox - v0 if nv is None else nv
+    c, pc = _f32(geo.collimator)
+    d, pd = _f32(geo.detector)
+    i, pi = _f32(geo.image)
+    p, pp = _f32(geo.physics)
+    m, pm = _f32(np.asarray(pe_matrix, dtype=np.float32).reshape(-1))
+    b = np.ascontiguousarray(bitmap, dtype=np.uint32)
+    dd, pdd = _dets(geo, dets)
+    out = np.zeros((dd.size, nv), dtype=np.float64)
+    rc = lib().oracle_scatter(pc, pd, pi, pp, pm, b.ctypes.data_as(_u32p), PART[part], prec, pdd,
+                              dd.size, v0, nv, out.ctypes.data_as(_dp), threads)
+    if rc:
+        raise RuntimeError(f"oracle_scatter failed ({rc})")
+    return out
+
+
+def box_chord(args, prec=64):
+    a = np.ascontiguousarray(args, dtype=np.float64)
+    return lib().oracle_box_chord(prec, a.ctypes.data_as(_dp))
+
+
+def box_chord_inside(args, prec=64):
+    a = np.ascontiguousarray(args, dtype=np.float64)
+    return lib().oracle_box_chord_inside(prec, a.ctypes.data_as(_dp))
+
+
+def cyl_chord(args, prec=64):
+    a = np.ascontiguousarray(args, dtype=np.float64)
+    return lib().oracle_cyl_chord(prec, a.ctypes.data_as(_dp))
+
+
+def kn_sum(e0, lo, hi, prec=64):
+    return lib().oracle_kn_sum(prec, e0, lo, hi)
