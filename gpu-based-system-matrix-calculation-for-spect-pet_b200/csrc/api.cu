@@ -43,13 +43,17 @@ struct sysmat_ctx {
     float* d_phys = nullptr;
     std::vector<float> h_phys;
     std::vector<float> h_img;
+    float h_col15 = 0.0f, h_col17 = 0.0f;   // layer-0 mu_total and mu_compton (scatter.cu:1716)
     // derived tables
     float4* d_tables = nullptr;
     // launch bookkeeping
     unsigned long long* d_counter = nullptr;
     int* d_status = nullptr;
-    // scatter pair tables (built lazily from bitmaps)
+    // scatter pair tables (sysmat_scatter_prepare)
     ScatterScratch scratch{};
+    int prepared_parts = 0;
+    PairRec* pairs = nullptr;
+    AttEntry* att = nullptr;
 };
 
 namespace {
@@ -166,6 +170,7 @@ extern "C" SYSMAT_API int sysmat_create(sysmat_ctx** out, int device, const floa
     ctx->g = g;
     ctx->n_holes0_host = nh0;
     ctx->h_img.assign(pI, pI + kNImage);
+    if (pC) { ctx->h_col15 = pC[15]; ctx->h_col17 = pC[17]; }
     if (pP) ctx->h_phys.assign(pP, pP + kNPhysics);
     cudaDeviceProp prop;
     if (cudaGetDeviceProperties(&prop, device) != cudaSuccess) { delete ctx; return SYSMAT_ERR_CUDA; }
@@ -190,6 +195,7 @@ extern "C" SYSMAT_API int sysmat_create(sysmat_ctx** out, int device, const floa
     if (!ok) { sysmat_destroy(ctx); return SYSMAT_ERR_CUDA; }
 
     float4* t = ctx->d_tables;
+    ctx->g.raw_det = ctx->d_det;
     ctx->g.cry.pos = t;
     ctx->g.cry.size = t + D;
     ctx->g.cry.mu = t + 2 * D;
@@ -268,12 +274,127 @@ extern "C" SYSMAT_API int sysmat_pe(sysmat_ctx* ctx, float rotation, int det_beg
     L.out = d_out;
     L.work_counter = ctx->d_counter;
     L.status = ctx->d_status;
+    L.counters = nullptr;
     if (launch_pe(ctx->g, L, mode, ctx->num_sms, s)) return SYSMAT_ERR_CUDA;
     int status = 0;
     CUDA_TRY(cudaMemcpyAsync(&status, ctx->d_status, sizeof(int), cudaMemcpyDeviceToHost, s));
     CUDA_TRY(cudaStreamSynchronize(s));
     if (status & kStatusCapacity) return SYSMAT_ERR_CAPACITY;
     return SYSMAT_OK;
+}
+
+extern "C" SYSMAT_API long long sysmat_bitmap_crystal_words(const sysmat_ctx* ctx)
+{
+    return ctx ? bitmap_crystal_words(ctx->g.n_det) : SYSMAT_ERR_ARG;
+}
+
+extern "C" SYSMAT_API long long sysmat_bitmap_collimator_words(const sysmat_ctx* ctx)
+{
+    return ctx ? bitmap_collimator_words(ctx->g.n_det, ctx->g.n_holes0) : SYSMAT_ERR_ARG;
+}
+
+extern "C" SYSMAT_API int sysmat_bitmap_crystal(sysmat_ctx* ctx, uint32_t* d_words, void* stream)
+{
+    if (!ctx || !d_words || !same_device(ctx)) return SYSMAT_ERR_ARG;
+    return launch_bitmap_crystal(ctx->g, d_words, (cudaStream_t)stream) ? SYSMAT_ERR_CUDA : SYSMAT_OK;
+}
+
+extern "C" SYSMAT_API int sysmat_bitmap_collimator(sysmat_ctx* ctx, uint32_t* d_words, void* stream)
+{
+    if (!ctx || !d_words || !same_device(ctx)) return SYSMAT_ERR_ARG;
+    return launch_bitmap_collimator(ctx->g, d_words, (cudaStream_t)stream) ? SYSMAT_ERR_CUDA : SYSMAT_OK;
+}
+
+extern "C" SYSMAT_API int sysmat_scatter_prepare(sysmat_ctx* ctx, int parts, const uint32_t* d_bm_crystal,
+                                                 const uint32_t* d_bm_collimator, void* stream)
+{
+    if (!ctx || !same_device(ctx)) return SYSMAT_ERR_ARG;
+    if (parts < 1 || parts > 3) return SYSMAT_ERR_ARG;
+    if ((parts & SYSMAT_SCATTER_CRYSTAL) && !d_bm_crystal) return SYSMAT_ERR_ARG;
+    if ((parts & SYSMAT_SCATTER_COLLIMATOR) && (!d_bm_collimator || ctx->g.n_holes0 < 1))
+        return SYSMAT_ERR_ARG;
+    ctx->prepared_parts = 0;
+    const int rc = build_scatter_pairs(ctx->g, parts, d_bm_crystal, d_bm_collimator, ctx->scratch,
+                                       &ctx->pairs, &ctx->att, (cudaStream_t)stream);
+    if (rc == -2) return SYSMAT_ERR_NOMEM;
+    if (rc) return SYSMAT_ERR_CUDA;
+    ctx->prepared_parts = parts;
+    return SYSMAT_OK;
+}
+
+extern "C" SYSMAT_API int sysmat_scatter(sysmat_ctx* ctx, int parts, int hole_model, float rotation,
+                                         const float* d_pe, int det_begin, int det_count,
+                                         long long vox_begin, long long vox_count, float* d_out,
+                                         long long ld, void* stream)
+{
+    int rc = check_block(ctx, det_begin, det_count, vox_begin, vox_count, d_out, ld);
+    if (rc) return rc;
+    if (parts < 1 || parts > 3 || (parts & ~ctx->prepared_parts)) return SYSMAT_ERR_ARG;
+    if (hole_model != SYSMAT_HOLE_MODEL_COMBINED && hole_model != SYSMAT_HOLE_MODEL_VARIANT)
+        return SYSMAT_ERR_ARG;
+    if ((parts & SYSMAT_SCATTER_CRYSTAL) && !d_pe) return SYSMAT_ERR_ARG;
+    if (ctx->h_phys.size() != (size_t)kNPhysics) return SYSMAT_ERR_ARG;
+    const float* P = ctx->h_phys.data();
+    ScatterPhysics ph;
+    ph.use_compton = (int)std::floor(P[0] + 0.5f) == 1;          // scatter.cu:1144
+    ph.same_window = (int)std::floor(P[4] + 0.5f) > 0;           // :1145, :1154
+    ph.lo = P[5];
+    ph.hi = P[6];
+    ph.e0 = P[7];
+    ph.integ = (float)kn_normalisation((double)P[7]);
+    ph.col_mu_tot0 = 0.0f;
+    ph.col_mu_c0 = 0.0f;
+    if (ctx->g.n_layers > 0) {
+        ph.col_mu_tot0 = ctx->h_col15;
+        ph.col_mu_c0 = ctx->h_col17;
+    }
+    ScatterLaunch L;
+    L.parts = parts;
+    L.hole_model = hole_model;
+    L.det_begin = det_begin;
+    L.det_count = det_count;
+    L.vox_begin = vox_begin;
+    L.vox_count = vox_count;
+    L.ld = ld;
+    L.rotation = rotation;
+    L.pe = d_pe;
+    L.pairs = ctx->pairs;
+    L.att = ctx->att;
+    L.out = d_out;
+    return launch_scatter(ctx->g, ph, L, (cudaStream_t)stream) ? SYSMAT_ERR_CUDA : SYSMAT_OK;
+}
+
+extern "C" SYSMAT_API int sysmat_pe_work(sysmat_ctx* ctx, float rotation, int det_begin, int det_count,
+                                         long long vox_begin, long long vox_count, float* d_out,
+                                         long long ld, unsigned long long* counts, void* stream)
+{
+    int rc = check_block(ctx, det_begin, det_count, vox_begin, vox_count, d_out, ld);
+    if (rc) return rc;
+    if (!counts) return SYSMAT_ERR_ARG;
+    unsigned long long* d_cnt = nullptr;
+    if (cudaMalloc(&d_cnt, 8 * sizeof(unsigned long long)) != cudaSuccess) return SYSMAT_ERR_NOMEM;
+    cudaStream_t s = (cudaStream_t)stream;
+    PeLaunch L;
+    L.det_begin = det_begin;
+    L.det_count = det_count;
+    L.vox_begin = vox_begin;
+    L.vox_count = vox_count;
+    L.ld = ld;
+    L.rotation = rotation;
+    L.out = d_out;
+    L.work_counter = ctx->d_counter;
+    L.status = ctx->d_status;
+    L.counters = d_cnt;
+    rc = SYSMAT_OK;
+    if (cudaMemsetAsync(d_cnt, 0, 8 * sizeof(unsigned long long), s) != cudaSuccess ||
+        cudaMemsetAsync(ctx->d_counter, 0, sizeof(unsigned long long), s) != cudaSuccess ||
+        cudaMemsetAsync(ctx->d_status, 0, sizeof(int), s) != cudaSuccess ||
+        launch_pe(ctx->g, L, SYSMAT_MODE_REFERENCE, ctx->num_sms, s) ||
+        cudaMemcpyAsync(counts, d_cnt, 6 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, s) != cudaSuccess ||
+        cudaStreamSynchronize(s) != cudaSuccess)
+        rc = SYSMAT_ERR_CUDA;
+    cudaFree(d_cnt);
+    return rc;
 }
 
 // ------------------------------------------------------------------------------------
@@ -288,12 +409,28 @@ uint64_t fnv1a(uint64_t h, const void* p, size_t n)
     return h;
 }
 
+struct DevBuf {
+    void* p = nullptr;
+    size_t cap = 0;
+    int ensure(size_t bytes)
+    {
+        if (cap >= bytes && p) return SYSMAT_OK;
+        cudaFree(p);
+        p = nullptr;
+        cap = 0;
+        if (cudaMalloc(&p, bytes ? bytes : 4) != cudaSuccess) { p = nullptr; return SYSMAT_ERR_NOMEM; }
+        cap = bytes;
+        return SYSMAT_OK;
+    }
+};
+
 struct LegacySlot {
     std::mutex mu;
     uint64_t key = 0;
     sysmat_ctx* ctx = nullptr;
     float* d_out = nullptr;
     size_t out_cap = 0;
+    DevBuf pe, bm_crystal, bm_collimator;
 };
 
 LegacySlot& slot_for(int device)
@@ -368,4 +505,155 @@ extern "C" SYSMAT_API int PESysMatGen(float* parameter_Collimator, float* parame
     if (rc) return rc;
     CUDA_TRY(cudaMemcpy(dst, slot.d_out, sizeof(float) * (size_t)D * (size_t)V, cudaMemcpyDeviceToHost));
     return (int)V;
+}
+
+namespace {
+
+// Write a device bitmap to a file the way the reference does (fopen "wb+", raw uint32).
+int bitmap_to_file(const char* fname, const uint32_t* d_words, long long n)
+{
+    if (!fname) return SYSMAT_ERR_ARG;
+    std::vector<uint32_t> h((size_t)n);
+    if (cudaMemcpy(h.data(), d_words, sizeof(uint32_t) * (size_t)n, cudaMemcpyDeviceToHost) != cudaSuccess)
+        return SYSMAT_ERR_CUDA;
+    FILE* f = std::fopen(fname, "wb+");
+    if (!f) return SYSMAT_ERR_IO;
+    const size_t w = std::fwrite(h.data(), sizeof(uint32_t), (size_t)n, f);
+    std::fclose(f);
+    return w == (size_t)n ? SYSMAT_OK : SYSMAT_ERR_IO;
+}
+
+// Read a bitmap file into device memory.  Like the reference (zero-initialised buffer and an
+// unchecked fread, scatter.cu:2156-2159), a short file leaves the remaining words zero.
+int bitmap_from_file(const char* fname, uint32_t* d_words, long long n)
+{
+    if (!fname) return SYSMAT_ERR_ARG;
+    FILE* f = std::fopen(fname, "rb");
+    if (!f) return SYSMAT_ERR_IO;
+    std::vector<uint32_t> h((size_t)n, 0u);
+    const size_t r = std::fread(h.data(), sizeof(uint32_t), (size_t)n, f);
+    std::fclose(f);
+    if (r != (size_t)n)
+        std::fprintf(stderr, "sysmat: %s holds %zu of %lld bitmap words; the rest read as 0\n", fname, r, n);
+    if (cudaMemcpy(d_words, h.data(), sizeof(uint32_t) * (size_t)n, cudaMemcpyHostToDevice) != cudaSuccess)
+        return SYSMAT_ERR_CUDA;
+    return SYSMAT_OK;
+}
+
+// Compute (flag set) or load a relationship bitmap for the reference-compatible scatter
+// programs (scatter.cu:2116-2167, :2246-2301).
+int legacy_bitmap(sysmat_ctx* ctx, bool crystal, bool compute, const char* fname, DevBuf& buf)
+{
+    const long long n = crystal ? sysmat_bitmap_crystal_words(ctx) : sysmat_bitmap_collimator_words(ctx);
+    if (n < 0) return (int)n;
+    int rc = buf.ensure(sizeof(uint32_t) * (size_t)(n > 0 ? n : 1));
+    if (rc) return rc;
+    uint32_t* words = (uint32_t*)buf.p;
+    if (compute) {
+        rc = crystal ? sysmat_bitmap_crystal(ctx, words, nullptr) : sysmat_bitmap_collimator(ctx, words, nullptr);
+        if (rc) return rc;
+        return bitmap_to_file(fname, words, n);
+    }
+    return bitmap_from_file(fname, words, n);
+}
+
+int legacy_scatter(int cuda_id, float* pC, float* pD, float* pI, float* pP, float* pe,
+                   const char* f_crystal, const char* f_collimator, float* dst, int parts,
+                   int hole_model, bool comp_crystal, bool comp_collimator)
+{
+    if (!pD || !pI || !pP || !dst) return SYSMAT_ERR_ARG;
+    if ((parts & SYSMAT_SCATTER_COLLIMATOR) && !pC) return SYSMAT_ERR_ARG;
+    if ((parts & SYSMAT_SCATTER_CRYSTAL) && !pe) return SYSMAT_ERR_ARG;
+    const int dev = select_device(cuda_id);
+    if (dev < 0) return dev;
+    LegacySlot& slot = slot_for(dev);
+    std::lock_guard<std::mutex> lock(slot.mu);
+    int rc = legacy_ctx(dev, (parts & SYSMAT_SCATTER_COLLIMATOR) ? pC : nullptr, pD, pI, pP, slot);
+    if (rc) return rc;
+    sysmat_ctx* ctx = slot.ctx;
+    const int D = ctx->g.n_det;
+    const long long V = ctx->g.nvox;
+    const size_t nel = (size_t)D * (size_t)V;
+    if (parts & SYSMAT_SCATTER_CRYSTAL) {
+        rc = legacy_bitmap(ctx, true, comp_crystal, f_crystal, slot.bm_crystal);
+        if (rc) return rc;
+        rc = slot.pe.ensure(sizeof(float) * nel);
+        if (rc) return rc;
+        CUDA_TRY(cudaMemcpy(slot.pe.p, pe, sizeof(float) * nel, cudaMemcpyHostToDevice));
+    }
+    if (parts & SYSMAT_SCATTER_COLLIMATOR) {
+        rc = legacy_bitmap(ctx, false, comp_collimator, f_collimator, slot.bm_collimator);
+        if (rc) return rc;
+    }
+    rc = legacy_out(slot, nel);
+    if (rc) return rc;
+    rc = sysmat_scatter_prepare(ctx, parts, (const uint32_t*)slot.bm_crystal.p,
+                                (const uint32_t*)slot.bm_collimator.p, nullptr);
+    if (rc) return rc;
+    rc = sysmat_scatter(ctx, parts, hole_model, pI[20], (const float*)slot.pe.p, 0, D, 0, V, slot.d_out,
+                        V, nullptr);
+    if (rc) return rc;
+    CUDA_TRY(cudaMemcpy(dst, slot.d_out, sizeof(float) * nel, cudaMemcpyDeviceToHost));
+    return (int)V;
+}
+
+}  // namespace
+
+extern "C" SYSMAT_API int scatter(float* parameter_Collimator, float* parameter_Detector,
+                                  float* parameter_Image, float* parameter_Physics, float* PE_SysMat,
+                                  const char* FnameGeoCrystal, const char* FnameGeoCollimator,
+                                  float* dst, int cuda_id)
+{
+    if (!parameter_Physics) return SYSMAT_ERR_ARG;
+    const bool cc = (int)std::floor(parameter_Physics[8]) == 1;                 // scatter.cu:2116
+    const bool ch = (int)std::floor(parameter_Physics[9] + 0.001f) == 1;        // scatter.cu:2246
+    return legacy_scatter(cuda_id, parameter_Collimator, parameter_Detector, parameter_Image,
+                          parameter_Physics, PE_SysMat, FnameGeoCrystal, FnameGeoCollimator, dst,
+                          SYSMAT_SCATTER_CRYSTAL | SYSMAT_SCATTER_COLLIMATOR,
+                          SYSMAT_HOLE_MODEL_COMBINED, cc, ch);
+}
+
+extern "C" SYSMAT_API int scatter_collimator(float* parameter_Collimator, float* parameter_Detector,
+                                             float* parameter_Image, float* parameter_Physics,
+                                             float* PE_SysMat, const char* FnameGeo, float* dst,
+                                             int cuda_id)
+{
+    if (!parameter_Physics) return SYSMAT_ERR_ARG;
+    const bool ch = (int)std::floor(parameter_Physics[9]) == 1;   // ScatterGen_Collimator/scatter.cu:1617
+    (void)PE_SysMat;   // the collimator part does not read the PE matrix
+    return legacy_scatter(cuda_id, parameter_Collimator, parameter_Detector, parameter_Image,
+                          parameter_Physics, nullptr, nullptr, FnameGeo, dst, SYSMAT_SCATTER_COLLIMATOR,
+                          SYSMAT_HOLE_MODEL_VARIANT, false, ch);
+}
+
+extern "C" SYSMAT_API int scatter_crystal(float* parameter_Detector, float* parameter_Image,
+                                          float* parameter_Physics, float* PE_SysMat, const char* FnameGeo,
+                                          float* dst, int cuda_id)
+{
+    if (!parameter_Physics) return SYSMAT_ERR_ARG;
+    const bool cc = (int)std::floor(parameter_Physics[8]) == 1;   // ScatterGen_Crystal/scatter.cu:1626
+    return legacy_scatter(cuda_id, nullptr, parameter_Detector, parameter_Image, parameter_Physics,
+                          PE_SysMat, FnameGeo, nullptr, dst, SYSMAT_SCATTER_CRYSTAL,
+                          SYSMAT_HOLE_MODEL_COMBINED, cc, false);
+}
+
+// Internal C names used by the C++-linkage aliases in cxx_abi.cpp (not in sysmat.h).
+extern "C" int sysmat_legacy_pe(float* pC, float* pD, float* pI, float* dst, int cuda_id)
+{
+    return PESysMatGen(pC, pD, pI, dst, cuda_id);
+}
+extern "C" int sysmat_legacy_scatter(float* pC, float* pD, float* pI, float* pP, float* pe,
+                                     const char* fc, const char* fh, float* dst, int cuda_id)
+{
+    return scatter(pC, pD, pI, pP, pe, fc, fh, dst, cuda_id);
+}
+extern "C" int sysmat_legacy_scatter_collimator(float* pC, float* pD, float* pI, float* pP, float* pe,
+                                                const char* fh, float* dst, int cuda_id)
+{
+    return scatter_collimator(pC, pD, pI, pP, pe, fh, dst, cuda_id);
+}
+extern "C" int sysmat_legacy_scatter_crystal(float* pD, float* pI, float* pP, float* pe, const char* fc,
+                                             float* dst, int cuda_id)
+{
+    return scatter_crystal(pD, pI, pP, pe, fc, dst, cuda_id);
 }

@@ -59,6 +59,7 @@ struct DevGeom {
     float fov;           // FOV-to-collimator distance, Params_Image[11]
     float angle_step;    // Params_Image[7]
     int nonneg_mu;       // all attenuation coefficients >= 0 (enables the blocked-ray early exit)
+    const float* raw_det;   // Params_Detector as uploaded (bitmaps use raw, un-offset values)
     CrystalTables cry;
     HoleTables hole;
     LayerInfo layer[kMaxLayers];

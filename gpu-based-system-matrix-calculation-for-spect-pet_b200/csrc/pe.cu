@@ -37,7 +37,7 @@ namespace {
 constexpr int kWarps = 8;
 constexpr int kThreads = kWarps * 32;
 constexpr int kSuperCap = 1024;         // block superset capacity (objects)
-constexpr int kChunk = 128;             // per-warp kept-object chunk
+constexpr int kChunk = 256;             // per-warp kept-object chunk
 constexpr int kBx = 4, kBy = 4, kBz = 2;
 constexpr float kSlopeMargin = 2e-4f;   // slope units; >> FP32 position error / depth
 constexpr float kMinDepth = 1.0f;       // mm; slope rectangles need objects this far behind
@@ -45,6 +45,7 @@ constexpr float kMinDepth = 1.0f;       // mm; slope rectangles need objects thi
 struct WarpSmem {
     float4 rect[kChunk];
     int id[kChunk];                      // holes: hole index; crystals: n_holes + crystal
+    unsigned short sub[kChunk];          // chunk entries overlapping the current round's rays
     float4 inner[kMaxLayers];            // plate "through both faces" slope rectangle
     float chain[32];
 };
@@ -215,6 +216,8 @@ struct Walk {
     float att;      // accumulated mu * L
     float len;      // hole chord sum of the current layer
     int lay;        // current layer
+    int hole_hits;  // non-zero hole chords (work counters only)
+    int cry_hits;   // non-zero crystal chords (work counters only)
 };
 
 __device__ __forceinline__ void close_layers(const DevGeom& g, Walk& s, int upto, float cosang)
@@ -227,12 +230,29 @@ __device__ __forceinline__ void close_layers(const DevGeom& g, Walk& s, int upto
     }
 }
 
-// Walk one chunk of kept objects for one sub-element ray (voxel -> (xD, yD, zD)).
-__device__ __forceinline__ void walk_chunk(const DevGeom& g, const WarpSmem& ws, int n, const Elem& e,
+// Indices of the chunk entries whose slope rectangle overlaps the bounding box of the 32
+// rays of this round; order is preserved.  Returns the count.
+__device__ __forceinline__ int round_sublist(WarpSmem& ws, int n, float4 box, int lane)
+{
+    int nr = 0;
+    for (int base = 0; base < n; base += 32) {
+        const int k = base + lane;
+        const bool keep = k < n && rects_overlap(ws.rect[k], box);
+        const unsigned m = __ballot_sync(0xffffffffu, keep);
+        if (keep) ws.sub[nr + __popc(m & ((1u << lane) - 1u))] = (unsigned short)k;
+        nr += __popc(m);
+    }
+    __syncwarp();
+    return nr;
+}
+
+// Walk the round's sub-list of kept objects for one sub-element ray (voxel -> (xD,yD,zD)).
+__device__ __forceinline__ void walk_chunk(const DevGeom& g, const WarpSmem& ws, int nr, const Elem& e,
                                            float xD, float yD, float zD, float sa_a, float sa_b,
                                            float cosang, Walk& s)
 {
-    for (int k = 0; k < n; ++k) {
+    for (int j = 0; j < nr; ++j) {
+        const int k = ws.sub[j];
         const int id = ws.id[k];
         if (id < g.n_holes) {
             const int m = layer_of_hole(g, id);
@@ -243,6 +263,7 @@ __device__ __forceinline__ void walk_chunk(const DevGeom& g, const WarpSmem& ws,
             const float tmp = cyl_chord(e.xI, e.yI, e.zI, xD, yD, zD, ha.x, ha.y, ha.z, ha.w, hb.x);
             s.len = s.len + tmp;                                 // :1276-1278
             s.att = s.att + hb.y * tmp;
+            s.hole_hits += (tmp != 0.0f);
         } else {
             if (s.lay < g.n_layers) close_layers(g, s, g.n_layers, cosang);
             if (!in_rect(ws.rect[k], sa_a, sa_b)) continue;
@@ -257,6 +278,7 @@ __device__ __forceinline__ void walk_chunk(const DevGeom& g, const WarpSmem& ws,
             const float la = box_chord(xa, ya, za, xb, yb, zb, -0.5f * so.x, -0.5f * so.y,
                                        -0.5f * so.z, 0.5f * so.x, 0.5f * so.y, 0.5f * so.z);
             s.att = s.att + la * mo;
+            s.cry_hits += (la != 0.0f);
         }
     }
 }
@@ -341,9 +363,10 @@ __device__ __forceinline__ float finish_sub_element(const Elem& e, const SubElem
     return eff * sa * absf;
 }
 
-template <int MODE>
+template <int MODE, bool COUNT>
 __device__ float pe_element(const DevGeom& g, const BlockSmem& bs, WarpSmem& ws, int d,
-                            long long v, float cr, float sr, int lane)
+                            long long v, float cr, float sr, int lane,
+                            unsigned long long* counters)
 {
     Elem e;
     voxel_centre(g, v, cr, sr, e.xI, e.yI, e.zI);
@@ -389,20 +412,34 @@ __device__ float pe_element(const DevGeom& g, const BlockSmem& bs, WarpSmem& ws,
 
     float chain = 0.0f;
     double dacc = 0.0;
+    int n_hole_hits = 0, n_cry_hits = 0, n_blocked = 0;
     for (int r = 0; r < 32; ++r) {
         const SubElem q = sub_element(e, r * 32 + lane);
-        Walk s{0.0f, 0.0f, 0};
+        Walk s{0.0f, 0.0f, 0, 0, 0};
         const bool blocked = plate_penalty(g, ws, e, q, s.att);
         const bool skip = blocked && g.nonneg_mu;
+        // slope box of the rays that still need the walk in this round
+        float4 box = make_float4(skip ? INFINITY : q.sa_a, skip ? -INFINITY : q.sa_a,
+                                 skip ? INFINITY : q.sa_b, skip ? -INFINITY : q.sa_b);
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1) {
+            box.x = fminf(box.x, __shfl_xor_sync(0xffffffffu, box.x, off));
+            box.y = fmaxf(box.y, __shfl_xor_sync(0xffffffffu, box.y, off));
+            box.z = fminf(box.z, __shfl_xor_sync(0xffffffffu, box.z, off));
+            box.w = fmaxf(box.w, __shfl_xor_sync(0xffffffffu, box.w, off));
+        }
         if (single) {
-            if (!skip) walk_chunk(g, ws, count, e, q.xD, q.yD, q.zD, q.sa_a, q.sa_b, q.cosang, s);
+            const int nr = round_sublist(ws, count, box, lane);
+            if (!skip) walk_chunk(g, ws, nr, e, q.xD, q.yD, q.zD, q.sa_a, q.sa_b, q.cosang, s);
+            __syncwarp();
         } else {
             // chunked walk: rebuild the chunks for this round (the warp stays converged)
             int cur = 0;
             while (cur < n_src) {
                 if (r > 0 || cur > 0) cur = build_chunk(g, bs, ws, e, d, cur, n_src, from_super, lane, &count);
                 else cur = cursor;
-                if (!skip) walk_chunk(g, ws, count, e, q.xD, q.yD, q.zD, q.sa_a, q.sa_b, q.cosang, s);
+                const int nr = round_sublist(ws, count, box, lane);
+                if (!skip) walk_chunk(g, ws, nr, e, q.xD, q.yD, q.zD, q.sa_a, q.sa_b, q.cosang, s);
                 __syncwarp();
             }
         }
@@ -410,6 +447,11 @@ __device__ float pe_element(const DevGeom& g, const BlockSmem& bs, WarpSmem& ws,
         if (!skip) {
             if (s.lay < g.n_layers) close_layers(g, s, g.n_layers, q.cosang);
             contrib = finish_sub_element(e, q, s.att);
+        }
+        if constexpr (COUNT) {
+            n_hole_hits += s.hole_hits;
+            n_cry_hits += s.cry_hits;
+            n_blocked += skip;
         }
         if constexpr (MODE == 0) {
             ws.chain[lane] = contrib;
@@ -419,6 +461,21 @@ __device__ float pe_element(const DevGeom& g, const BlockSmem& bs, WarpSmem& ws,
             __syncwarp();
         } else {
             dacc += (double)contrib;
+        }
+    }
+    if constexpr (COUNT) {
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1) {
+            n_hole_hits += __shfl_xor_sync(0xffffffffu, n_hole_hits, off);
+            n_cry_hits += __shfl_xor_sync(0xffffffffu, n_cry_hits, off);
+            n_blocked += __shfl_xor_sync(0xffffffffu, n_blocked, off);
+        }
+        if (lane == 0) {
+            atomicAdd(&counters[0], 1024ull);
+            atomicAdd(&counters[1], (unsigned long long)n_hole_hits);
+            atomicAdd(&counters[2], (unsigned long long)n_cry_hits);
+            atomicAdd(&counters[3], 1ull);
+            atomicAdd(&counters[4], (unsigned long long)n_blocked);
         }
     }
     if constexpr (MODE == 0) return chain;
@@ -482,10 +539,11 @@ __device__ void build_superset(const DevGeom& g, BlockSmem& bs, int d, float cx,
     __syncthreads();
 }
 
-template <int MODE>
+template <int MODE, bool COUNT>
 __global__ void __launch_bounds__(kThreads, 2) pe_kernel(DevGeom g, PeLaunch L)
 {
-    __shared__ BlockSmem bs;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    BlockSmem& bs = *reinterpret_cast<BlockSmem*>(smem_raw);
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     WarpSmem& ws = bs.w[wid];
     const float ang = L.rotation * g.angle_step;           // :1006
@@ -525,7 +583,7 @@ __global__ void __launch_bounds__(kThreads, 2) pe_kernel(DevGeom g, PeLaunch L)
             if (ix >= g.nx || iy >= g.ny || iz > z1) continue;
             const long long v = ix + g.nx * ((long long)iy + (long long)g.ny * iz);
             if (v < L.vox_begin || v > vlast) continue;
-            const float val = pe_element<MODE>(g, bs, ws, d, v, cr, sr, lane);
+            const float val = pe_element<MODE, COUNT>(g, bs, ws, d, v, cr, sr, lane, L.counters);
             if (lane == 0) L.out[(long long)di * L.ld + (v - L.vox_begin)] = val;
             __syncwarp();
         }
@@ -535,16 +593,32 @@ __global__ void __launch_bounds__(kThreads, 2) pe_kernel(DevGeom g, PeLaunch L)
 
 }  // namespace
 
+template <int MODE, bool COUNT>
+static int launch_mode(const DevGeom& g, const PeLaunch& L, int num_sms, cudaStream_t stream)
+{
+    const int smem = (int)sizeof(BlockSmem);
+    static unsigned long long configured = 0;   // one bit per device
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return -1;
+    const unsigned long long bit = 1ull << (dev & 63);
+    if (!(__atomic_load_n(&configured, __ATOMIC_ACQUIRE) & bit)) {
+        if (cudaFuncSetAttribute(pe_kernel<MODE, COUNT>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem) !=
+            cudaSuccess)
+            return -1;
+        __atomic_fetch_or(&configured, bit, __ATOMIC_RELEASE);
+    }
+    int per_sm = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, pe_kernel<MODE, COUNT>, kThreads, smem);
+    if (per_sm < 1) per_sm = 1;
+    pe_kernel<MODE, COUNT><<<num_sms * per_sm, kThreads, smem, stream>>>(g, L);
+    return cudaGetLastError() == cudaSuccess ? 0 : -1;
+}
+
 int launch_pe(const DevGeom& g, const PeLaunch& L, int mode, int num_sms, cudaStream_t stream)
 {
-    int per_sm = 0;
-    if (mode == 0) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, pe_kernel<0>, kThreads, 0);
-    else           cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, pe_kernel<1>, kThreads, 0);
-    if (per_sm < 1) per_sm = 1;
-    const int blocks = num_sms * per_sm;
-    if (mode == 0) pe_kernel<0><<<blocks, kThreads, 0, stream>>>(g, L);
-    else           pe_kernel<1><<<blocks, kThreads, 0, stream>>>(g, L);
-    return cudaGetLastError() == cudaSuccess ? 0 : -1;
+    if (L.counters) return launch_mode<0, true>(g, L, num_sms, stream);
+    return mode == 0 ? launch_mode<0, false>(g, L, num_sms, stream)
+                     : launch_mode<1, false>(g, L, num_sms, stream);
 }
 
 }  // namespace sysmat

@@ -23,6 +23,10 @@ struct PeLaunch {
     float* out;
     unsigned long long* work_counter;      // zeroed before the launch
     int* status;                           // zeroed before the launch
+    // optional work counters (nullptr in timed runs): [0] sub-elements evaluated,
+    // [1] non-zero hole chords, [2] non-zero crystal chords, [3] elements, [4] plate-blocked
+    // sub-elements, [5] cone-test candidates (holes + crystals)
+    unsigned long long* counters;
 };
 
 int launch_pe(const DevGeom& g, const PeLaunch& L, int mode, int num_sms, cudaStream_t stream);

@@ -1,0 +1,595 @@
+// Primary-Compton scatter kernels and geometry-relationship bitmaps for sm_100a.
+//
+// Physics follows the reference kernels crystalScatterSysMatCuda
+// (ScatterGen_RayTracing_CircularHole/scatter.cu:1077-1437) and collimatorScatterSysMatCuda
+// (:1544-1936; hole solid angle of the collimator-only program at
+// ScatterGen_Collimator/scatter.cu:1212-1215).  Execution plan:
+//
+//  * everything that depends only on the (scatterer s, detector d) pair is computed once
+//    per pair instead of once per (d, v, s) item: the scatter point in d's frame, the
+//    scatter-to-detector distance, the absorption chord in d, and the list of attenuating
+//    crystals flagged by the relationship bitmap with a non-zero chord (the reference scans
+//    all D crystals of the bitmap for every item, :1343-1401);
+//  * the self-attenuation term (:1404-1417) is exactly 0 with the reference's 1x1x1
+//    detector sub-division (the crystal box and the sub-element box are the same floats), so
+//    it is not evaluated;
+//  * the Klein-Nishina angular ratio is the reference's left Riemann sum with
+//    n = (int)((theta_max - theta_min) / 0.01f) + 1 terms (:980-993, :1338).  It is
+//    evaluated through the Euler-Maclaurin identity
+//      sum_{i=0..n} F(a + i h) h = int_a^b F + h/2 (F(a) + F(b)) + h^2/12 (F'(b) - F'(a)) + O(h^4)
+//    with an 8-point Gauss-Legendre integral, instead of n+1 cos/sin evaluations; theta_min,
+//    theta_max and n are computed with the reference's float formulas, so the step count
+//    matches.  The normalisation over [0, pi] is a host FP64 sum;
+//  * one thread per matrix element (d, v); a block shares d, so pair records are staged in
+//    shared memory and attenuator lists are broadcast loads; each element sums its items in
+//    FP64 (the reference adds float items with atomicAdd in an unspecified order).
+#include <cub/cub.cuh>
+
+#include "scatter.cuh"
+
+namespace sysmat {
+
+namespace {
+
+constexpr int kItemThreads = 128;
+constexpr int kPairChunk = 128;
+
+// ---- reference helper formulas (scatter.cu:961-1038) ----
+
+__device__ __forceinline__ float cone_angle(float xs, float ys, float zs, float xa, float ya, float za,
+                                            float xd, float yd, float zd)
+{
+    const float a0 = xa - xs, a1 = ya - ys, a2 = za - zs;
+    const float b0 = xd - xa, b1 = yd - ya, b2 = zd - za;
+    const float dot = b0 * a0 + b1 * a1 + b2 * a2;
+    const float ma = sqrtf(a0 * a0 + a1 * a1 + a2 * a2);
+    const float mb = sqrtf(b0 * b0 + b1 * b1 + b2 * b2);
+    float c = dot / (ma * mb);
+    if (c > 1.0f) c = 1.0f;
+    if (c < -1.0f) c = -1.0f;
+    return acosf(c);
+}
+
+__device__ __forceinline__ float dist3(float x1, float y1, float z1, float x2, float y2, float z2)
+{
+    return sqrtf((x1 - x2) * (x1 - x2) + (y1 - y2) * (y1 - y2) + (z1 - z2) * (z1 - z2));
+}
+
+// Klein-Nishina shape times sin(theta), and its derivative, in float.
+__device__ __forceinline__ float kn_f(float th, float alpha)
+{
+    float s, c;
+    sincosf(th, &s, &c);
+    const float f1 = alpha * (1.0f - c);
+    const float f2 = 1.0f + c * c;
+    const float p = 1.0f + f1;
+    return f2 / p / p * (1.0f + f1 * f1 / f2 / p) * s;
+}
+
+__device__ __forceinline__ float kn_fprime(float th, float alpha)
+{
+    float s, c;
+    sincosf(th, &s, &c);
+    const float om = 1.0f - c;
+    const float p = 1.0f + alpha * om;
+    const float ip = 1.0f / p;
+    const float ip2 = ip * ip, ip3 = ip2 * ip, ip4 = ip3 * ip;
+    const float g = (1.0f + c * c) * ip2 + alpha * alpha * om * om * ip3;
+    const float gp = 2.0f * c * ip2 + 2.0f * alpha * (1.0f + c * c) * ip3 -
+                     2.0f * alpha * alpha * om * ip3 + 3.0f * alpha * alpha * alpha * om * om * ip4;
+    return c * g - s * s * gp;
+}
+
+// Reference Riemann sum with n + 1 terms starting at a, step 0.01f, via Euler-Maclaurin.
+// The integral uses 8-point Gauss-Legendre panels no wider than 0.8 rad (relative error
+// below 1e-12 in exact arithmetic; the float evaluation error, ~1e-7, dominates).
+__device__ float kn_sum(float a, int n, float alpha)
+{
+    const float h = 0.01f;
+    const float b = a + (float)n * h;
+    const float fa = kn_f(a, alpha), fb = kn_f(b, alpha);
+    float integral = 0.0f;
+    if (n > 0) {
+        const float xg[4] = {0.1834346424956498f, 0.5255324099163290f, 0.7966664774136267f,
+                             0.9602898564975363f};
+        const float wg[4] = {0.3626837833783620f, 0.3137066458778873f, 0.2223810344533745f,
+                             0.1012285362903763f};
+        const int panels = (int)ceilf((b - a) * 1.25f);
+        const float width = (b - a) / (float)panels;
+        for (int p = 0; p < panels; ++p) {
+            const float lo = a + (float)p * width;
+            const float half = 0.5f * width, mid = lo + half;
+            float acc = 0.0f;
+#pragma unroll
+            for (int k = 0; k < 4; ++k)
+                acc += wg[k] * (kn_f(mid - half * xg[k], alpha) + kn_f(mid + half * xg[k], alpha));
+            integral += half * acc;
+        }
+    }
+    return integral + 0.5f * h * (fa + fb) + (h * h / 12.0f) * (kn_fprime(b, alpha) - kn_fprime(a, alpha));
+}
+
+__device__ __forceinline__ float window_prob(float e, float res, float lo, float hi)
+{
+    const float sigma = res / 2.35482f * e;
+    const float s2 = (float)((double)sigma * 1.4142135623730951);   // sigma * sqrt(2.0)
+    const float z1 = (lo - e) / s2;
+    const float z2 = (hi - e) / s2;
+    return 0.5f * (erff(z2) - erff(z1));
+}
+
+// Crystal d's single sub-element centre (1x1x1 division, :1242-1252) in its own frame and
+// in world coordinates.
+struct DetPoint {
+    float xDs, yDs, zDs, xD, yD, zD;
+};
+
+__device__ __forceinline__ DetPoint det_point(float4 P, float4 S, float4 T)
+{
+    DetPoint q;
+    const float w = S.x, t = S.y, h = S.z;
+    q.xDs = -w / 2.0f + ((float)0 + 0.5f) / 1.0f * w;
+    q.zDs = -h / 2.0f + ((float)0 + 0.5f) / 1.0f * h;
+    q.yDs = -t / 2.0f + ((float)0 + 0.5f) / 1.0f * t;
+    q.xD = P.x + (q.xDs * T.x - q.zDs * T.y);
+    q.zD = P.z + (q.xDs * T.y + q.zDs * T.x);
+    q.yD = P.y + q.yDs;
+    return q;
+}
+
+// ---- relationship bitmaps, one thread per 32-bit word (no atomics) ----
+
+__global__ void bitmap_crystal_kernel(const float* __restrict__ det, int n, long long words,
+                                      uint32_t* __restrict__ out)
+{
+    const long long w = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (w >= words) return;
+    const long long total_pairs = (long long)n * (n + 1) / 2;
+    long long bit = w * 32;
+    long long pair = bit / n;
+    int a = (int)(bit - pair * n);
+    // row i of pair index p = i*n - i(i+1)/2 + j (i <= j)
+    double disc = (2.0 * n + 1.0) * (2.0 * n + 1.0) - 8.0 * (double)pair;
+    long long i = (long long)floor(((2.0 * n + 1.0) - sqrt(disc > 0 ? disc : 0)) / 2.0);
+    if (i < 0) i = 0;
+    while (i > 0 && i * n - i * (i - 1) / 2 > pair) --i;
+    while ((i + 1) * n - (i + 1) * i / 2 <= pair) ++i;
+    long long j = pair - (i * n - i * (i + 1) / 2);
+    uint32_t word = 0;
+    for (int b = 0; b < 32; ++b) {
+        if (pair >= total_pairs) break;
+        const int ii = (int)i, jj = (int)j, k = a;
+        if (ii < jj && k != ii && k != jj) {
+            // scatter.cu:1465-1534
+            const float* pi = det + 12 * ii;
+            const float* pj = det + 12 * jj;
+            const float* pk = det + 12 * k;
+            const float ri = sqrtf(pi[4] * pi[4] + pi[6] * pi[6] + pi[5] * pi[5]) / 2.0f;
+            const float rj = sqrtf(pj[4] * pj[4] + pj[6] * pj[6] + pj[5] * pj[5]) / 2.0f;
+            const float lij = dist3(pi[1], pi[2], pi[3], pj[1], pj[2], pj[3]);
+            const float cij = ri / lij, cji = rj / lij;
+            const float rk = sqrtf(pk[4] * pk[4] + pk[6] * pk[6] + pk[5] * pk[5]) / 2.0f;
+            const float lik = dist3(pk[1], pk[2], pk[3], pi[1], pi[2], pi[3]);
+            const float cki = rk / lik;
+            const float ljk = dist3(pk[1], pk[2], pk[3], pj[1], pj[2], pj[3]);
+            const float ckj = rk / ljk;
+            const float d_i = dist3((pk[1] - pi[1]) / lik, (pk[2] - pi[2]) / lik, (pk[3] - pi[3]) / lik,
+                                    (pj[1] - pi[1]) / lij, (pj[2] - pi[2]) / lij, (pj[3] - pi[3]) / lij);
+            bool hit = d_i <= cki + cji;
+            if (!hit) {
+                const float d_j = dist3((pk[1] - pj[1]) / ljk, (pk[2] - pj[2]) / ljk, (pk[3] - pj[3]) / ljk,
+                                        (pi[1] - pj[1]) / lij, (pi[2] - pj[2]) / lij, (pi[3] - pj[3]) / lij);
+                hit = d_j <= ckj + cij;
+            }
+            if (hit) word |= 1u << b;
+        }
+        if (++a == n) {
+            a = 0;
+            ++pair;
+            if (++j == n) { ++i; j = i; }
+        }
+    }
+    out[w] = word;
+}
+
+__global__ void bitmap_collimator_kernel(const float* __restrict__ det, const float4* __restrict__ hraw,
+                                         int n, int nh, long long words, uint32_t* __restrict__ out)
+{
+    const long long w = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (w >= words) return;
+    const long long total = (long long)nh * n * n;
+    long long bit = w * 32;
+    uint32_t word = 0;
+    for (int b = 0; b < 32 && bit < total; ++b, ++bit) {
+        const int k = (int)(bit % n);
+        const long long ij = bit / n;
+        const int j = (int)(ij % n);
+        const int i = (int)(ij / n);
+        // scatter.cu:1963-2006 (raw y, no FOV offset)
+        const float4 hr = __ldg(&hraw[i]);
+        const float xi = hr.x, yi = (hr.y + hr.z) / 2.0f, zi = hr.w;
+        const float* pj = det + 12 * j;
+        const float* pk = det + 12 * k;
+        const float rj = sqrtf(pj[4] * pj[4] + pj[6] * pj[6] + pj[5] * pj[5]) / 2.0f;
+        const float lij = dist3(xi, yi, zi, pj[1], pj[2], pj[3]);
+        const float cji = rj / lij;
+        const float rk = sqrtf(pk[4] * pk[4] + pk[6] * pk[6] + pk[5] * pk[5]) / 2.0f;
+        const float lik = dist3(pk[1], pk[2], pk[3], xi, yi, zi);
+        const float cki = rk / lik;
+        const float dd = dist3((pk[1] - xi) / lik, (pk[2] - yi) / lik, (pk[3] - zi) / lik,
+                               (pj[1] - xi) / lij, (pj[2] - yi) / lij, (pj[3] - zi) / lij);
+        if (dd <= cki + cji) word |= 1u << b;
+    }
+    out[w] = word;
+}
+
+// ---- pair tables ----
+
+__device__ __forceinline__ bool test_bit(const uint32_t* bm, long long bit)
+{
+    return (__ldg(&bm[bit >> 5]) >> (bit & 31)) & 1u;
+}
+
+// Scatter point of scatterer s: crystal centre (y + FOV) or hole centre
+// ((y1 + y2) / 2 + FOV), scatter.cu:1221-1223, :1707-1709.
+__device__ __forceinline__ void scatter_point(const DevGeom& g, int s, float& xs, float& ys, float& zs)
+{
+    if (s < g.n_det) {
+        const float4 p = __ldg(&g.cry.pos[s]);
+        xs = p.x; ys = p.y; zs = p.z;
+    } else {
+        const float4 r = __ldg(&g.hole.raw[s - g.n_det]);
+        xs = r.x;
+        ys = (r.y + r.z) / 2.0f + g.fov;
+        zs = r.w;
+    }
+}
+
+// Visit the attenuators of pair (s, d) with non-zero chords, in ascending crystal order.
+template <typename F>
+__device__ void for_each_attenuator(const DevGeom& g, const uint32_t* bm_cry, const uint32_t* bm_col,
+                                    int s, int d, float xs, float ys, float zs, const DetPoint& q, F&& f)
+{
+    const int n = g.n_det;
+    long long base;
+    if (s < n) {
+        const long long i = s < d ? s : d, j = s < d ? d : s;
+        base = (i * n - (i * (i + 1)) / 2 + j) * n;
+    } else {
+        base = ((long long)(s - n) * n + d) * n;
+    }
+    const uint32_t* bm = s < n ? bm_cry : bm_col;
+    for (int a = 0; a < n; ++a) {
+        if (a == d || (s < n && a == s)) continue;
+        if (!test_bit(bm, base + a)) continue;
+        const float4 pa = __ldg(&g.cry.pos[a]);
+        const float4 sa = __ldg(&g.cry.size[a]);
+        const float4 ta = __ldg(&g.cry.trig[a]);
+        float xa, ya, za, xb, yb, zb;                            // :1377-1394
+        to_crystal_frame(pa.x, pa.y, pa.z, ta.z, ta.w, xs, ys, zs, xa, ya, za);
+        to_crystal_frame(pa.x, pa.y, pa.z, ta.z, ta.w, q.xD, q.yD, q.zD, xb, yb, zb);
+        const float len = box_chord(xa, ya, za, xb, yb, zb, -0.5f * sa.x, -0.5f * sa.y, -0.5f * sa.z,
+                                    0.5f * sa.x, 0.5f * sa.y, 0.5f * sa.z);
+        if (len != 0.0f) f(a, len);
+    }
+}
+
+__device__ __forceinline__ bool pair_enabled(const DevGeom& g, int parts, int s, int d)
+{
+    if (s < g.n_det) return (parts & 1) && s != d;
+    return (parts & 2) != 0;
+}
+
+__global__ void pair_count_kernel(DevGeom g, int parts, const uint32_t* bm_cry, const uint32_t* bm_col,
+                                  int* counts)
+{
+    const int ns = g.n_det + g.n_holes0;
+    const long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= (long long)g.n_det * ns) return;
+    const int d = (int)(p / ns), s = (int)(p - (long long)d * ns);
+    int c = 0;
+    if (pair_enabled(g, parts, s, d)) {
+        float xs, ys, zs;
+        scatter_point(g, s, xs, ys, zs);
+        const DetPoint q = det_point(__ldg(&g.cry.pos[d]), __ldg(&g.cry.size[d]), __ldg(&g.cry.trig[d]));
+        for_each_attenuator(g, bm_cry, bm_col, s, d, xs, ys, zs, q, [&](int, float) { ++c; });
+    }
+    counts[p] = c;
+}
+
+__global__ void pair_fill_kernel(DevGeom g, int parts, const uint32_t* bm_cry, const uint32_t* bm_col,
+                                 const int* offsets, PairRec* pairs, AttEntry* att)
+{
+    const int ns = g.n_det + g.n_holes0;
+    const long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= (long long)g.n_det * ns) return;
+    const int d = (int)(p / ns), s = (int)(p - (long long)d * ns);
+    PairRec r{};
+    r.valid = pair_enabled(g, parts, s, d);
+    if (r.valid) {
+        float xs, ys, zs;
+        scatter_point(g, s, xs, ys, zs);
+        const float4 P = __ldg(&g.cry.pos[d]), S = __ldg(&g.cry.size[d]), T = __ldg(&g.cry.trig[d]);
+        const DetPoint q = det_point(P, S, T);
+        to_crystal_frame(P.x, P.y, P.z, T.z, T.w, xs, ys, zs, r.xss, r.yss, r.zss);   // :1290-1292
+        r.lsd = dist3(xs, ys, zs, q.xD, q.yD, q.zD);                                   // :1275
+        // absorption chord along the extended scatter->detector ray (:1420-1424)
+        const float ux1 = ((float)0 / (float)1 - 0.5f) * S.x, ux2 = (((float)0 + 1.0f) / (float)1 - 0.5f) * S.x;
+        const float uy1 = ((float)0 / (float)1 - 0.5f) * S.y, uy2 = (((float)0 + 1.0f) / (float)1 - 0.5f) * S.y;
+        const float uz1 = ((float)0 / (float)1 - 0.5f) * S.z, uz2 = (((float)0 + 1.0f) / (float)1 - 0.5f) * S.z;
+        const float xt = q.xDs + 1000.0f * (q.xDs - r.xss) / r.lsd;
+        const float yt = q.yDs + 1000.0f * (q.yDs - r.yss) / r.lsd;
+        const float zt = q.zDs + 1000.0f * (q.zDs - r.zss) / r.lsd;
+        r.labs = box_chord(r.xss, r.yss, r.zss, xt, yt, zt, ux1, uy1, uz1, ux2, uy2, uz2);
+        r.att_begin = offsets[p];
+        int k = 0;
+        for_each_attenuator(g, bm_cry, bm_col, s, d, xs, ys, zs, q, [&](int a, float len) {
+            const float4 mu = __ldg(&g.cry.mu[a]);
+            att[r.att_begin + k] = AttEntry{len, mu.y, mu.z};
+            ++k;
+        });
+        r.att_count = k;
+    }
+    pairs[p] = r;
+}
+
+// ---- scatter items ----
+
+struct ElemConst {
+    float xI, yI, zI, xIs, yIs, zIs;
+    DetPoint q;
+    float w, t, h;
+    float mu_pe, mu_c, eres;
+    float lo, hi;
+    float rdet;
+    float ux1, ux2, uy1, uy2, uz1, uz2;
+};
+
+// One (d, v, s) item; w_s is the interaction weight (PE * muC/muPE or hole solid angle *
+// muC/mu of layer 0).  Returns the float the reference would atomically add.
+__device__ float scatter_item(const ElemConst& e, const PairRec& pr, const AttEntry* __restrict__ att,
+                              float xs, float ys, float zs, float w_s, float e0, float integ)
+{
+    const float cone = cone_angle(e.xI, e.yI, e.zI, xs, ys, zs, e.q.xD, e.q.yD, e.q.zD);
+    const float es = e0 / (1.0f + (e0 / 511.0f) * (1.0f - cosf(cone)));     // :1016-1023
+    const float res = e.eres * sqrtf(es / e0);
+    if ((es * (1 + 2 * res / 2.35482f)) <= e.lo || (es * (1 - 2 * res / 2.35482f)) >= e.hi)
+        return 0.0f;                                                         // :1263-1269
+    const float pwin = window_prob(es, res, e.lo, e.hi);
+    const float sc = sinf(cone);
+    float phi;
+    if (pr.lsd * sc * 2.0f <= e.rdet) phi = (float)(2.0f * 3.14159265358979323846);
+    else {
+        const float arg = e.rdet / 2.0f / pr.lsd / sc;
+        phi = 4.0f * asinf((arg <= 1.0f) ? arg : 1.0f);
+    }
+    // theta range over the 8 corners of the (single) detector unit (:1305-1335)
+    const float dis = dist3(pr.xss, pr.yss, pr.zss, e.xIs, e.yIs, e.zIs);
+    const float xt = pr.xss + 1000.0f * (pr.xss - e.xIs) / dis;
+    const float yt = pr.yss + 1000.0f * (pr.yss - e.yIs) / dis;
+    const float zt = pr.zss + 1000.0f * (pr.zss - e.zIs) / dis;
+    const float lthr = box_chord(e.xIs, e.yIs, e.zIs, xt, yt, zt, e.ux1, e.uy1, e.uz1, e.ux2, e.uy2, e.uz2);
+    float tmin = 0.0f, tmax = 0.0f;
+#pragma unroll
+    for (int c = 0; c < 8; ++c) {
+        // corner order of the reference: (x1,y1,z1),(x2,y1,z1),(x1,y2,z1),(x1,y1,z2),
+        // (x2,y2,z1),(x2,y1,z2),(x1,y2,z2),(x2,y2,z2)
+        const int cx = (c == 1 || c == 4 || c == 5 || c == 7);
+        const int cy = (c == 2 || c == 4 || c == 6 || c == 7);
+        const int cz = (c == 3 || c == 5 || c == 6 || c == 7);
+        const float th = cone_angle(e.xIs, e.yIs, e.zIs, pr.xss, pr.yss, pr.zss, cx ? e.ux2 : e.ux1,
+                                    cy ? e.uy2 : e.uy1, cz ? e.uz2 : e.uz1);
+        if (c == 0) { tmin = th; tmax = th; }
+        else {
+            if (th > tmax) tmax = th;
+            if (th < tmin) tmin = th;
+        }
+    }
+    if (lthr > 0.001f) tmin = 0.0f;
+    const int n = (int)((tmax - tmin) / 0.01f);
+    const float ratio = kn_sum(tmin, n, e0 / 511.0f) / integ;
+    // attenuation by the flagged crystals at the scattered energy (:1369-1396)
+    float a_sum = 0.0f;
+    for (int k = 0; k < pr.att_count; ++k) {
+        const AttEntry ae = att[pr.att_begin + k];
+        const float mpe = ae.mu_pe * e0 * e0 * e0 / es / es / es;
+        const float mc = ae.mu_c * e0 / es;
+        const float mt = mpe + mc;
+        a_sum = a_sum + ae.len * mt;
+    }
+    const float mpe_s = e.mu_pe * e0 * e0 * e0 / es / es / es;              // :1411-1417
+    const float mc_s = e.mu_c * e0 / es;
+    const float mt_s = mpe_s + mc_s;
+    const double c = (double)(w_s * phi / 2.0f) / 3.14159265358979323846 * (double)ratio *
+                     (double)pwin * (double)expf(-a_sum) *
+                     (double)(1.0f - expf(-pr.labs * mt_s)) * (double)mpe_s / (double)mt_s;
+    return (float)c;
+}
+
+__global__ void __launch_bounds__(kItemThreads)
+scatter_kernel(DevGeom g, ScatterPhysics ph, ScatterLaunch L)
+{
+    __shared__ PairRec sp[kPairChunk];
+    const int di = blockIdx.y;
+    const int d = L.det_begin + di;
+    const long long vi = (long long)blockIdx.x * kItemThreads + threadIdx.x;
+    const bool active = vi < L.vox_count;
+    const long long v = L.vox_begin + (active ? vi : 0);
+    const int ns = g.n_det + g.n_holes0;
+
+    const float4 P = __ldg(&g.cry.pos[d]), S = __ldg(&g.cry.size[d]);
+    const float4 M = __ldg(&g.cry.mu[d]), T = __ldg(&g.cry.trig[d]);
+    const bool run = ph.use_compton && (M.x > 0.01f);                       // :1226-1228
+
+    ElemConst e;
+    const float ang = L.rotation * g.angle_step;
+    voxel_centre(g, v, cosf(ang), sinf(ang), e.xI, e.yI, e.zI);
+    to_crystal_frame(P.x, P.y, P.z, T.z, T.w, e.xI, e.yI, e.zI, e.xIs, e.yIs, e.zIs);
+    e.q = det_point(P, S, T);
+    e.w = S.x; e.t = S.y; e.h = S.z;
+    e.mu_pe = M.y; e.mu_c = M.z; e.eres = M.w;
+    if (ph.same_window) { e.lo = ph.lo; e.hi = ph.hi; }
+    else {
+        e.lo = (1 - e.eres / 2.0f) * ph.e0;                                  // :1161-1162
+        e.hi = (1 + e.eres / 2.0f) * ph.e0;
+    }
+    e.rdet = sqrtf(e.w * e.w / (float)1 / (float)1 + e.h * e.h / (float)1 / (float)1 +
+                   e.t * e.t / (float)1 / (float)1) / 2.0f;
+    e.ux1 = ((float)0 / (float)1 - 0.5f) * e.w; e.ux2 = (((float)0 + 1.0f) / (float)1 - 0.5f) * e.w;
+    e.uy1 = ((float)0 / (float)1 - 0.5f) * e.t; e.uy2 = (((float)0 + 1.0f) / (float)1 - 0.5f) * e.t;
+    e.uz1 = ((float)0 / (float)1 - 0.5f) * e.h; e.uz2 = (((float)0 + 1.0f) / (float)1 - 0.5f) * e.h;
+
+    double acc_c = 0.0, acc_h = 0.0;
+    const int s_begin = (L.parts & 1) ? 0 : g.n_det;
+    const int s_end = (L.parts & 2) ? ns : g.n_det;
+    const PairRec* prow = L.pairs + (long long)d * ns;
+    for (int s0 = s_begin; s0 < s_end; s0 += kPairChunk) {
+        const int cnt = min(kPairChunk, s_end - s0);
+        __syncthreads();
+        for (int k = threadIdx.x; k < cnt; k += kItemThreads) sp[k] = prow[s0 + k];
+        __syncthreads();
+        if (!run || !active) continue;
+        for (int k = 0; k < cnt; ++k) {
+            const int s = s0 + k;
+            const PairRec& pr = sp[k];
+            if (!pr.valid) continue;
+            float xs, ys, zs, w_s;
+            if (s < g.n_det) {
+                w_s = __ldg(&L.pe[(long long)s * g.nvox + v]) * e.mu_c / e.mu_pe;   // :1218-1219
+                if (w_s == 0.0f) continue;          // the item is exactly 0
+                const float4 ps = __ldg(&g.cry.pos[s]);
+                xs = ps.x; ys = ps.y; zs = ps.z;
+                acc_c += (double)scatter_item(e, pr, L.att, xs, ys, zs, w_s, ph.e0, ph.integ);
+            } else {
+                const float4 hr = __ldg(&g.hole.raw[s - g.n_det]);
+                xs = hr.x;
+                ys = (hr.y + hr.z) / 2.0f + g.fov;
+                zs = hr.w;
+                const float lih = dist3(e.xI, e.yI, e.zI, xs, ys, zs);
+                float sa;
+                if (L.hole_model == 0) {                                  // :1711-1715
+                    const float vr = 0.1f;
+                    sa = (float)(((double)(vr * vr) * 3.14159265358979323846 + (double)((hr.z - hr.y) * vr)) /
+                                 (4.0f * 3.14159265358979323846 * (double)lih * (double)lih) *
+                                 (double)fabsf(ys - e.yI) / (double)lih);
+                } else {                                                  // ScatterGen_Collimator :1212-1215
+                    const float vr = 0.2f;
+                    sa = (vr * vr + (hr.z - hr.y) * vr) / (4.0f * lih * lih);
+                }
+                w_s = sa / ph.col_mu_tot0 * ph.col_mu_c0;                // :1716
+                acc_h += (double)scatter_item(e, pr, L.att, xs, ys, zs, w_s, ph.e0, ph.integ);
+            }
+        }
+    }
+    if (!active) return;
+    float outv;
+    if ((L.parts & 3) == 3) outv = (float)acc_h + (float)acc_c;              // :2354-2357
+    else if (L.parts & 1) outv = (float)acc_c;
+    else outv = (float)acc_h;
+    L.out[(long long)di * L.ld + vi] = outv;
+}
+
+}  // namespace
+
+long long bitmap_crystal_words(int n)
+{
+    const long long pairs = (long long)n * (n + 1) / 2;
+    return (pairs * n + 31) / 32;
+}
+
+long long bitmap_collimator_words(int n, int nh0)
+{
+    return ((long long)n * n * nh0 + 31) / 32;
+}
+
+int launch_bitmap_crystal(const DevGeom& g, uint32_t* words, cudaStream_t s)
+{
+    const long long nw = bitmap_crystal_words(g.n_det);
+    if (nw == 0) return 0;
+    const long long blocks = (nw + 255) / 256;
+    bitmap_crystal_kernel<<<(unsigned)blocks, 256, 0, s>>>(g.raw_det, g.n_det, nw, words);
+    return cudaGetLastError() == cudaSuccess ? 0 : -1;
+}
+
+int launch_bitmap_collimator(const DevGeom& g, uint32_t* words, cudaStream_t s)
+{
+    const long long nw = bitmap_collimator_words(g.n_det, g.n_holes0);
+    if (nw == 0) return 0;
+    const long long blocks = (nw + 255) / 256;
+    bitmap_collimator_kernel<<<(unsigned)blocks, 256, 0, s>>>(g.raw_det, g.hole.raw, g.n_det,
+                                                              g.n_holes0, nw, words);
+    return cudaGetLastError() == cudaSuccess ? 0 : -1;
+}
+
+int build_scatter_pairs(const DevGeom& g, int parts, const uint32_t* bm_cry, const uint32_t* bm_col,
+                        ScatterScratch& scratch, PairRec** pairs, AttEntry** att, cudaStream_t s)
+{
+    const int ns = g.n_det + g.n_holes0;
+    const long long np = (long long)g.n_det * ns;
+    // layout: [counts/offsets (np+1 ints)][cub temp][pairs][att]
+    size_t temp_bytes = 0;
+    cub::DeviceScan::ExclusiveSum(nullptr, temp_bytes, (int*)nullptr, (int*)nullptr, (int)(np + 1), s);
+    auto align = [](size_t x) { return (x + 255) & ~size_t(255); };
+    const size_t off_counts = 0;
+    const size_t off_offsets = align(off_counts + sizeof(int) * (np + 1));
+    const size_t off_temp = align(off_offsets + sizeof(int) * (np + 1));
+    const size_t off_pairs = align(off_temp + temp_bytes);
+    const size_t fixed = align(off_pairs + sizeof(PairRec) * np);
+    if (scratch.bytes < fixed) {
+        scatter_scratch_free(scratch);
+        if (cudaMalloc(&scratch.base, fixed) != cudaSuccess) { scratch.base = nullptr; return -2; }
+        scratch.bytes = fixed;
+    }
+    char* base = (char*)scratch.base;
+    int* counts = (int*)(base + off_counts);
+    int* offsets = (int*)(base + off_offsets);
+    const unsigned blocks = (unsigned)((np + 255) / 256);
+    pair_count_kernel<<<blocks, 256, 0, s>>>(g, parts, bm_cry, bm_col, counts);
+    if (cudaMemsetAsync(counts + np, 0, sizeof(int), s) != cudaSuccess) return -1;
+    cub::DeviceScan::ExclusiveSum(base + off_temp, temp_bytes, counts, offsets, (int)(np + 1), s);
+    int total = 0;
+    if (cudaMemcpyAsync(&total, offsets + np, sizeof(int), cudaMemcpyDeviceToHost, s) != cudaSuccess) return -1;
+    if (cudaStreamSynchronize(s) != cudaSuccess) return -1;
+    const size_t need = fixed + sizeof(AttEntry) * (size_t)(total > 0 ? total : 1);
+    if (scratch.bytes < need) {
+        // grow, keeping nothing but the offsets (re-run the cheap count+scan afterwards)
+        scatter_scratch_free(scratch);
+        if (cudaMalloc(&scratch.base, need) != cudaSuccess) { scratch.base = nullptr; return -2; }
+        scratch.bytes = need;
+        base = (char*)scratch.base;
+        counts = (int*)(base + off_counts);
+        offsets = (int*)(base + off_offsets);
+        pair_count_kernel<<<blocks, 256, 0, s>>>(g, parts, bm_cry, bm_col, counts);
+        if (cudaMemsetAsync(counts + np, 0, sizeof(int), s) != cudaSuccess) return -1;
+        cub::DeviceScan::ExclusiveSum(base + off_temp, temp_bytes, counts, offsets, (int)(np + 1), s);
+    }
+    *pairs = (PairRec*)(base + off_pairs);
+    *att = (AttEntry*)(base + fixed);
+    pair_fill_kernel<<<blocks, 256, 0, s>>>(g, parts, bm_cry, bm_col, offsets, *pairs, *att);
+    return cudaGetLastError() == cudaSuccess ? 0 : -1;
+}
+
+int launch_scatter(const DevGeom& g, const ScatterPhysics& ph, const ScatterLaunch& L, cudaStream_t s)
+{
+    if (L.det_count == 0 || L.vox_count == 0) return 0;
+    dim3 grid((unsigned)((L.vox_count + kItemThreads - 1) / kItemThreads), (unsigned)L.det_count);
+    scatter_kernel<<<grid, kItemThreads, 0, s>>>(g, ph, L);
+    return cudaGetLastError() == cudaSuccess ? 0 : -1;
+}
+
+double kn_normalisation(double e0)
+{
+    const float step = 0.01f;
+    const int n = (int)((float)3.14159265358979323846 / step);
+    const double alpha = e0 / 511.0;
+    double sum = 0.0;
+    for (int i = 0; i <= n; ++i) {
+        const double th = (double)((float)i * step);
+        const double c = std::cos(th), sn = std::sin(th);
+        const double f1 = alpha * (1.0 - c), f2 = 1.0 + c * c, p = 1.0 + f1;
+        sum += f2 / p / p * (1.0 + f1 * f1 / f2 / p) * sn * (double)step;
+    }
+    return sum;
+}
+
+}  // namespace sysmat

@@ -1,13 +1,16 @@
-// Launch interface of the primary-Compton scatter kernels (scatter.cu).
+// Launch interface of the primary-Compton scatter kernels and the relationship-bitmap
+// kernels (scatter.cu).
 #pragma once
 
+#include <cstdint>
 #include <cuda_runtime.h>
 
 #include "geom.cuh"
 
 namespace sysmat {
 
-// Device scratch owned by a context for the scatter path.
+// Device scratch owned by a context for the scatter path: per-(scatterer, detector) pair
+// records and the attenuator lists they index.
 struct ScatterScratch {
     void* base = nullptr;
     size_t bytes = 0;
@@ -19,5 +22,64 @@ inline void scatter_scratch_free(ScatterScratch& s)
     s.base = nullptr;
     s.bytes = 0;
 }
+
+// Pair record of scatterer s (crystal k = s, or hole h = s - D) and detector crystal d,
+// stored at index d * (D + H0) + s.
+struct PairRec {
+    float xss, yss, zss;   // scatter point in crystal d's frame
+    float lsd;             // |scatter point - crystal d centre| (world)
+    float labs;            // chord of the absorption ray inside crystal d
+    int att_begin;         // first entry in the attenuator list
+    int att_count;         // number of attenuators with a non-zero chord
+    int valid;             // 0 for the excluded pair s == d
+};
+
+// Attenuator entry: chord length and the attenuator's photoelectric and Compton
+// coefficients at the photopeak energy.
+struct AttEntry {
+    float len, mu_pe, mu_c;
+};
+
+struct ScatterPhysics {
+    int use_compton;       // (int)floor(P[0] + 0.5f) == 1
+    int same_window;       // (int)floor(P[4] + 0.5f) > 0
+    float lo, hi;          // P[5], P[6]
+    float e0;              // P[7]
+    float integ;           // KN normalisation over [0, pi] (FP64 sum, rounded)
+    float col_mu_tot0;     // C[15]
+    float col_mu_c0;       // C[17]
+};
+
+struct ScatterLaunch {
+    int parts;             // bit 0 crystal, bit 1 collimator
+    int hole_model;        // 0 combined program, 1 collimator-only program
+    int det_begin, det_count;
+    long long vox_begin, vox_count, ld;
+    float rotation;
+    const float* pe;       // D x V photoelectric matrix (crystal part)
+    const PairRec* pairs;
+    const AttEntry* att;
+    float* out;
+};
+
+// Word counts of the reference bitmap layouts (scatter.cu:2053-2056, :2234-2237).
+long long bitmap_crystal_words(int n_det);
+long long bitmap_collimator_words(int n_det, int n_holes0);
+
+int launch_bitmap_crystal(const DevGeom& g, uint32_t* words, cudaStream_t s);
+int launch_bitmap_collimator(const DevGeom& g, uint32_t* words, cudaStream_t s);
+
+// Build pair records and attenuator lists.  Allocates/grows `scratch` as needed (synchronises
+// `s` once to size the attenuator list).  parts selects which pairs are built.
+int build_scatter_pairs(const DevGeom& g, int parts, const uint32_t* bm_crystal,
+                        const uint32_t* bm_collimator, ScatterScratch& scratch, PairRec** pairs,
+                        AttEntry** att, cudaStream_t s);
+
+int launch_scatter(const DevGeom& g, const ScatterPhysics& ph, const ScatterLaunch& L,
+                   cudaStream_t s);
+
+// Klein-Nishina normalisation of the reference, sum over theta_i = float(i * 0.01f),
+// i = 0..floor(float(pi)/0.01f), evaluated in double (scatter.cu:980-993, :1169).
+double kn_normalisation(double e0);
 
 }  // namespace sysmat

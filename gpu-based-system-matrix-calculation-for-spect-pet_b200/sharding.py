@@ -1,0 +1,23 @@
+"""Work partitioning of a system-matrix job across ranks (one process per GPU).
+
+Matrix elements are independent, so ranks share no data: each rank owns whole voxel
+planes (z) of the image grid for every detector, the unit the benchmark and the
+multi-GPU driver hand out.  No collective touches the data path; only the timing
+reduction (max over ranks) crosses ranks.
+"""
+from __future__ import annotations
+
+
+def plane_for_step(step: int, rank: int, world: int, n_planes: int, first: int = 0) -> int:
+    """z-plane processed by `rank` at `step`: ranks take interleaved planes so per-rank work
+    is fixed as the world grows (weak scaling) and no two ranks of a step share a plane
+    while step * world + rank < n_planes."""
+    return first + (step * world + rank) % n_planes
+
+
+def detector_slab(n_det: int, rank: int, world: int) -> tuple[int, int]:
+    """Contiguous detector rows [begin, begin + count) of `rank` when rows are split;
+    sizes differ by at most one."""
+    base, extra = divmod(n_det, world)
+    begin = rank * base + min(rank, extra)
+    return begin, base + (1 if rank < extra else 0)

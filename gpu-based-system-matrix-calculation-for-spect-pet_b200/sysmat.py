@@ -30,7 +30,8 @@ HOLE_MODEL_VARIANT = 1
 EXPORTS = ("PESysMatGen", "scatter", "scatter_collimator", "scatter_crystal", "sysmat_create",
            "sysmat_destroy", "sysmat_dims", "sysmat_pe", "sysmat_bitmap_crystal_words",
            "sysmat_bitmap_collimator_words", "sysmat_bitmap_crystal", "sysmat_bitmap_collimator",
-           "sysmat_scatter", "sysmat_error_string", "sysmat_version")
+           "sysmat_scatter_prepare", "sysmat_scatter", "sysmat_pe_work", "sysmat_measure_peaks",
+           "sysmat_error_string", "sysmat_version")
 
 _fp = ctypes.POINTER(ctypes.c_float)
 _vp = ctypes.c_void_p
@@ -69,9 +70,15 @@ def lib():
             "sysmat_bitmap_collimator_words": ([_vp], ctypes.c_longlong),
             "sysmat_bitmap_crystal": ([_vp, _vp, _vp], ctypes.c_int),
             "sysmat_bitmap_collimator": ([_vp, _vp, _vp], ctypes.c_int),
-            "sysmat_scatter": ([_vp, ctypes.c_int, ctypes.c_int, ctypes.c_float, _vp, _vp, _vp,
-                                ctypes.c_int, ctypes.c_int, ctypes.c_longlong, ctypes.c_longlong, _vp,
+            "sysmat_scatter_prepare": ([_vp, ctypes.c_int, _vp, _vp, _vp], ctypes.c_int),
+            "sysmat_scatter": ([_vp, ctypes.c_int, ctypes.c_int, ctypes.c_float, _vp, ctypes.c_int,
+                                ctypes.c_int, ctypes.c_longlong, ctypes.c_longlong, _vp,
                                 ctypes.c_longlong, _vp], ctypes.c_int),
+            "sysmat_pe_work": ([_vp, ctypes.c_float, ctypes.c_int, ctypes.c_int, ctypes.c_longlong,
+                                ctypes.c_longlong, _vp, ctypes.c_longlong,
+                                ctypes.POINTER(ctypes.c_ulonglong), _vp], ctypes.c_int),
+            "sysmat_measure_peaks": ([ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double)],
+                                     ctypes.c_int),
             "sysmat_error_string": ([ctypes.c_int], ctypes.c_char_p),
             "sysmat_version": ([], ctypes.c_char_p),
         }
@@ -191,6 +198,18 @@ class Context:
                                _ptr(out), ld, mode, _stream(stream)), "sysmat_pe")
         return out
 
+    def pe_work(self, out, rotation=0.0, det_begin=0, det_count=None, vox_begin=0, vox_count=None,
+                stream=None):
+        """Reference-mode PE block with work counters; returns a dict of counts."""
+        det_count = self.n_det - det_begin if det_count is None else det_count
+        vox_count = self.n_vox - vox_begin if vox_count is None else vox_count
+        ld = out.stride(0) if out.dim() == 2 else vox_count
+        c = (ctypes.c_ulonglong * 6)()
+        _check(lib().sysmat_pe_work(self.handle, float(rotation), det_begin, det_count, vox_begin,
+                                    vox_count, _ptr(out), ld, c, _stream(stream)), "sysmat_pe_work")
+        keys = ("subelements", "hole_hits", "crystal_hits", "elements", "blocked", "reserved")
+        return dict(zip(keys, (int(x) for x in c)))
+
     def bitmap_crystal(self, stream=None):
         import torch
         n = lib().sysmat_bitmap_crystal_words(self.handle)
@@ -206,16 +225,29 @@ class Context:
                "bitmap_collimator")
         return out[:n]
 
-    def scatter(self, out, pe, parts=SCATTER_CRYSTAL | SCATTER_COLLIMATOR,
-                hole_model=HOLE_MODEL_COMBINED, bm_crystal=None, bm_collimator=None, rotation=0.0,
-                det_begin=0, det_count=None, vox_begin=0, vox_count=None, stream=None):
+    def scatter_prepare(self, bm_crystal=None, bm_collimator=None,
+                        parts=SCATTER_CRYSTAL | SCATTER_COLLIMATOR, stream=None):
+        nullp = ctypes.c_void_p(0)
+        _check(lib().sysmat_scatter_prepare(self.handle, parts,
+                                            _ptr(bm_crystal) if bm_crystal is not None else nullp,
+                                            _ptr(bm_collimator) if bm_collimator is not None else nullp,
+                                            _stream(stream)), "sysmat_scatter_prepare")
+
+    def scatter(self, out, pe=None, parts=SCATTER_CRYSTAL | SCATTER_COLLIMATOR,
+                hole_model=HOLE_MODEL_COMBINED, rotation=0.0, det_begin=0, det_count=None,
+                vox_begin=0, vox_count=None, stream=None):
         det_count = self.n_det - det_begin if det_count is None else det_count
         vox_count = self.n_vox - vox_begin if vox_count is None else vox_count
         ld = out.stride(0) if out.dim() == 2 else vox_count
-        nullp = ctypes.c_void_p(0)
-        _check(lib().sysmat_scatter(self.handle, parts, hole_model, float(rotation), _ptr(pe),
-                                    _ptr(bm_crystal) if bm_crystal is not None else nullp,
-                                    _ptr(bm_collimator) if bm_collimator is not None else nullp,
-                                    det_begin, det_count, vox_begin, vox_count, _ptr(out), ld,
-                                    _stream(stream)), "sysmat_scatter")
+        _check(lib().sysmat_scatter(self.handle, parts, hole_model, float(rotation),
+                                    _ptr(pe) if pe is not None else ctypes.c_void_p(0), det_begin,
+                                    det_count, vox_begin, vox_count, _ptr(out), ld, _stream(stream)),
+               "sysmat_scatter")
         return out
+
+
+def measure_peaks():
+    """(FP32 TFLOP/s, MUFU Tops/s) measured on the current device."""
+    f, m = ctypes.c_double(), ctypes.c_double()
+    _check(lib().sysmat_measure_peaks(ctypes.byref(f), ctypes.byref(m)), "sysmat_measure_peaks")
+    return f.value, m.value

@@ -112,15 +112,35 @@ SYSMAT_API long long sysmat_bitmap_collimator_words(const sysmat_ctx* ctx);
 SYSMAT_API int sysmat_bitmap_crystal(sysmat_ctx* ctx, uint32_t* d_words, void* stream);
 SYSMAT_API int sysmat_bitmap_collimator(sysmat_ctx* ctx, uint32_t* d_words, void* stream);
 
-/* Primary-Compton scatter block.  parts: SYSMAT_SCATTER_* mask.  d_pe: the D x V
- * photoelectric matrix (row stride V) the crystal part reads.  d_bm_crystal /
- * d_bm_collimator: bitmaps as produced above or loaded from the reference's files.
- * hole_model: SYSMAT_HOLE_MODEL_*.  With both parts the result is
- * float(collimator) + float(crystal), as the reference sums on the host. */
-SYSMAT_API int sysmat_scatter(sysmat_ctx* ctx, int parts, int hole_model, float rotation, const float* d_pe,
-                   const uint32_t* d_bm_crystal, const uint32_t* d_bm_collimator, int det_begin,
-                   int det_count, long long vox_begin, long long vox_count, float* d_out,
-                   long long ld, void* stream);
+/* Build the scatter path's per-(scatterer, detector) pair tables from relationship bitmaps
+ * (as produced above or loaded from the reference's files).  parts: SYSMAT_SCATTER_* mask;
+ * the bitmap of a part that is not requested may be NULL.  Synchronises `stream` once.
+ * The tables stay valid until the next prepare or sysmat_destroy. */
+SYSMAT_API int sysmat_scatter_prepare(sysmat_ctx* ctx, int parts, const uint32_t* d_bm_crystal,
+                                      const uint32_t* d_bm_collimator, void* stream);
+
+/* Primary-Compton scatter block (parts must have been prepared).  d_pe: the D x V
+ * photoelectric matrix (row stride V) the crystal part reads.  hole_model:
+ * SYSMAT_HOLE_MODEL_*.  With both parts the result is float(collimator) + float(crystal),
+ * as the reference sums on the host (scatter.cu:2354-2357). */
+SYSMAT_API int sysmat_scatter(sysmat_ctx* ctx, int parts, int hole_model, float rotation,
+                              const float* d_pe, int det_begin, int det_count, long long vox_begin,
+                              long long vox_count, float* d_out, long long ld, void* stream);
+
+/* ---------------------------------------------------------------------------------- */
+/* Diagnostics (benchmark roofline).                                                     */
+
+/* Same block as sysmat_pe (reference summation) with work counters: counts[0] sub-elements
+ * evaluated, [1] hole chords that are non-zero, [2] crystal chords that are non-zero,
+ * [3] elements, [4] sub-elements stopped by the plate-bypass penalty, [5] reserved.
+ * Synchronous. */
+SYSMAT_API int sysmat_pe_work(sysmat_ctx* ctx, float rotation, int det_begin, int det_count,
+                              long long vox_begin, long long vox_count, float* d_out, long long ld,
+                              unsigned long long* counts, void* stream);
+
+/* Measured FP32 FMA throughput (TFLOP/s, FMA = 2 flops) and MUFU throughput (Tops/s) of
+ * the current device, from two short calibration kernels. */
+SYSMAT_API int sysmat_measure_peaks(double* fp32_tflops, double* mufu_tops);
 
 /* Text for a SYSMAT_ERR_* code. */
 SYSMAT_API const char* sysmat_error_string(int code);

@@ -49,6 +49,9 @@ def lib():
         for name in ("oracle_box_chord", "oracle_box_chord_inside", "oracle_cyl_chord"):
             getattr(L, name).argtypes = [ctypes.c_int, _dp]
             getattr(L, name).restype = ctypes.c_double
+        L.oracle_scatter_trace.argtypes = [_fp, _fp, _fp, _fp, _fp, _u32p, ctypes.c_int, ctypes.c_int,
+                                           ctypes.c_int, ctypes.c_longlong, _dp]
+        L.oracle_scatter_trace.restype = ctypes.c_double
         L.oracle_kn_sum.argtypes = [ctypes.c_int, ctypes.c_double, ctypes.c_double, ctypes.c_double]
         L.oracle_kn_sum.restype = ctypes.c_double
         _lib = L
@@ -140,3 +143,18 @@ def cyl_chord(args, prec=64):
 
 def kn_sum(e0, lo, hi, prec=64):
     return lib().oracle_kn_sum(prec, e0, lo, hi)
+
+
+def scatter_trace(geo, pe_matrix, part, bitmap, d, v, prec=64):
+    """(element value, per-item trace array (n_items, 9)) for one scatter element."""
+    c, pc = _f32(geo.collimator)
+    dd, pd = _f32(geo.detector)
+    i, pi = _f32(geo.image)
+    p, pp = _f32(geo.physics)
+    m, pm = _f32(np.asarray(pe_matrix, dtype=np.float32).reshape(-1))
+    b = np.ascontiguousarray(bitmap, dtype=np.uint32)
+    n = geo.n_det if part == "crystal" else geo.n_holes_layer0
+    tr = np.full((n, 9), np.nan)
+    val = lib().oracle_scatter_trace(pc, pd, pi, pp, pm, b.ctypes.data_as(_u32p), PART[part], prec, d, v,
+                                     tr.ctypes.data_as(_dp))
+    return val, tr

@@ -429,7 +429,7 @@ static inline REAL FN(dist3)(REAL x1, REAL y1, REAL z1, REAL x2, REAL y2, REAL z
 static REAL FN(scatter_item)(const ogeo* g, int kind, int d, int k, REAL xs, REAL ys, REAL zs,
                              REAL w_s, const FN(crystal)* cd, REAL xI, REAL yI, REAL zI,
                              REAL xIs, REAL yIs, REAL zIs, REAL e0, REAL lo_w, REAL hi_w,
-                             REAL integ, const uint32_t* bitmap)
+                             REAL integ, const uint32_t* bitmap, double* trace)
 {
     REAL xDs = -cd->w / (REAL)2.0f + (REAL)((REAL)0 + (REAL)0.5f) / (REAL)1 * cd->w;
     REAL zDs = -cd->h / (REAL)2.0f + (REAL)((REAL)0 + (REAL)0.5f) / (REAL)1 * cd->h;
@@ -441,6 +441,10 @@ static REAL FN(scatter_item)(const ogeo* g, int kind, int d, int k, REAL xs, REA
     REAL cone = FN(cone_angle)(xI, yI, zI, xs, ys, zs, xD, yD, zD);
     REAL es = e0 / ((REAL)1.0f + (e0 / (REAL)511.0f) * ((REAL)1.0f - COS(cone)));
     REAL res_s = cd->eres * SQRT(es / e0);
+    if (trace) {
+        trace[1] = (double)(es * ((REAL)1 + (REAL)2 * res_s / (REAL)2.35482f)) - (double)lo_w;
+        trace[2] = (double)hi_w - (double)(es * ((REAL)1 - (REAL)2 * res_s / (REAL)2.35482f));
+    }
     if ((es * ((REAL)1 + (REAL)2 * res_s / (REAL)2.35482f)) <= lo_w ||
         (es * ((REAL)1 - (REAL)2 * res_s / (REAL)2.35482f)) >= hi_w)
         return 0;                                              /* 2-sigma window reject :1263 */
@@ -474,6 +478,12 @@ static REAL FN(scatter_item)(const ogeo* g, int kind, int d, int k, REAL xs, REA
         if (th[i] < tmin) tmin = th[i];
     }
     if (lthr > (REAL)0.001f) tmin = 0;
+    if (trace) {
+        trace[3] = (double)lthr;
+        trace[4] = (double)((tmax - tmin) / (REAL)0.01f);
+        trace[5] = (double)tmin;
+        trace[6] = (double)tmax;
+    }
     REAL ratio = FN(kn_sum)(e0, tmin, tmax, (REAL)0.01f) / integ;
 
     /* attenuation by other crystals flagged in the relationship bitmap (:1343-1401) */
@@ -518,6 +528,11 @@ static REAL FN(scatter_item)(const ogeo* g, int kind, int d, int k, REAL xs, REA
     REAL labs = FN(box_chord)(xss, yss, zss, xt, yt, zt, ux1, uy1, uz1, ux2, uy2, uz2);
     double c = (double)(w_s * phi / (REAL)2.0f) / M_PI * (double)ratio * (double)pwin *
                (double)EXP(-att) * (double)((REAL)1.0f - EXP(-labs * mt_s)) * (double)mpe_s / (double)mt_s;
+    if (trace) {
+        trace[0] = (double)(REAL)c;
+        trace[7] = (double)att;
+        trace[8] = (double)phi;
+    }
     return (REAL)c;
 }
 
@@ -526,7 +541,7 @@ static REAL FN(scatter_item)(const ogeo* g, int kind, int d, int k, REAL xs, REA
  * (scatter.cu:1711-1716), part 3 = collimator scatter with the collimator-only program's
  * solid angle (ScatterGen_Collimator/scatter.cu:1212-1215). */
 static REAL FN(scatter_element)(const ogeo* g, int part, int d, long long v, const float* pe,
-                                const uint32_t* bitmap)
+                                const uint32_t* bitmap, double* trace)
 {
     const float* P = g->P;
     const float* C = g->C;
@@ -555,7 +570,8 @@ static REAL FN(scatter_element)(const ogeo* g, int part, int d, long long v, con
             FN(crystal) ck;
             FN(load_crystal)(g, k, &ck);
             sum = sum + FN(scatter_item)(g, 1, d, k, ck.x, ck.y, ck.z, prob, &cd, xI, yI, zI,
-                                         xIs, yIs, zIs, e0, lo_w, hi_w, integ, bitmap);
+                                         xIs, yIs, zIs, e0, lo_w, hi_w, integ, bitmap,
+                                         trace ? trace + 9 * k : NULL);
         }
     } else {
         for (int h = 0; h < g->nh0; ++h) {
@@ -576,7 +592,8 @@ static REAL FN(scatter_element)(const ogeo* g, int part, int d, long long v, con
             }
             REAL prob = sa / (REAL)C[15] * (REAL)C[17];
             sum = sum + FN(scatter_item)(g, 2, d, h, hx, hy, hz, prob, &cd, xI, yI, zI,
-                                         xIs, yIs, zIs, e0, lo_w, hi_w, integ, bitmap);
+                                         xIs, yIs, zIs, e0, lo_w, hi_w, integ, bitmap,
+                                         trace ? trace + 9 * h : NULL);
         }
     }
     return sum;

@@ -153,8 +153,8 @@ int oracle_scatter(const float* C, const float* D, const float* I, const float* 
     for (long long e = 0; e < total; ++e) {
         int d = dets[e / nv];
         long long v = v0 + e % nv;
-        if (prec == 32) out[e] = (double)scatter_element_f32(&g, part, d, v, pe, bitmap);
-        else            out[e] = scatter_element_f64(&g, part, d, v, pe, bitmap);
+        if (prec == 32) out[e] = (double)scatter_element_f32(&g, part, d, v, pe, bitmap, NULL);
+        else            out[e] = scatter_element_f64(&g, part, d, v, pe, bitmap, NULL);
     }
     return 0;
 }
@@ -277,4 +277,18 @@ double oracle_kn_sum(int prec, double e0, double lo, double hi)
 {
     if (prec == 32) return kn_sum_f32((float)e0, (float)lo, (float)hi, 0.01f);
     return kn_sum_f64(e0, lo, hi, (double)0.01f);
+}
+
+/* Per-item trace of one scatter element (debugging and tests): for item s, 9 values at
+ * trace[9*s]: contribution, window margins (lower, upper), extended-ray chord, KN step
+ * ratio (theta_max-theta_min)/0.01, theta_min, theta_max, attenuation, phi range.  Items
+ * rejected before a field is computed leave it unchanged. */
+double oracle_scatter_trace(const float* C, const float* D, const float* I, const float* P,
+                            const float* pe, const uint32_t* bitmap, int part, int prec, int d,
+                            long long v, double* trace)
+{
+    ogeo g;
+    if (parse(&g, C, D, I, P)) return NAN;
+    if (prec == 32) return (double)scatter_element_f32(&g, part, d, v, pe, bitmap, trace);
+    return scatter_element_f64(&g, part, d, v, pe, bitmap, trace);
 }

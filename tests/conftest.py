@@ -1,0 +1,64 @@
+"""Shared fixtures: the package modules (loaded by path: the package directory name is not a
+Python identifier), the CPU oracle (checker only), golden fixtures and comparison helpers."""
+from __future__ import annotations
+
+import importlib.util
+import os
+import sys
+
+import numpy as np
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+PKG_DIR = os.path.join(ROOT, "gpu-based-system-matrix-calculation-for-spect-pet_b200")
+GOLDEN_DIR = os.path.join(ROOT, "tests", "golden")
+sys.path.insert(0, os.path.join(ROOT, "oracle"))
+
+
+def _load(name, path):
+    if name in sys.modules:
+        return sys.modules[name]
+    spec = importlib.util.spec_from_file_location(name, path)
+    mod = importlib.util.module_from_spec(spec)
+    sys.modules[name] = mod
+    spec.loader.exec_module(mod)
+    return mod
+
+
+geometry = _load("sysmat_geometry", os.path.join(PKG_DIR, "geometry.py"))
+sysmat = _load("sysmat_binding", os.path.join(PKG_DIR, "sysmat.py"))
+
+import oracle  # noqa: E402  (test infrastructure)
+
+
+def pytest_configure(config):
+    config.addinivalue_line("markers", "gpu: needs a CUDA GPU (B200) and the built libsysmat.so")
+
+
+def golden(name):
+    z = np.load(os.path.join(GOLDEN_DIR, f"{name}.npz"))
+    geo = geometry.Geometry(name, z["collimator"], z["detector"], z["image"], z["physics"])
+    return geo, z
+
+
+def rel_err(a, b, scale=None):
+    """|a - b| / max(|b|, tau), tau = 1e-6 * max|b| over the matrix (guards near-zero
+    elements); `scale` gives that matrix maximum when b is a sample of it."""
+    a = np.asarray(a, dtype=np.float64)
+    b = np.asarray(b, dtype=np.float64)
+    m = float(scale) if scale is not None else (np.abs(b).max() if b.size else 0.0)
+    tau = 1e-6 * m if m > 0 else 1e-300
+    return np.abs(a - b) / np.maximum(np.abs(b), tau)
+
+
+# Per-element tolerance of the system matrix against the reference (north star: 1e-5).
+TOL = 1e-5
+
+
+@pytest.fixture(scope="session")
+def gpu():
+    """A CUDA device; GPU tests fail loudly (not skip) when it or the library is missing."""
+    import torch
+    assert torch.cuda.is_available(), "GPU test run without a CUDA device"
+    sysmat.lib()
+    return torch
