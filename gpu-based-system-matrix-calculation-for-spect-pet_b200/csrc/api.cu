@@ -372,7 +372,7 @@ extern "C" SYSMAT_API int sysmat_pe_work(sysmat_ctx* ctx, float rotation, int de
     if (rc) return rc;
     if (!counts) return SYSMAT_ERR_ARG;
     unsigned long long* d_cnt = nullptr;
-    if (cudaMalloc(&d_cnt, 8 * sizeof(unsigned long long)) != cudaSuccess) return SYSMAT_ERR_NOMEM;
+    if (cudaMalloc(&d_cnt, 16 * sizeof(unsigned long long)) != cudaSuccess) return SYSMAT_ERR_NOMEM;
     cudaStream_t s = (cudaStream_t)stream;
     PeLaunch L;
     L.det_begin = det_begin;
@@ -386,11 +386,11 @@ extern "C" SYSMAT_API int sysmat_pe_work(sysmat_ctx* ctx, float rotation, int de
     L.status = ctx->d_status;
     L.counters = d_cnt;
     rc = SYSMAT_OK;
-    if (cudaMemsetAsync(d_cnt, 0, 8 * sizeof(unsigned long long), s) != cudaSuccess ||
+    if (cudaMemsetAsync(d_cnt, 0, 16 * sizeof(unsigned long long), s) != cudaSuccess ||
         cudaMemsetAsync(ctx->d_counter, 0, sizeof(unsigned long long), s) != cudaSuccess ||
         cudaMemsetAsync(ctx->d_status, 0, sizeof(int), s) != cudaSuccess ||
         launch_pe(ctx->g, L, SYSMAT_MODE_REFERENCE, ctx->num_sms, s) ||
-        cudaMemcpyAsync(counts, d_cnt, 6 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, s) != cudaSuccess ||
+        cudaMemcpyAsync(counts, d_cnt, 10 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, s) != cudaSuccess ||
         cudaStreamSynchronize(s) != cudaSuccess)
         rc = SYSMAT_ERR_CUDA;
     cudaFree(d_cnt);

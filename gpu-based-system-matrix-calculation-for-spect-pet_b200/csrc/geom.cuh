@@ -189,6 +189,50 @@ __device__ __forceinline__ float box_chord_inside(float xi, float yi, float zi, 
     return tmax - tmin;
 }
 
+// Interval part of box_chord_inside for one box, given the segment's shared terms.
+__device__ __forceinline__ float inside_from_slabs(float xi, float yi, float zi, float ix, float iy,
+                                                   float iz, float tio, float x1, float y1, float z1,
+                                                   float x2, float y2, float z2)
+{
+    float tmin, tmax, a0, a1;
+    slab_interval(xi, x1, x2, ix, tmin, tmax);
+    slab_interval(yi, y1, y2, iy, a0, a1);
+    if (tmin > a1 || a0 > tmax) return 0.0f;
+    tmin = (a0 > tmin) ? a0 : tmin;
+    tmax = (a1 < tmax) ? a1 : tmax;
+    slab_interval(zi, z1, z2, iz, a0, a1);
+    if (tmin > a1 || a0 > tmax) return 0.0f;
+    tmin = (a0 > tmin) ? a0 : tmin;
+    tmax = (a1 < tmax) ? a1 : tmax;
+    if ((tmax - tmin) < kEps) return 0.0f;
+    if (tmin >= tio) return 0.0f;
+    if (tmax <= kEps) return 0.0f;
+    if ((tmax >= tio) && (tmin > kEps)) return tio - tmin;
+    if ((tmin <= kEps) && (tmax <= tio)) return tmax;
+    if ((tmin <= kEps) && (tmax >= tio)) return tio;
+    return tmax - tmin;
+}
+
+// box_chord_inside of one segment against two boxes A and B.  The segment terms (parallel
+// tests, length, the three reciprocal steps) are computed once; every result is the float
+// box_chord_inside returns for that box.
+__device__ __forceinline__ void box_chord_inside2(float xi, float yi, float zi, float xo, float yo,
+                                                  float zo, const float* a, const float* b,
+                                                  float& la, float& lb)
+{
+    const float dx = xo - xi, dy = yo - yi, dz = zo - zi;
+    if (fabsf(dy) < 0.001f) { la = 0.0f; lb = 0.0f; return; }
+    if (fabsf(dx) < kEps || fabsf(dz) < kEps) {
+        la = box_chord_parallel(xi, yi, zi, xo, yo, zo, a[0], a[1], a[2], a[3], a[4], a[5], 1);
+        lb = box_chord_parallel(xi, yi, zi, xo, yo, zo, b[0], b[1], b[2], b[3], b[4], b[5], 1);
+        return;
+    }
+    const float tio = sqrtf(dx * dx + dy * dy + dz * dz);
+    const float ix = tio / dx, iy = tio / dy, iz = tio / dz;
+    la = inside_from_slabs(xi, yi, zi, ix, iy, iz, tio, a[0], a[1], a[2], a[3], a[4], a[5]);
+    lb = inside_from_slabs(xi, yi, zi, ix, iy, iz, tio, b[0], b[1], b[2], b[3], b[4], b[5]);
+}
+
 // Chord through the y-parallel cylinder (x-xc)^2 + (z-zc)^2 <= r^2, y in [y1, y2]
 // (PESysMatGen.cu:688-799).
 __device__ __forceinline__ float cyl_chord(float xi, float yi, float zi, float xo, float yo,

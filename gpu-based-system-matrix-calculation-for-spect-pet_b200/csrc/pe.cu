@@ -45,6 +45,7 @@ constexpr float kMinDepth = 1.0f;       // mm; slope rectangles need objects thi
 struct WarpSmem {
     float4 rect[kChunk];
     int id[kChunk];                      // holes: hole index; crystals: n_holes + crystal
+    unsigned char layer[kChunk];         // layer of a hole entry (crystals: n_layers)
     unsigned short sub[kChunk];          // chunk entries overlapping the current round's rays
     float4 inner[kMaxLayers];            // plate "through both faces" slope rectangle
     float chain[32];
@@ -202,6 +203,7 @@ __device__ int build_chunk(const DevGeom& g, const BlockSmem& bs, WarpSmem& ws, 
             const int pos = n + __popc(m & ((1u << lane) - 1u));
             ws.rect[pos] = rect;
             ws.id[pos] = id;
+            ws.layer[pos] = (unsigned char)(id < g.n_holes ? layer_of_hole(g, id) : g.n_layers);
         }
         n += __popc(m);
         cursor += 32;
@@ -246,27 +248,95 @@ __device__ __forceinline__ int round_sublist(WarpSmem& ws, int n, float4 box, in
     return nr;
 }
 
+// Terms of the reference cylinder chord (PESysMatGen.cu:688-799) that depend only on the
+// ray (voxel -> sub-element) and on the cap planes y1, y2.  Hoisting them out of the
+// per-hole evaluation keeps every float identical: each is the same operation on the same
+// operands as in the per-hole formula.
+struct RayCyl {
+    float xi, yi, zi, tio, kx, ky, kz, rx, rz, kk;
+    float y1, y2;                // cap planes the cached terms below belong to
+    bool degenerate;             // |y1 - y2| < 0.001
+    float ta, tb, xl, xr, zl, zr;
+};
+
+__device__ __forceinline__ void ray_cyl_init(RayCyl& c, float xi, float yi, float zi, float xo, float yo,
+                                             float zo)
+{
+    const float dx = xo - xi, dy = yo - yi, dz = zo - zi;
+    c.xi = xi; c.yi = yi; c.zi = zi;
+    c.tio = sqrtf(dx * dx + dy * dy + dz * dz);
+    c.kx = dx / c.tio;
+    c.ky = dy / c.tio;
+    c.kz = dz / c.tio;
+    c.rx = c.kx / c.ky;
+    c.rz = c.kz / c.ky;
+    c.kk = c.kx * c.kx + c.kz * c.kz;
+    c.y1 = NAN;                  // no cap planes cached yet (NaN never compares equal)
+    c.y2 = NAN;
+}
+
+__device__ __forceinline__ void ray_cyl_caps(RayCyl& c, float y1, float y2)
+{
+    if (y1 == c.y1 && y2 == c.y2) return;
+    c.y1 = y1;
+    c.y2 = y2;
+    c.degenerate = fabsf(y1 - y2) < 0.001f;
+    c.xl = c.xi + c.rx * (y1 - c.yi);
+    c.xr = c.xi + c.rx * (y2 - c.yi);
+    c.zl = c.zi + c.rz * (y1 - c.yi);
+    c.zr = c.zi + c.rz * (y2 - c.yi);
+    c.ta = (y1 - c.yi) / c.ky;
+    c.tb = (y2 - c.yi) / c.ky;
+}
+
+// Cylinder chord of hole (xc, zc, r) with cap planes already cached in c.
+__device__ __forceinline__ float ray_cyl_chord(const RayCyl& c, float xc, float zc, float r)
+{
+    if (c.degenerate) return 0.0f;
+    const bool fl = (c.xl - xc) * (c.xl - xc) + (c.zl - zc) * (c.zl - zc) <= r * r;
+    const bool fr = (c.xr - xc) * (c.xr - xc) + (c.zr - zc) * (c.zr - zc) <= r * r;
+    if (fl && fr) {
+        if (c.ta <= 0.0001f || c.tb <= 0.0001f) return 0.0f;
+        if (c.ta >= c.tio || c.tb >= c.tio) return 0.0f;
+        return fabsf(c.tb - c.ta);
+    }
+    const float ox = c.xi - xc, oz = c.zi - zc;
+    const float disc = c.kk * r * r - (c.kx * oz - c.kz * ox) * (c.kx * oz - c.kz * ox);
+    if (disc <= 0.00001f) return 0.0f;
+    const float t1 = (-(c.kx * ox + c.kz * oz) - sqrtf(disc)) / c.kk;
+    const float t2 = (-(c.kx * ox + c.kz * oz) + sqrtf(disc)) / c.kk;
+    float ea, eb;
+    if (!fl && !fr) {
+        if (!(t1 >= c.ta && t2 <= c.tb)) return 0.0f;
+        ea = t1; eb = t2;
+    } else if (fl) { ea = c.ta; eb = t2; }
+    else           { ea = t1; eb = c.tb; }
+    if (eb <= 0.0001f || ea <= 0.0001f) return 0.0f;
+    if (eb >= c.tio || ea >= c.tio) return 0.0f;
+    return eb - ea;
+}
+
 // Walk the round's sub-list of kept objects for one sub-element ray (voxel -> (xD,yD,zD)).
 __device__ __forceinline__ void walk_chunk(const DevGeom& g, const WarpSmem& ws, int nr, const Elem& e,
                                            float xD, float yD, float zD, float sa_a, float sa_b,
-                                           float cosang, Walk& s)
+                                           float cosang, RayCyl& rc, Walk& s)
 {
     for (int j = 0; j < nr; ++j) {
         const int k = ws.sub[j];
+        const int m = ws.layer[k];
+        if (m != s.lay) close_layers(g, s, m, cosang);
+        if (!in_rect(ws.rect[k], sa_a, sa_b)) continue;
         const int id = ws.id[k];
-        if (id < g.n_holes) {
-            const int m = layer_of_hole(g, id);
-            if (m != s.lay) close_layers(g, s, m, cosang);
-            if (!in_rect(ws.rect[k], sa_a, sa_b)) continue;
+        if (m < g.n_layers) {
             const float4 ha = __ldg(&g.hole.a[id]);
-            const float4 hb = __ldg(&g.hole.b[id]);
-            const float tmp = cyl_chord(e.xI, e.yI, e.zI, xD, yD, zD, ha.x, ha.y, ha.z, ha.w, hb.x);
+            const float r = __ldg(&g.hole.b[id].x);
+            const float mu = __ldg(&g.hole.b[id].y);
+            ray_cyl_caps(rc, ha.y, ha.z);
+            const float tmp = ray_cyl_chord(rc, ha.x, ha.w, r);
             s.len = s.len + tmp;                                 // :1276-1278
-            s.att = s.att + hb.y * tmp;
+            s.att = s.att + mu * tmp;
             s.hole_hits += (tmp != 0.0f);
         } else {
-            if (s.lay < g.n_layers) close_layers(g, s, g.n_layers, cosang);
-            if (!in_rect(ws.rect[k], sa_a, sa_b)) continue;
             const int o = id - g.n_holes;
             const float4 po = __ldg(&g.cry.pos[o]);
             const float4 so = __ldg(&g.cry.size[o]);
@@ -340,10 +410,10 @@ __device__ __forceinline__ float finish_sub_element(const Elem& e, const SubElem
     const float uy2 = (((float)q.iy + 1.0f) / 16.0f - 0.5f) * t;
     const float uz1 = ((float)q.iz / 8.0f - 0.5f) * h;
     const float uz2 = (((float)q.iz + 1.0f) / 8.0f - 0.5f) * h;
-    const float l1 = box_chord_inside(e.xIs, e.yIs, e.zIs, q.xDs, q.yDs, q.zDs, -w / 2.0f, -t / 2.0f,
-                                      -h / 2.0f, w / 2.0f, t / 2.0f, h / 2.0f);
-    const float l2 = box_chord_inside(e.xIs, e.yIs, e.zIs, q.xDs, q.yDs, q.zDs, ux1, uy1, uz1, ux2,
-                                      uy2, uz2);
+    const float cbox[6] = {-w / 2.0f, -t / 2.0f, -h / 2.0f, w / 2.0f, t / 2.0f, h / 2.0f};
+    const float ubox[6] = {ux1, uy1, uz1, ux2, uy2, uz2};
+    float l1, l2;
+    box_chord_inside2(e.xIs, e.yIs, e.zIs, q.xDs, q.yDs, q.zDs, cbox, ubox, l1, l2);
     att = att + (l1 - l2) * e.mu_t;
     const float eff = 1.0f * expf(-att);
     const float xt = q.xDs + 1000.0f * (q.xDs - e.xIs) / q.sq;
@@ -413,9 +483,12 @@ __device__ float pe_element(const DevGeom& g, const BlockSmem& bs, WarpSmem& ws,
     float chain = 0.0f;
     double dacc = 0.0;
     int n_hole_hits = 0, n_cry_hits = 0, n_blocked = 0;
+    long long n_sub_entries = 0;
     for (int r = 0; r < 32; ++r) {
         const SubElem q = sub_element(e, r * 32 + lane);
         Walk s{0.0f, 0.0f, 0, 0, 0};
+        RayCyl rc;
+        ray_cyl_init(rc, e.xI, e.yI, e.zI, q.xD, q.yD, q.zD);
         const bool blocked = plate_penalty(g, ws, e, q, s.att);
         const bool skip = blocked && g.nonneg_mu;
         // slope box of the rays that still need the walk in this round
@@ -430,7 +503,8 @@ __device__ float pe_element(const DevGeom& g, const BlockSmem& bs, WarpSmem& ws,
         }
         if (single) {
             const int nr = round_sublist(ws, count, box, lane);
-            if (!skip) walk_chunk(g, ws, nr, e, q.xD, q.yD, q.zD, q.sa_a, q.sa_b, q.cosang, s);
+            if constexpr (COUNT) n_sub_entries += nr;
+            if (!skip) walk_chunk(g, ws, nr, e, q.xD, q.yD, q.zD, q.sa_a, q.sa_b, q.cosang, rc, s);
             __syncwarp();
         } else {
             // chunked walk: rebuild the chunks for this round (the warp stays converged)
@@ -439,7 +513,7 @@ __device__ float pe_element(const DevGeom& g, const BlockSmem& bs, WarpSmem& ws,
                 if (r > 0 || cur > 0) cur = build_chunk(g, bs, ws, e, d, cur, n_src, from_super, lane, &count);
                 else cur = cursor;
                 const int nr = round_sublist(ws, count, box, lane);
-                if (!skip) walk_chunk(g, ws, nr, e, q.xD, q.yD, q.zD, q.sa_a, q.sa_b, q.cosang, s);
+                if (!skip) walk_chunk(g, ws, nr, e, q.xD, q.yD, q.zD, q.sa_a, q.sa_b, q.cosang, rc, s);
                 __syncwarp();
             }
         }
@@ -476,6 +550,11 @@ __device__ float pe_element(const DevGeom& g, const BlockSmem& bs, WarpSmem& ws,
             atomicAdd(&counters[2], (unsigned long long)n_cry_hits);
             atomicAdd(&counters[3], 1ull);
             atomicAdd(&counters[4], (unsigned long long)n_blocked);
+            atomicAdd(&counters[5], single ? 0ull : 1ull);                 // chunked elements
+            atomicAdd(&counters[6], (unsigned long long)count);            // kept objects (1st chunk)
+            atomicAdd(&counters[7], (unsigned long long)n_sub_entries);    // round sub-list entries
+            atomicAdd(&counters[8], bs.s_count < 0 ? 1ull : 0ull);         // superset overflow
+            atomicAdd(&counters[9], (unsigned long long)(bs.s_count < 0 ? 0 : bs.s_count));
         }
     }
     if constexpr (MODE == 0) return chain;
