@@ -390,7 +390,7 @@ extern "C" SYSMAT_API int sysmat_pe_work(sysmat_ctx* ctx, float rotation, int de
         cudaMemsetAsync(ctx->d_counter, 0, sizeof(unsigned long long), s) != cudaSuccess ||
         cudaMemsetAsync(ctx->d_status, 0, sizeof(int), s) != cudaSuccess ||
         launch_pe(ctx->g, L, SYSMAT_MODE_REFERENCE, ctx->num_sms, s) ||
-        cudaMemcpyAsync(counts, d_cnt, 10 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, s) != cudaSuccess ||
+        cudaMemcpyAsync(counts, d_cnt, 12 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, s) != cudaSuccess ||
         cudaStreamSynchronize(s) != cudaSuccess)
         rc = SYSMAT_ERR_CUDA;
     cudaFree(d_cnt);

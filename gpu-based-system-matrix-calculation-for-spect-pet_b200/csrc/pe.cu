@@ -220,6 +220,8 @@ struct Walk {
     int lay;        // current layer
     int hole_hits;  // non-zero hole chords (work counters only)
     int cry_hits;   // non-zero crystal chords (work counters only)
+    int hole_evals; // hole chords evaluated (work counters only)
+    int cry_evals;  // crystal chords evaluated (work counters only)
 };
 
 __device__ __forceinline__ void close_layers(const DevGeom& g, Walk& s, int upto, float cosang)
@@ -336,6 +338,7 @@ __device__ __forceinline__ void walk_chunk(const DevGeom& g, const WarpSmem& ws,
             s.len = s.len + tmp;                                 // :1276-1278
             s.att = s.att + mu * tmp;
             s.hole_hits += (tmp != 0.0f);
+            ++s.hole_evals;
         } else {
             const int o = id - g.n_holes;
             const float4 po = __ldg(&g.cry.pos[o]);
@@ -349,6 +352,7 @@ __device__ __forceinline__ void walk_chunk(const DevGeom& g, const WarpSmem& ws,
                                        -0.5f * so.z, 0.5f * so.x, 0.5f * so.y, 0.5f * so.z);
             s.att = s.att + la * mo;
             s.cry_hits += (la != 0.0f);
+            ++s.cry_evals;
         }
     }
 }
@@ -482,11 +486,11 @@ __device__ float pe_element(const DevGeom& g, const BlockSmem& bs, WarpSmem& ws,
 
     float chain = 0.0f;
     double dacc = 0.0;
-    int n_hole_hits = 0, n_cry_hits = 0, n_blocked = 0;
+    int n_hole_hits = 0, n_cry_hits = 0, n_blocked = 0, n_hole_evals = 0, n_cry_evals = 0;
     long long n_sub_entries = 0;
     for (int r = 0; r < 32; ++r) {
         const SubElem q = sub_element(e, r * 32 + lane);
-        Walk s{0.0f, 0.0f, 0, 0, 0};
+        Walk s{0.0f, 0.0f, 0, 0, 0, 0, 0};
         RayCyl rc;
         ray_cyl_init(rc, e.xI, e.yI, e.zI, q.xD, q.yD, q.zD);
         const bool blocked = plate_penalty(g, ws, e, q, s.att);
@@ -525,6 +529,8 @@ __device__ float pe_element(const DevGeom& g, const BlockSmem& bs, WarpSmem& ws,
         if constexpr (COUNT) {
             n_hole_hits += s.hole_hits;
             n_cry_hits += s.cry_hits;
+            n_hole_evals += s.hole_evals;
+            n_cry_evals += s.cry_evals;
             n_blocked += skip;
         }
         if constexpr (MODE == 0) {
@@ -543,6 +549,8 @@ __device__ float pe_element(const DevGeom& g, const BlockSmem& bs, WarpSmem& ws,
             n_hole_hits += __shfl_xor_sync(0xffffffffu, n_hole_hits, off);
             n_cry_hits += __shfl_xor_sync(0xffffffffu, n_cry_hits, off);
             n_blocked += __shfl_xor_sync(0xffffffffu, n_blocked, off);
+            n_hole_evals += __shfl_xor_sync(0xffffffffu, n_hole_evals, off);
+            n_cry_evals += __shfl_xor_sync(0xffffffffu, n_cry_evals, off);
         }
         if (lane == 0) {
             atomicAdd(&counters[0], 1024ull);
@@ -555,6 +563,8 @@ __device__ float pe_element(const DevGeom& g, const BlockSmem& bs, WarpSmem& ws,
             atomicAdd(&counters[7], (unsigned long long)n_sub_entries);    // round sub-list entries
             atomicAdd(&counters[8], bs.s_count < 0 ? 1ull : 0ull);         // superset overflow
             atomicAdd(&counters[9], (unsigned long long)(bs.s_count < 0 ? 0 : bs.s_count));
+            atomicAdd(&counters[10], (unsigned long long)n_hole_evals);
+            atomicAdd(&counters[11], (unsigned long long)n_cry_evals);
         }
     }
     if constexpr (MODE == 0) return chain;

@@ -204,11 +204,12 @@ class Context:
         det_count = self.n_det - det_begin if det_count is None else det_count
         vox_count = self.n_vox - vox_begin if vox_count is None else vox_count
         ld = out.stride(0) if out.dim() == 2 else vox_count
-        c = (ctypes.c_ulonglong * 10)()
+        c = (ctypes.c_ulonglong * 12)()
         _check(lib().sysmat_pe_work(self.handle, float(rotation), det_begin, det_count, vox_begin,
                                     vox_count, _ptr(out), ld, c, _stream(stream)), "sysmat_pe_work")
         keys = ("subelements", "hole_hits", "crystal_hits", "elements", "blocked", "chunked",
-                "kept", "sublist_entries", "superset_overflow", "superset_sum")
+                "kept", "sublist_entries", "superset_overflow", "superset_sum", "hole_evals",
+                "crystal_evals")
         return dict(zip(keys, (int(x) for x in c)))
 
     def bitmap_crystal(self, stream=None):
@@ -252,3 +253,4 @@ def measure_peaks():
     f, m = ctypes.c_double(), ctypes.c_double()
     _check(lib().sysmat_measure_peaks(ctypes.byref(f), ctypes.byref(m)), "sysmat_measure_peaks")
     return f.value, m.value
+

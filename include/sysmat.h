@@ -130,12 +130,12 @@ SYSMAT_API int sysmat_scatter(sysmat_ctx* ctx, int parts, int hole_model, float 
 /* ---------------------------------------------------------------------------------- */
 /* Diagnostics (benchmark roofline).                                                     */
 
-/* Same block as sysmat_pe (reference summation) with work counters (10 values):
+/* Same block as sysmat_pe (reference summation) with work counters (12 values):
  * counts[0] sub-elements evaluated, [1] hole chords that are non-zero, [2] crystal chords
  * that are non-zero, [3] elements, [4] sub-elements stopped by the plate-bypass penalty,
  * [5] elements walked in several chunks, [6] kept candidate objects, [7] round sub-list
  * entries, [8] work items whose candidate superset overflowed shared memory, [9] summed
- * superset sizes.  Synchronous. */
+ * superset sizes, [10] hole chords evaluated, [11] crystal chords evaluated.  Synchronous. */
 SYSMAT_API int sysmat_pe_work(sysmat_ctx* ctx, float rotation, int det_begin, int det_count,
                               long long vox_begin, long long vox_count, float* d_out, long long ld,
                               unsigned long long* counts, void* stream);
