@@ -137,6 +137,14 @@ bool same_device(const sysmat_ctx* ctx)
 
 }  // namespace
 
+// Parameter decoding for other translation units of the library (see noalloc.cu).
+namespace sysmat {
+int sysmat_decode_geometry(const float* pC, const float* pD, const float* pI, DevGeom& g, int& n_holes0)
+{
+    return decode(pC, pD, pI, g, n_holes0);
+}
+}  // namespace sysmat
+
 extern "C" SYSMAT_API const char* sysmat_error_string(int code)
 {
     switch (code) {

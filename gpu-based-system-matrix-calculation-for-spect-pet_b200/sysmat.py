@@ -30,7 +30,8 @@ HOLE_MODEL_VARIANT = 1
 EXPORTS = ("PESysMatGen", "scatter", "scatter_collimator", "scatter_crystal", "sysmat_create",
            "sysmat_destroy", "sysmat_dims", "sysmat_pe", "sysmat_bitmap_crystal_words",
            "sysmat_bitmap_collimator_words", "sysmat_bitmap_crystal", "sysmat_bitmap_collimator",
-           "sysmat_scatter_prepare", "sysmat_scatter", "sysmat_pe_work", "sysmat_measure_peaks",
+           "sysmat_scatter_prepare", "sysmat_scatter", "sysmat_pe_noalloc", "sysmat_pe_work",
+           "sysmat_measure_peaks",
            "sysmat_error_string", "sysmat_version")
 
 _fp = ctypes.POINTER(ctypes.c_float)
@@ -79,6 +80,9 @@ def lib():
                                 ctypes.POINTER(ctypes.c_ulonglong), _vp], ctypes.c_int),
             "sysmat_measure_peaks": ([ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double)],
                                      ctypes.c_int),
+            "sysmat_pe_noalloc": ([_fp, _fp, _fp, ctypes.c_float, ctypes.c_int, ctypes.c_int,
+                                   ctypes.c_longlong, ctypes.c_longlong, _vp, ctypes.c_longlong,
+                                   ctypes.c_int, _vp], ctypes.c_int),
             "sysmat_error_string": ([ctypes.c_int], ctypes.c_char_p),
             "sysmat_version": ([], ctypes.c_char_p),
         }
@@ -254,3 +258,18 @@ def measure_peaks():
     _check(lib().sysmat_measure_peaks(ctypes.byref(f), ctypes.byref(m)), "sysmat_measure_peaks")
     return f.value, m.value
 
+
+def pe_noalloc(geo, out, rotation=0.0, det_begin=0, det_count=None, vox_begin=0, vox_count=None,
+               mode=MODE_REFERENCE, stream=None):
+    """Photoelectric block through sysmat_pe_noalloc (no device allocation; host parameter
+    arrays, `out` a CUDA float32 tensor).  Returns `out`."""
+    (c, pc), (d, pd), (i, pi) = _f32(geo.collimator), _f32(geo.detector), _f32(geo.image)
+    n_det = int(np.floor(float(geo.detector[0]) + 1e-4))
+    n_vox = geo.n_vox
+    det_count = n_det - det_begin if det_count is None else det_count
+    vox_count = n_vox - vox_begin if vox_count is None else vox_count
+    ld = out.stride(0) if out.dim() == 2 else vox_count
+    _check(lib().sysmat_pe_noalloc(pc, pd, pi, float(rotation), det_begin, det_count, vox_begin,
+                                   vox_count, _ptr(out), ld, mode, _stream(stream)),
+           "sysmat_pe_noalloc")
+    return out

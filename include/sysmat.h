@@ -127,6 +127,21 @@ SYSMAT_API int sysmat_scatter(sysmat_ctx* ctx, int parts, int hole_model, float 
                               const float* d_pe, int det_begin, int det_count, long long vox_begin,
                               long long vox_count, float* d_out, long long ld, void* stream);
 
+/* Photoelectric block like sysmat_pe, for callers that cannot allocate device memory when
+ * they call (for example a host that gives all device memory to its own pool at start-up,
+ * or a plug-in host that forbids allocation after initialisation).  No counterpart in the
+ * reference.  pC/pD/pI are host arrays of 80000/80000/100 floats; d_out is device memory
+ * of det_count rows with stride ld.  Nothing is allocated: the parameter copies, derived
+ * tables, work counter and status word live in a static device array of about 1.6 MB
+ * (each GPU that loads the library holds it until exit), limited to 6666 crystals and 8877
+ * holes (larger systems return SYSMAT_ERR_CAPACITY).  The first call on a device looks
+ * up that array's device address and should come before any stream capture.  Calls
+ * share the array: calls that overlap on the GPU race.  Synchronous on `stream`. */
+SYSMAT_API int sysmat_pe_noalloc(const float* pC, const float* pD, const float* pI, float rotation,
+                                 int det_begin, int det_count, long long vox_begin,
+                                 long long vox_count, float* d_out, long long ld, int mode,
+                                 void* stream);
+
 /* ---------------------------------------------------------------------------------- */
 /* Diagnostics (benchmark roofline).                                                     */
 
