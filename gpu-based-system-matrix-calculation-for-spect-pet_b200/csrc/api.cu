@@ -54,6 +54,8 @@ struct sysmat_ctx {
     int prepared_parts = 0;
     PairRec* pairs = nullptr;
     AttEntry* att = nullptr;
+    double* d_kn_tab = nullptr;     // Klein-Nishina table for kn_e0
+    float kn_e0 = -1.0f;
 };
 
 namespace {
@@ -227,6 +229,7 @@ extern "C" SYSMAT_API int sysmat_destroy(sysmat_ctx* ctx)
 {
     if (!ctx) return SYSMAT_OK;
     scatter_scratch_free(ctx->scratch);
+    cudaFree(ctx->d_kn_tab);
     cudaFree(ctx->d_det);
     cudaFree(ctx->d_col);
     cudaFree(ctx->d_img);
@@ -369,6 +372,20 @@ extern "C" SYSMAT_API int sysmat_scatter(sysmat_ctx* ctx, int parts, int hole_mo
     L.pairs = ctx->pairs;
     L.att = ctx->att;
     L.out = d_out;
+    if (!ctx->d_kn_tab || ctx->kn_e0 != ph.e0) {     // (re)build the FP64 Klein-Nishina table
+        std::vector<double> tab(3 * (size_t)(kKnTable + 1));
+        kn_table_build((double)ph.e0, tab.data());
+        if (!ctx->d_kn_tab &&
+            cudaMalloc(&ctx->d_kn_tab, sizeof(double) * tab.size()) != cudaSuccess) {
+            ctx->d_kn_tab = nullptr;
+            return SYSMAT_ERR_NOMEM;
+        }
+        CUDA_TRY(cudaMemcpyAsync(ctx->d_kn_tab, tab.data(), sizeof(double) * tab.size(),
+                                 cudaMemcpyHostToDevice, (cudaStream_t)stream));
+        CUDA_TRY(cudaStreamSynchronize((cudaStream_t)stream));
+        ctx->kn_e0 = ph.e0;
+    }
+    L.kn_tab = ctx->d_kn_tab;
     return launch_scatter(ctx->g, ph, L, (cudaStream_t)stream) ? SYSMAT_ERR_CUDA : SYSMAT_OK;
 }
 

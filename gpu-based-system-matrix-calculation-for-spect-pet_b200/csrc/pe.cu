@@ -38,17 +38,24 @@ constexpr int kWarps = 8;
 constexpr int kThreads = kWarps * 32;
 constexpr int kSuperCap = 1024;         // block superset capacity (objects)
 constexpr int kChunk = 256;             // per-warp kept-object chunk
+constexpr int kRound = 64;              // per-warp round buffer
 constexpr int kBx = 4, kBy = 4, kBz = 2;
 constexpr float kSlopeMargin = 2e-4f;   // slope units; >> FP32 position error / depth
 constexpr float kMinDepth = 1.0f;       // mm; slope rectangles need objects this far behind
 
 struct WarpSmem {
+    // kept objects of the element (reference cone test + bundle filter), reference order
     float4 rect[kChunk];
     int id[kChunk];                      // holes: hole index; crystals: n_holes + crystal
-    unsigned char layer[kChunk];         // layer of a hole entry (crystals: n_layers)
-    unsigned short sub[kChunk];          // chunk entries overlapping the current round's rays
+    // the current round's objects (kept objects whose rectangle meets the round's rays),
+    // with their geometry, so the walk reads contiguous shared memory:
+    //   hole:    A = (x, z, R, mu),   B = (y1, y2, -, -)
+    //   crystal: A = (x, y, z, mu),   B = (cos(-rot), sin(-rot), w, t),
+    //            C = (h, voxel x, y, z in the crystal's frame)
+    float4 rr[kRound], ra[kRound], rb[kRound], rc[kRound];
+    int rl[kRound];                      // layer of a hole entry; n_layers for crystals
     float4 inner[kMaxLayers];            // plate "through both faces" slope rectangle
-    float chain[32];
+    float chain[256];                    // contributions of sub-elements 256p .. 256p+255
 };
 
 struct BlockSmem {
@@ -203,7 +210,6 @@ __device__ int build_chunk(const DevGeom& g, const BlockSmem& bs, WarpSmem& ws, 
             const int pos = n + __popc(m & ((1u << lane) - 1u));
             ws.rect[pos] = rect;
             ws.id[pos] = id;
-            ws.layer[pos] = (unsigned char)(id < g.n_holes ? layer_of_hole(g, id) : g.n_layers);
         }
         n += __popc(m);
         cursor += 32;
@@ -232,22 +238,6 @@ __device__ __forceinline__ void close_layers(const DevGeom& g, Walk& s, int upto
         s.len = 0.0f;
         ++s.lay;
     }
-}
-
-// Indices of the chunk entries whose slope rectangle overlaps the bounding box of the 32
-// rays of this round; order is preserved.  Returns the count.
-__device__ __forceinline__ int round_sublist(WarpSmem& ws, int n, float4 box, int lane)
-{
-    int nr = 0;
-    for (int base = 0; base < n; base += 32) {
-        const int k = base + lane;
-        const bool keep = k < n && rects_overlap(ws.rect[k], box);
-        const unsigned m = __ballot_sync(0xffffffffu, keep);
-        if (keep) ws.sub[nr + __popc(m & ((1u << lane) - 1u))] = (unsigned short)k;
-        nr += __popc(m);
-    }
-    __syncwarp();
-    return nr;
 }
 
 // Terms of the reference cylinder chord (PESysMatGen.cu:688-799) that depend only on the
@@ -318,42 +308,125 @@ __device__ __forceinline__ float ray_cyl_chord(const RayCyl& c, float xc, float 
     return eb - ea;
 }
 
-// Walk the round's sub-list of kept objects for one sub-element ray (voxel -> (xD,yD,zD)).
-__device__ __forceinline__ void walk_chunk(const DevGeom& g, const WarpSmem& ws, int nr, const Elem& e,
+// Slope-space shadow of a y-aligned object (hole cylinder, or crystal in the disk around its
+// xz footprint) seen from the voxel: every line from the voxel that meets the object at a
+// depth y in [y0, y1] has slopes within rho(y) = R/(y - yI) of the point c(y) on the
+// segment c(y0) -> c(y1), so within rho(y0) of that segment.  capsule_meets_box is false
+// only when that capsule (radius inflated by the slope margin) is separated from the box
+// along x, along z, or along the segment's normal; decided without divisions.
+__device__ __forceinline__ bool capsule_meets_box(float xo, float zo, float y0, float y1, float R,
+                                                  const Elem& e, float4 box)
+{
+    const float r0 = __frcp_rn(y0 - e.yI), r1 = __frcp_rn(y1 - e.yI);
+    const float ax = (xo - e.xI) * r0, az = (zo - e.zI) * r0;
+    const float bx = (xo - e.xI) * r1, bz = (zo - e.zI) * r1;
+    const float rho = R * r0 * 1.0001f + kSlopeMargin;
+    if (fminf(ax, bx) - rho > box.y || fmaxf(ax, bx) + rho < box.x) return false;
+    if (fminf(az, bz) - rho > box.w || fmaxf(az, bz) + rho < box.z) return false;
+    const float dx = bx - ax, dz = bz - az;
+    const float mx = 0.5f * (box.x + box.y) - ax, mz = 0.5f * (box.z + box.w) - az;
+    const float sep = fabsf(dx * mz - dz * mx) - (fabsf(dz) * 0.5f * (box.y - box.x) +
+                                                  fabsf(dx) * 0.5f * (box.w - box.z));
+    return !(sep > 0.0f && sep * sep > rho * rho * (dx * dx + dz * dz));
+}
+
+// Copy kept entries [k0, k1) whose rectangle and capsule meet the round's slope box into
+// the round buffer from position n, with their geometry (one entry per lane); returns the
+// new count.  Stops before the buffer could overflow; *next receives the first entry not
+// examined.
+__device__ __forceinline__ int fill_round(const DevGeom& g, WarpSmem& ws, const Elem& e, int k0, int k1,
+                                          float4 box, int n, int lane, int* next, int* nh)
+{
+    int k = k0;
+    while (k < k1 && n <= kRound - 32) {
+        const int kk = k + lane;
+        bool keep = false;
+        int id = 0;
+        float4 rect;
+        if (kk < k1) {
+            rect = ws.rect[kk];
+            keep = rects_overlap(rect, box);
+            if (keep && !isinf(rect.x)) {                  // finite: object wholly behind the voxel
+                id = ws.id[kk];
+                if (id < g.n_holes) {
+                    const float4 ha = __ldg(&g.hole.a[id]);
+                    keep = capsule_meets_box(ha.x, ha.w, ha.y, ha.z, __ldg(&g.hole.b[id].x), e, box);
+                } else {
+                    const int o = id - g.n_holes;
+                    const float4 po = __ldg(&g.cry.pos[o]);
+                    const float4 so = __ldg(&g.cry.size[o]);
+                    keep = capsule_meets_box(po.x, po.z, po.y - 0.5f * so.y, po.y + 0.5f * so.y,
+                                             0.5f * sqrtf(so.x * so.x + so.z * so.z), e, box);
+                }
+            }
+        }
+        const unsigned m = __ballot_sync(0xffffffffu, keep);
+        if (keep) id = ws.id[kk];
+        *nh += __popc(__ballot_sync(0xffffffffu, keep && id < g.n_holes));
+        if (keep) {
+            const int pos = n + __popc(m & ((1u << lane) - 1u));
+            ws.rr[pos] = rect;
+            if (id < g.n_holes) {
+                const float4 ha = __ldg(&g.hole.a[id]);
+                const float4 hb = __ldg(&g.hole.b[id]);
+                ws.ra[pos] = make_float4(ha.x, ha.w, hb.x, hb.y);
+                ws.rb[pos] = make_float4(ha.y, ha.z, 0.0f, 0.0f);
+                ws.rl[pos] = layer_of_hole(g, id);
+            } else {
+                const int o = id - g.n_holes;
+                const float4 po = __ldg(&g.cry.pos[o]);
+                const float4 so = __ldg(&g.cry.size[o]);
+                const float4 to = __ldg(&g.cry.trig[o]);
+                float xa, ya, za;                                   // :1305-1307
+                to_crystal_frame(po.x, po.y, po.z, to.z, to.w, e.xI, e.yI, e.zI, xa, ya, za);
+                ws.ra[pos] = make_float4(po.x, po.y, po.z, __ldg(&g.cry.mu[o].x));
+                ws.rb[pos] = make_float4(to.z, to.w, so.x, so.y);
+                ws.rc[pos] = make_float4(so.z, xa, ya, za);
+                ws.rl[pos] = g.n_layers;
+            }
+        }
+        n += __popc(m);
+        k += 32;
+    }
+    __syncwarp();
+    *next = k < k1 ? k : k1;
+    return n;
+}
+
+// Walk round-buffer entries [0, nr) for one sub-element ray (voxel -> (xD, yD, zD)); holes
+// occupy [0, nh) and crystals [nh, nr), both in the reference's object order; the layer
+// terms are added when the walk leaves a layer.
+__device__ __forceinline__ void walk_round(const DevGeom& g, const WarpSmem& ws, int nh, int nr,
                                            float xD, float yD, float zD, float sa_a, float sa_b,
                                            float cosang, RayCyl& rc, Walk& s)
 {
-    for (int j = 0; j < nr; ++j) {
-        const int k = ws.sub[j];
-        const int m = ws.layer[k];
+    for (int j = 0; j < nh; ++j) {
+        const int m = ws.rl[j];
         if (m != s.lay) close_layers(g, s, m, cosang);
-        if (!in_rect(ws.rect[k], sa_a, sa_b)) continue;
-        const int id = ws.id[k];
-        if (m < g.n_layers) {
-            const float4 ha = __ldg(&g.hole.a[id]);
-            const float r = __ldg(&g.hole.b[id].x);
-            const float mu = __ldg(&g.hole.b[id].y);
-            ray_cyl_caps(rc, ha.y, ha.z);
-            const float tmp = ray_cyl_chord(rc, ha.x, ha.w, r);
-            s.len = s.len + tmp;                                 // :1276-1278
-            s.att = s.att + mu * tmp;
-            s.hole_hits += (tmp != 0.0f);
-            ++s.hole_evals;
-        } else {
-            const int o = id - g.n_holes;
-            const float4 po = __ldg(&g.cry.pos[o]);
-            const float4 so = __ldg(&g.cry.size[o]);
-            const float4 to = __ldg(&g.cry.trig[o]);
-            const float mo = __ldg(&g.cry.mu[o].x);
-            float xa, ya, za, xb, yb, zb;                        // :1295-1323
-            to_crystal_frame(po.x, po.y, po.z, to.z, to.w, e.xI, e.yI, e.zI, xa, ya, za);
-            to_crystal_frame(po.x, po.y, po.z, to.z, to.w, xD, yD, zD, xb, yb, zb);
-            const float la = box_chord(xa, ya, za, xb, yb, zb, -0.5f * so.x, -0.5f * so.y,
-                                       -0.5f * so.z, 0.5f * so.x, 0.5f * so.y, 0.5f * so.z);
-            s.att = s.att + la * mo;
-            s.cry_hits += (la != 0.0f);
-            ++s.cry_evals;
-        }
+        if (!in_rect(ws.rr[j], sa_a, sa_b)) continue;
+        const float4 A = ws.ra[j];
+        const float4 B = ws.rb[j];
+        ray_cyl_caps(rc, B.x, B.y);
+        const float tmp = ray_cyl_chord(rc, A.x, A.y, A.z);
+        s.len = s.len + tmp;                                     // :1276-1278
+        s.att = s.att + A.w * tmp;
+        s.hole_hits += (tmp != 0.0f);
+        ++s.hole_evals;
+    }
+    if (nr <= nh) return;
+    if (s.lay < g.n_layers) close_layers(g, s, g.n_layers, cosang);
+    for (int j = nh; j < nr; ++j) {
+        if (!in_rect(ws.rr[j], sa_a, sa_b)) continue;
+        const float4 A = ws.ra[j];
+        const float4 B = ws.rb[j];
+        const float4 C = ws.rc[j];
+        float xb, yb, zb;                                        // :1318-1320
+        to_crystal_frame(A.x, A.y, A.z, B.x, B.y, xD, yD, zD, xb, yb, zb);
+        const float la = box_chord(C.y, C.z, C.w, xb, yb, zb, -0.5f * B.z, -0.5f * B.w, -0.5f * C.x,
+                                   0.5f * B.z, 0.5f * B.w, 0.5f * C.x);
+        s.att = s.att + la * A.w;
+        s.cry_hits += (la != 0.0f);
+        ++s.cry_evals;
     }
 }
 
@@ -488,8 +561,13 @@ __device__ float pe_element(const DevGeom& g, const BlockSmem& bs, WarpSmem& ws,
     double dacc = 0.0;
     int n_hole_hits = 0, n_cry_hits = 0, n_blocked = 0, n_hole_evals = 0, n_cry_evals = 0;
     long long n_sub_entries = 0;
+    // Round r covers sub-elements iz in {2p, 2p+1}, all 8 ix, iy in {2u, 2u+1} (p = r/8,
+    // u = r%8): a compact patch of the crystal, so a small slope box.  The 8 rounds of one p
+    // cover the reference indices s = 256p .. 256p+255, summed in index order after them.
     for (int r = 0; r < 32; ++r) {
-        const SubElem q = sub_element(e, r * 32 + lane);
+        const int sidx = ((r >> 3) * 2 + (lane >> 4)) * 128 + ((lane >> 1) & 7) * 16 + (r & 7) * 2 +
+                         (lane & 1);
+        const SubElem q = sub_element(e, sidx);
         Walk s{0.0f, 0.0f, 0, 0, 0, 0, 0};
         RayCyl rc;
         ray_cyl_init(rc, e.xI, e.yI, e.zI, q.xD, q.yD, q.zD);
@@ -505,21 +583,29 @@ __device__ float pe_element(const DevGeom& g, const BlockSmem& bs, WarpSmem& ws,
             box.z = fminf(box.z, __shfl_xor_sync(0xffffffffu, box.z, off));
             box.w = fmaxf(box.w, __shfl_xor_sync(0xffffffffu, box.w, off));
         }
-        if (single) {
-            const int nr = round_sublist(ws, count, box, lane);
-            if constexpr (COUNT) n_sub_entries += nr;
-            if (!skip) walk_chunk(g, ws, nr, e, q.xD, q.yD, q.zD, q.sa_a, q.sa_b, q.cosang, rc, s);
-            __syncwarp();
-        } else {
-            // chunked walk: rebuild the chunks for this round (the warp stays converged)
-            int cur = 0;
-            while (cur < n_src) {
-                if (r > 0 || cur > 0) cur = build_chunk(g, bs, ws, e, d, cur, n_src, from_super, lane, &count);
+        // walk this round's objects: kept entries meeting the round box, copied with their
+        // geometry into the round buffer; an overfull round is walked in pieces (the walk
+        // state of each lane carries over, so the attenuation order is unchanged)
+        int cur = 0;
+        bool first_chunk = true;
+        while (true) {
+            if (!single && !first_chunk) {
+                cur = build_chunk(g, bs, ws, e, d, cur, n_src, from_super, lane, &count);
+            } else if (!single) {
+                if (r > 0) cur = build_chunk(g, bs, ws, e, d, 0, n_src, from_super, lane, &count);
                 else cur = cursor;
-                const int nr = round_sublist(ws, count, box, lane);
-                if (!skip) walk_chunk(g, ws, nr, e, q.xD, q.yD, q.zD, q.sa_a, q.sa_b, q.cosang, rc, s);
-                __syncwarp();
             }
+            first_chunk = false;
+            int k = 0;
+            while (k < count) {
+                int next = count, nh = 0;
+                const int nr = fill_round(g, ws, e, k, count, box, 0, lane, &next, &nh);
+                if constexpr (COUNT) n_sub_entries += nr;
+                if (!skip) walk_round(g, ws, nh, nr, q.xD, q.yD, q.zD, q.sa_a, q.sa_b, q.cosang, rc, s);
+                __syncwarp();
+                k = next;
+            }
+            if (single || cur >= n_src) break;
         }
         float contrib = 0.0f;
         if (!skip) {
@@ -534,11 +620,13 @@ __device__ float pe_element(const DevGeom& g, const BlockSmem& bs, WarpSmem& ws,
             n_blocked += skip;
         }
         if constexpr (MODE == 0) {
-            ws.chain[lane] = contrib;
-            __syncwarp();
-#pragma unroll
-            for (int k = 0; k < 32; ++k) chain = chain + ws.chain[k];
-            __syncwarp();
+            ws.chain[sidx & 255] = contrib;
+            if ((r & 7) == 7) {
+                __syncwarp();
+#pragma unroll 16
+                for (int k = 0; k < 256; ++k) chain = chain + ws.chain[k];
+                __syncwarp();
+            }
         } else {
             dacc += (double)contrib;
         }
@@ -567,10 +655,13 @@ __device__ float pe_element(const DevGeom& g, const BlockSmem& bs, WarpSmem& ws,
             atomicAdd(&counters[11], (unsigned long long)n_cry_evals);
         }
     }
-    if constexpr (MODE == 0) return chain;
+    if constexpr (MODE == 0) {
+        return chain;
+    } else {
 #pragma unroll
-    for (int off = 16; off > 0; off >>= 1) dacc += __shfl_xor_sync(0xffffffffu, dacc, off);
-    return (float)dacc;
+        for (int off = 16; off > 0; off >>= 1) dacc += __shfl_xor_sync(0xffffffffu, dacc, off);
+        return (float)dacc;
+    }
 }
 
 // Block superset of the reference cone test over all voxels within radius rho of

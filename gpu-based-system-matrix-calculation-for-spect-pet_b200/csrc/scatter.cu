@@ -23,6 +23,8 @@
 //  * one thread per matrix element (d, v); a block shares d, so pair records are staged in
 //    shared memory and attenuator lists are broadcast loads; each element sums its items in
 //    FP64 (the reference adds float items with atomicAdd in an unspecified order).
+#include <cmath>
+
 #include <cub/cub.cuh>
 
 #include "scatter.cuh"
@@ -114,6 +116,41 @@ __device__ float kn_sum(float a, int n, float alpha)
         }
     }
     return integral + 0.5f * h * (fa + fb) + (h * h / 12.0f) * (kn_fprime(b, alpha) - kn_fprime(a, alpha));
+}
+
+// Reference Riemann sum with n + 1 terms from a, step 0.01f, in FP64 from the table:
+//   sum = G(b) - G(a) + h/2 (F(a) + F(b)) + h^2/12 (F'(b) - F'(a)),  b = a + n h,
+// G and F by cubic Hermite interpolation on the table (error ~1e-14), F' linearly.
+__device__ __forceinline__ void kn_tab_eval(const double* __restrict__ tab, double th, double& G,
+                                            double& F, double& Fp)
+{
+    const double hc = 3.14159265358979323846 / kKnTable;
+    double x = th / hc;
+    int i = (int)x;
+    i = i < 0 ? 0 : (i > kKnTable - 1 ? kKnTable - 1 : i);
+    const double t = x - (double)i;
+    const double t2 = t * t, t3 = t2 * t;
+    const double h00 = 2.0 * t3 - 3.0 * t2 + 1.0, h10 = t3 - 2.0 * t2 + t;
+    const double h01 = -2.0 * t3 + 3.0 * t2, h11 = t3 - t2;
+    const double* Gt = tab;
+    const double* Ft = tab + (kKnTable + 1);
+    const double* Pt = tab + 2 * (kKnTable + 1);
+    const double g0 = __ldg(&Gt[i]), g1 = __ldg(&Gt[i + 1]);
+    const double f0 = __ldg(&Ft[i]), f1 = __ldg(&Ft[i + 1]);
+    const double p0 = __ldg(&Pt[i]), p1 = __ldg(&Pt[i + 1]);
+    G = h00 * g0 + h10 * hc * f0 + h01 * g1 + h11 * hc * f1;
+    F = h00 * f0 + h10 * hc * p0 + h01 * f1 + h11 * hc * p1;
+    Fp = (1.0 - t) * p0 + t * p1;
+}
+
+__device__ __forceinline__ double kn_sum_tab(float a, int n, const double* __restrict__ tab)
+{
+    const double h = (double)0.01f;
+    const double ad = (double)a, bd = ad + (double)n * h;
+    double Ga, Fa, Pa, Gb, Fb, Pb;
+    kn_tab_eval(tab, ad, Ga, Fa, Pa);
+    kn_tab_eval(tab, bd, Gb, Fb, Pb);
+    return (Gb - Ga) + 0.5 * h * (Fa + Fb) + (h * h / 12.0) * (Pb - Pa);
 }
 
 __device__ __forceinline__ float window_prob(float e, float res, float lo, float hi)
@@ -355,7 +392,8 @@ struct ElemConst {
 // One (d, v, s) item; w_s is the interaction weight (PE * muC/muPE or hole solid angle *
 // muC/mu of layer 0).  Returns the float the reference would atomically add.
 __device__ float scatter_item(const ElemConst& e, const PairRec& pr, const AttEntry* __restrict__ att,
-                              float xs, float ys, float zs, float w_s, float e0, float integ)
+                              float xs, float ys, float zs, float w_s, float e0, float integ,
+                              const double* __restrict__ kn_tab)
 {
     const float cone = cone_angle(e.xI, e.yI, e.zI, xs, ys, zs, e.q.xD, e.q.yD, e.q.zD);
     const float es = e0 / (1.0f + (e0 / 511.0f) * (1.0f - cosf(cone)));     // :1016-1023
@@ -394,14 +432,21 @@ __device__ float scatter_item(const ElemConst& e, const PairRec& pr, const AttEn
     }
     if (lthr > 0.001f) tmin = 0.0f;
     const int n = (int)((tmax - tmin) / 0.01f);
-    const float ratio = kn_sum(tmin, n, e0 / 511.0f) / integ;
+    const float ratio = (float)kn_sum_tab(tmin, n, kn_tab) / integ;
     // attenuation by the flagged crystals at the scattered energy (:1369-1396)
+    // the scaled coefficient depends only on the attenuator's (mu_pe, mu_c) and E': it is
+    // recomputed only when those change along the list (same operands, same float)
     float a_sum = 0.0f;
+    float c_pe = NAN, c_c = NAN, mt = 0.0f;
     for (int k = 0; k < pr.att_count; ++k) {
         const AttEntry ae = att[pr.att_begin + k];
-        const float mpe = ae.mu_pe * e0 * e0 * e0 / es / es / es;
-        const float mc = ae.mu_c * e0 / es;
-        const float mt = mpe + mc;
+        if (!(ae.mu_pe == c_pe && ae.mu_c == c_c)) {
+            c_pe = ae.mu_pe;
+            c_c = ae.mu_c;
+            const float mpe = ae.mu_pe * e0 * e0 * e0 / es / es / es;
+            const float mc = ae.mu_c * e0 / es;
+            mt = mpe + mc;
+        }
         a_sum = a_sum + ae.len * mt;
     }
     const float mpe_s = e.mu_pe * e0 * e0 * e0 / es / es / es;              // :1411-1417
@@ -466,7 +511,7 @@ scatter_kernel(DevGeom g, ScatterPhysics ph, ScatterLaunch L)
                 if (w_s == 0.0f) continue;          // the item is exactly 0
                 const float4 ps = __ldg(&g.cry.pos[s]);
                 xs = ps.x; ys = ps.y; zs = ps.z;
-                acc_c += (double)scatter_item(e, pr, L.att, xs, ys, zs, w_s, ph.e0, ph.integ);
+                acc_c += (double)scatter_item(e, pr, L.att, xs, ys, zs, w_s, ph.e0, ph.integ, L.kn_tab);
             } else {
                 const float4 hr = __ldg(&g.hole.raw[s - g.n_det]);
                 xs = hr.x;
@@ -484,7 +529,7 @@ scatter_kernel(DevGeom g, ScatterPhysics ph, ScatterLaunch L)
                     sa = (vr * vr + (hr.z - hr.y) * vr) / (4.0f * lih * lih);
                 }
                 w_s = sa / ph.col_mu_tot0 * ph.col_mu_c0;                // :1716
-                acc_h += (double)scatter_item(e, pr, L.att, xs, ys, zs, w_s, ph.e0, ph.integ);
+                acc_h += (double)scatter_item(e, pr, L.att, xs, ys, zs, w_s, ph.e0, ph.integ, L.kn_tab);
             }
         }
     }
@@ -582,6 +627,44 @@ int launch_scatter(const DevGeom& g, const ScatterPhysics& ph, const ScatterLaun
     dim3 grid((unsigned)((L.vox_count + kItemThreads - 1) / kItemThreads), (unsigned)L.det_count);
     scatter_kernel<<<grid, kItemThreads, 0, s>>>(g, ph, L);
     return cudaGetLastError() == cudaSuccess ? 0 : -1;
+}
+
+static double kn_shape_sin(double th, double alpha)
+{
+    const double c = std::cos(th), sn = std::sin(th);
+    const double f1 = alpha * (1.0 - c), f2 = 1.0 + c * c, p = 1.0 + f1;
+    return f2 / p / p * (1.0 + f1 * f1 / f2 / p) * sn;
+}
+
+static double kn_shape_sin_prime(double th, double alpha)
+{
+    const double c = std::cos(th), s = std::sin(th), om = 1.0 - c, p = 1.0 + alpha * om;
+    const double g = (1.0 + c * c) / (p * p) + alpha * alpha * om * om / (p * p * p);
+    const double gp = 2.0 * c / (p * p) + 2.0 * alpha * (1.0 + c * c) / (p * p * p) -
+                      2.0 * alpha * alpha * om / (p * p * p) + 3.0 * alpha * alpha * alpha * om * om / (p * p * p * p);
+    return c * g - s * s * gp;
+}
+
+void kn_table_build(double e0, double* tab)
+{
+    const int N = kKnTable;
+    const double alpha = e0 / 511.0, hc = 3.14159265358979323846 / N;
+    static const double xg[4] = {0.1834346424956498, 0.5255324099163290, 0.7966664774136267, 0.9602898564975363};
+    static const double wg[4] = {0.3626837833783620, 0.3137066458778873, 0.2223810344533745, 0.1012285362903763};
+    double G = 0.0;
+    for (int i = 0; i <= N; ++i) {
+        const double th = i * hc;
+        if (i > 0) {                       // exact-to-rounding 8-point Gauss-Legendre per cell
+            const double mid = th - 0.5 * hc, half = 0.5 * hc;
+            double acc = 0.0;
+            for (int k = 0; k < 4; ++k)
+                acc += wg[k] * (kn_shape_sin(mid - half * xg[k], alpha) + kn_shape_sin(mid + half * xg[k], alpha));
+            G += half * acc;
+        }
+        tab[i] = G;
+        tab[(N + 1) + i] = kn_shape_sin(th, alpha);
+        tab[2 * (N + 1) + i] = kn_shape_sin_prime(th, alpha);
+    }
 }
 
 double kn_normalisation(double e0)

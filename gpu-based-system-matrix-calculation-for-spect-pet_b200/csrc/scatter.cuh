@@ -59,8 +59,14 @@ struct ScatterLaunch {
     const float* pe;       // D x V photoelectric matrix (crystal part)
     const PairRec* pairs;
     const AttEntry* att;
+    const double* kn_tab;  // Klein-Nishina table (kn_table_build), kKnTable + 1 nodes on [0, pi]
     float* out;
 };
+
+// FP64 table of the Klein-Nishina shape on [0, pi]: nodes theta_i = i * pi / kKnTable;
+// [0 .. N] integral from 0, [N+1 .. 2N+1] F = KN(theta) sin(theta), [2N+2 .. 3N+2] dF/dtheta.
+constexpr int kKnTable = 4096;
+void kn_table_build(double e0, double* host_tab);   // host buffer of 3 * (kKnTable + 1) doubles
 
 // Word counts of the reference bitmap layouts (scatter.cu:2053-2056, :2234-2237).
 long long bitmap_crystal_words(int n_det);

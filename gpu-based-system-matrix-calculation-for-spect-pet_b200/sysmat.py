@@ -30,7 +30,8 @@ HOLE_MODEL_VARIANT = 1
 EXPORTS = ("PESysMatGen", "scatter", "scatter_collimator", "scatter_crystal", "sysmat_create",
            "sysmat_destroy", "sysmat_dims", "sysmat_pe", "sysmat_bitmap_crystal_words",
            "sysmat_bitmap_collimator_words", "sysmat_bitmap_crystal", "sysmat_bitmap_collimator",
-           "sysmat_scatter_prepare", "sysmat_scatter", "sysmat_pe_noalloc", "sysmat_pe_work",
+           "sysmat_scatter_prepare", "sysmat_scatter", "sysmat_pe_noalloc", "sysmat_csr_count",
+           "sysmat_csr_fill", "sysmat_pe_work",
            "sysmat_measure_peaks",
            "sysmat_error_string", "sysmat_version")
 
@@ -83,6 +84,10 @@ def lib():
             "sysmat_pe_noalloc": ([_fp, _fp, _fp, ctypes.c_float, ctypes.c_int, ctypes.c_int,
                                    ctypes.c_longlong, ctypes.c_longlong, _vp, ctypes.c_longlong,
                                    ctypes.c_int, _vp], ctypes.c_int),
+            "sysmat_csr_count": ([_vp, ctypes.c_int, ctypes.c_longlong, ctypes.c_longlong, ctypes.c_float,
+                                  _vp, _vp, _vp], ctypes.c_int),
+            "sysmat_csr_fill": ([_vp, ctypes.c_int, ctypes.c_longlong, ctypes.c_longlong, ctypes.c_float,
+                                 ctypes.c_longlong, _vp, _vp, _vp, _vp], ctypes.c_int),
             "sysmat_error_string": ([ctypes.c_int], ctypes.c_char_p),
             "sysmat_version": ([], ctypes.c_char_p),
         }
@@ -273,3 +278,22 @@ def pe_noalloc(geo, out, rotation=0.0, det_begin=0, det_count=None, vox_begin=0,
                                    vox_count, _ptr(out), ld, mode, _stream(stream)),
            "sysmat_pe_noalloc")
     return out
+
+
+def to_csr(dense, threshold=1e-9, col_offset=0, stream=None):
+    """CSR (row_ptr int64 [rows+1], col_idx int64, values float32) of a CUDA float32 block,
+    keeping entries > threshold.  Two device passes; one small host read of the total."""
+    import torch
+    rows, cols = dense.shape
+    ld = dense.stride(0)
+    dev = dense.device
+    nnz = torch.empty(rows, dtype=torch.int64, device=dev)
+    ptr = torch.empty(rows + 1, dtype=torch.int64, device=dev)
+    _check(lib().sysmat_csr_count(_ptr(dense), rows, cols, ld, float(threshold), _ptr(nnz), _ptr(ptr),
+                                  _stream(stream)), "sysmat_csr_count")
+    total = int(ptr[rows].item())
+    col = torch.empty(max(total, 1), dtype=torch.int64, device=dev)
+    val = torch.empty(max(total, 1), dtype=torch.float32, device=dev)
+    _check(lib().sysmat_csr_fill(_ptr(dense), rows, cols, ld, float(threshold), int(col_offset), _ptr(ptr),
+                                 _ptr(col), _ptr(val), _stream(stream)), "sysmat_csr_fill")
+    return ptr, col[:total], val[:total]

@@ -143,6 +143,22 @@ SYSMAT_API int sysmat_pe_noalloc(const float* pC, const float* pD, const float* 
                                  void* stream);
 
 /* ---------------------------------------------------------------------------------- */
+/* Compressed output.  A dense block (rows x cols, row stride ld) becomes CSR with the      */
+/* entries whose value is > threshold (1e-9 for production matrices), in column order.      */
+
+/* Pass 1: d_row_nnz[rows] receives the per-row counts, d_row_ptr[rows + 1] their exclusive
+ * prefix sum (d_row_ptr[rows] = total).  Asynchronous on `stream`. */
+SYSMAT_API int sysmat_csr_count(const float* d_dense, int rows, long long cols, long long ld,
+                                float threshold, long long* d_row_nnz, long long* d_row_ptr,
+                                void* stream);
+
+/* Pass 2: writes column indices (+ col_offset, e.g. the block's first voxel) and values at
+ * the row pointers of pass 1; d_col_idx and d_val hold d_row_ptr[rows] entries. */
+SYSMAT_API int sysmat_csr_fill(const float* d_dense, int rows, long long cols, long long ld,
+                               float threshold, long long col_offset, const long long* d_row_ptr,
+                               long long* d_col_idx, float* d_val, void* stream);
+
+/* ---------------------------------------------------------------------------------- */
 /* Diagnostics (benchmark roofline).                                                     */
 
 /* Same block as sysmat_pe (reference summation) with work counters (12 values):
