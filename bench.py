@@ -261,6 +261,10 @@ def run_sysmat(args, rank, world, local):
     if not args.no_scatter and world == 1:
         scatter = run_scatter(args, sysmat, torch)
 
+    batch = None
+    if not args.no_batch and world == 1:
+        batch = run_batch(args, sysmat, torch)
+
     result = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": region_ms / args.steps, "higher_is_better": True,
@@ -270,7 +274,7 @@ def run_sysmat(args, rank, world, local):
                    "elements_per_step_per_gpu": D * nxy, "summation": "reference order (float chain)",
                    "l2": "flushed between steps (256 MB write)"},
         "clocks": clk.summary(), "gpu_launches": args.steps,
-        "roofline": roof, "e2e": e2e, "scatter": scatter,
+        "roofline": roof, "e2e": e2e, "scatter": scatter, "batch": batch,
     }
     return result
 
@@ -322,6 +326,56 @@ def run_scatter(args, sysmat, torch):
     return {"value": ctx.n_det * ctx.n_vox / (ms * 1e-3), "unit": UNIT, "ms_per_step": ms,
             "workload": "config3 primary Compton (crystal + collimator) on z-plane 8: 1024 crystals x "
                         "2304 voxels, 1024 layer-0 holes"}
+
+
+def run_batch(args, sysmat, torch, n_instances=64, rows=8):
+    """Design sweep of configuration 4: every instance x every one of its rotations, each task
+    a block of `rows` crystals (centre of the 32x32 array) x one z-plane (1024 voxels).  The
+    batched form (one autotuned persistent launch, replayed as a CUDA graph) against the plain
+    form (one sysmat_pe call per instance and rotation), same outputs."""
+    geos = geometry.config4(n_instances=n_instances)
+    ctxs = [sysmat.Context(gg) for gg in geos]
+    d0, v0, nv = 16 * 32 + 12, 1024 * 8, 1024
+    tasks = [(k, float(r), d0, rows, v0, nv) for k, gg in enumerate(geos) for r in range(gg.n_rot)]
+    out = torch.empty((len(tasks), rows, nv), dtype=torch.float32, device="cuda")
+    plan = sysmat.BatchPlan(ctxs, [t + (out[i],) for i, t in enumerate(tasks)])
+    stream = torch.cuda.current_stream()
+    tiles = plan.tune(stream=stream)
+    plan.run(stream=stream)                                   # capture + warm-up
+    torch.cuda.synchronize()
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    n = 2
+    a.record(stream)
+    for _ in range(n):
+        plan.run(stream=stream)
+    b.record(stream)
+    torch.cuda.synchronize()
+    batch_ms = a.elapsed_time(b) / n
+    ref = out.clone()
+
+    def plain():
+        for i, (k, r, dd, nd, vv, nn) in enumerate(tasks):
+            ctxs[k].pe(out[i], rotation=r, det_begin=dd, det_count=nd, vox_begin=vv, vox_count=nn,
+                       stream=stream)
+
+    plain()                                                   # warm-up
+    torch.cuda.synchronize()
+    a.record(stream)
+    plain()
+    b.record(stream)
+    torch.cuda.synchronize()
+    plain_ms = a.elapsed_time(b)
+    same = bool(torch.equal(out, ref))
+    plan.close()
+    nel = len(tasks) * rows * nv
+    return {"value": nel / (batch_ms * 1e-3), "unit": UNIT, "ms_per_step": batch_ms,
+            "plain_value": nel / (plain_ms * 1e-3), "plain_ms_per_step": plain_ms,
+            "speedup_vs_plain": plain_ms / batch_ms, "outputs_identical": same,
+            "tiles": list(tiles), "tasks": len(tasks), "elements_per_step": nel,
+            "gpu_launches_per_step": {"batched": 1, "plain": len(tasks)},
+            "workload": f"config4 design sweep: {n_instances} seeded collimators x their 12-60 rotations "
+                        f"({len(tasks)} tasks), each crystals {d0}..{d0 + rows - 1} x z-plane 8 "
+                        f"(1024 voxels)"}
 
 
 # ---------------------------------------------------------------------------------------
@@ -408,6 +462,7 @@ def main():
                     help="first N crystals only (small cases for profiling)")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-scatter", action="store_true")
+    ap.add_argument("--no-batch", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
     if args.warmup < 3 and args.impl == "sysmat":

@@ -1,0 +1,113 @@
+"""Differentiable forward projection and MLEM reconstruction over libsysmat's on-the-fly
+projector (sysmat_project / sysmat_vjp / sysmat_backproject).
+
+The reference only writes the dense system matrix (PEGen_RayTracing_CircularHole/
+PESysMatGen.cu:1368-1437); its consumers multiply it.  Here the matrix is recomputed brick by
+brick inside each product, so a calibration loop over collimator parameters theta, or an MLEM
+reconstruction, needs no matrix memory.  theta = (mu_W, mu_crystal, hole radius, dx, dy, dz,
+tilt), as geometry.apply_theta applies it to the parameter arrays.
+"""
+from __future__ import annotations
+
+import importlib.util
+import os
+import sys
+
+import numpy as np
+import torch
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+
+
+def _load(name, path):
+    if name in sys.modules:
+        return sys.modules[name]
+    spec = importlib.util.spec_from_file_location(name, path)
+    mod = importlib.util.module_from_spec(spec)
+    sys.modules[name] = mod
+    spec.loader.exec_module(mod)
+    return mod
+
+
+sysmat = _load("sysmat_binding", os.path.join(HERE, "sysmat.py"))
+geometry = _load("sysmat_geometry", os.path.join(HERE, "geometry.py"))
+
+
+class Projector:
+    """A system whose parameters theta may change; keeps the context of the last theta."""
+
+    def __init__(self, geo, device=0, rotation=0.0, det_begin=0, det_count=None):
+        self.geo = geo
+        self.device = device
+        self.rotation = float(rotation)
+        self.det_begin = det_begin
+        self.det_count = geo.n_det - det_begin if det_count is None else det_count
+        self._theta = None
+        self._ctx = None
+
+    def context(self, theta=None):
+        theta = geometry.theta_of(self.geo) if theta is None else np.asarray(theta, dtype=np.float64)
+        if self._ctx is None or not np.array_equal(theta, self._theta):
+            if self._ctx is not None:
+                self._ctx.close()
+            self._ctx = sysmat.Context(geometry.apply_theta(self.geo, theta), device=self.device)
+            self._theta = theta.copy()
+        return self._ctx
+
+    def project(self, x, theta=None):
+        return self.context(theta).project(x, rotation=self.rotation, det_begin=self.det_begin,
+                                           det_count=self.det_count)
+
+    def backproject(self, u, theta=None):
+        return self.context(theta).backproject(u, rotation=self.rotation, det_begin=self.det_begin,
+                                               det_count=self.det_count)
+
+    def vjp(self, x, u, theta=None):
+        return self.context(theta).vjp(x, u, rotation=self.rotation, det_begin=self.det_begin,
+                                       det_count=self.det_count)
+
+
+class Projection(torch.autograd.Function):
+    """p = A(theta) x.  theta: CPU float64 tensor of 7; x: CUDA float32 tensor of n_vox;
+    p: CUDA float64 tensor of the projector's detector rows.  Backward gives d/d theta through
+    sysmat_vjp and d/d x through sysmat_backproject."""
+
+    @staticmethod
+    def forward(fctx, theta, x, projector):
+        th = theta.detach().cpu().numpy().astype(np.float64)
+        x = x.detach().to(torch.float32).contiguous()
+        fctx.projector = projector
+        fctx.theta = th
+        fctx.save_for_backward(x)
+        return projector.project(x, th)
+
+    @staticmethod
+    def backward(fctx, grad_p):
+        (x,) = fctx.saved_tensors
+        u = grad_p.detach().to(torch.float32).contiguous()
+        g_theta = g_x = None
+        if fctx.needs_input_grad[0]:
+            g = fctx.projector.vjp(x, u, fctx.theta)
+            g_theta = g[:sysmat.THETA_N].cpu().to(torch.float64)
+        if fctx.needs_input_grad[1]:
+            g_x = fctx.projector.backproject(u, fctx.theta).to(torch.float32)
+        return g_theta, g_x, None
+
+
+def project(theta, x, projector):
+    return Projection.apply(theta, x, projector)
+
+
+def mlem(projector, y, n_iter, x0=None, theta=None):
+    """MLEM reconstruction x <- x / (A^T 1) * A^T (y / A x) with the on-the-fly projector.
+    y: CUDA tensor of the projector's detector rows; returns a float32 CUDA tensor of n_vox."""
+    dev = y.device
+    sens = projector.backproject(torch.ones(projector.det_count, dtype=torch.float32, device=dev), theta)
+    x = torch.ones(projector.geo.n_vox, dtype=torch.float32, device=dev) if x0 is None else x0.clone()
+    yd = y.to(torch.float64)
+    for _ in range(n_iter):
+        p = projector.project(x, theta)
+        ratio = torch.where(p > 0, yd / p, torch.zeros_like(p)).to(torch.float32)
+        bp = projector.backproject(ratio, theta)
+        x = torch.where(sens > 0, x.to(torch.float64) * bp / sens, torch.zeros_like(sens)).to(torch.float32)
+    return x

@@ -18,6 +18,7 @@
 #include "geom.cuh"
 #include "pe.cuh"
 #include "scatter.cuh"
+#include "ctx.cuh"
 
 using namespace sysmat;
 
@@ -31,32 +32,6 @@ using namespace sysmat;
         }                                                                                  \
     } while (0)
 
-struct sysmat_ctx {
-    int device = -1;
-    int num_sms = 0;
-    DevGeom g{};
-    int n_holes0_host = 0;
-    // raw parameter arrays on the device (bitmap kernels read them like the reference)
-    float* d_col = nullptr;
-    float* d_det = nullptr;
-    float* d_img = nullptr;
-    float* d_phys = nullptr;
-    std::vector<float> h_phys;
-    std::vector<float> h_img;
-    float h_col15 = 0.0f, h_col17 = 0.0f;   // layer-0 mu_total and mu_compton (scatter.cu:1716)
-    // derived tables
-    float4* d_tables = nullptr;
-    // launch bookkeeping
-    unsigned long long* d_counter = nullptr;
-    int* d_status = nullptr;
-    // scatter pair tables (sysmat_scatter_prepare)
-    ScatterScratch scratch{};
-    int prepared_parts = 0;
-    PairRec* pairs = nullptr;
-    AttEntry* att = nullptr;
-    double* d_kn_tab = nullptr;     // Klein-Nishina table for kn_e0
-    float kn_e0 = -1.0f;
-};
 
 namespace {
 
@@ -253,8 +228,9 @@ extern "C" SYSMAT_API int sysmat_dims(const sysmat_ctx* ctx, int* n_det, long lo
     return SYSMAT_OK;
 }
 
-static int check_block(const sysmat_ctx* ctx, int det_begin, int det_count, long long vox_begin,
-                       long long vox_count, const float* d_out, long long ld)
+namespace sysmat {
+int check_block(const sysmat_ctx* ctx, int det_begin, int det_count, long long vox_begin,
+                long long vox_count, const float* d_out, long long ld)
 {
     if (!ctx || !d_out) return SYSMAT_ERR_ARG;
     if (det_begin < 0 || det_count < 0 || det_begin + det_count > ctx->g.n_det) return SYSMAT_ERR_ARG;
@@ -263,6 +239,7 @@ static int check_block(const sysmat_ctx* ctx, int det_begin, int det_count, long
     if (!same_device(ctx)) return SYSMAT_ERR_ARG;
     return SYSMAT_OK;
 }
+}  // namespace sysmat
 
 extern "C" SYSMAT_API int sysmat_pe(sysmat_ctx* ctx, float rotation, int det_begin, int det_count,
                          long long vox_begin, long long vox_count, float* d_out, long long ld,

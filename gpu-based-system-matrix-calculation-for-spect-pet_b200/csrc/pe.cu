@@ -39,7 +39,6 @@ constexpr int kThreads = kWarps * 32;
 constexpr int kSuperCap = 1024;         // block superset capacity (objects)
 constexpr int kChunk = 256;             // per-warp kept-object chunk
 constexpr int kRound = 64;              // per-warp round buffer
-constexpr int kBx = 4, kBy = 4, kBz = 2;
 constexpr float kSlopeMargin = 2e-4f;   // slope units; >> FP32 position error / depth
 constexpr float kMinDepth = 1.0f;       // mm; slope rectangles need objects this far behind
 
@@ -510,12 +509,12 @@ __device__ __forceinline__ float finish_sub_element(const Elem& e, const SubElem
     return eff * sa * absf;
 }
 
-template <int MODE, bool COUNT>
-__device__ float pe_element(const DevGeom& g, const BlockSmem& bs, WarpSmem& ws, int d,
-                            long long v, float cr, float sr, int lane,
-                            unsigned long long* counters)
+// Per-element set-up shared by the lanes of a warp: voxel centre, crystal d, reference cone
+// constants, slope rectangle and the plate "through both faces" rectangles.  False when the
+// crystal's attenuation is too low for the reference to compute the element (it is 0).
+__device__ __forceinline__ bool init_element(const DevGeom& g, WarpSmem& ws, int d, long long v, float cr,
+                                             float sr, int lane, Elem& e)
 {
-    Elem e;
     voxel_centre(g, v, cr, sr, e.xI, e.yI, e.zI);
     const float4 P = __ldg(&g.cry.pos[d]);
     const float4 S = __ldg(&g.cry.size[d]);
@@ -525,7 +524,7 @@ __device__ float pe_element(const DevGeom& g, const BlockSmem& bs, WarpSmem& ws,
     e.w = S.x; e.t = S.y; e.h = S.z;
     e.mu_t = M.x; e.mu_pe = M.y;
     e.cosr = T.x; e.sinr = T.y;
-    if (!(e.mu_t > 0.01f)) return 0.0f;                    // :1107, :1194
+    if (!(e.mu_t > 0.01f)) return false;                   // :1107, :1194
     to_crystal_frame(e.xd, e.yd, e.zd, T.z, T.w, e.xI, e.yI, e.zI, e.xIs, e.yIs, e.zIs);
     const float dist = sqrtf((e.yd - e.yI) * (e.yd - e.yI) + (e.xd - e.xI) * (e.xd - e.xI) +
                              (e.zd - e.zI) * (e.zd - e.zI));
@@ -551,6 +550,16 @@ __device__ float pe_element(const DevGeom& g, const BlockSmem& bs, WarpSmem& ws,
         ws.inner[lane] = inner;
     }
 
+    return true;
+}
+
+template <int MODE, bool COUNT>
+__device__ double pe_element(const DevGeom& g, const BlockSmem& bs, WarpSmem& ws, int d,
+                             long long v, float cr, float sr, int lane,
+                             unsigned long long* counters)
+{
+    Elem e;
+    if (!init_element(g, ws, d, v, cr, sr, lane, e)) return 0.0;
     const bool from_super = bs.s_count >= 0;
     const int n_src = from_super ? bs.s_count : g.n_holes + g.n_det;
     int count = 0;
@@ -660,7 +669,7 @@ __device__ float pe_element(const DevGeom& g, const BlockSmem& bs, WarpSmem& ws,
     } else {
 #pragma unroll
         for (int off = 16; off > 0; off >>= 1) dacc += __shfl_xor_sync(0xffffffffu, dacc, off);
-        return (float)dacc;
+        return dacc;
     }
 }
 
@@ -719,6 +728,47 @@ __device__ void build_superset(const DevGeom& g, BlockSmem& bs, int d, float cx,
     __syncthreads();
 }
 
+// Output block of one brick: rows (crystals) from det_begin, voxels vox_begin .. vlast.
+struct BrickOut {
+    float* out;
+    long long ld, vox_begin, vlast;
+    int det_begin;
+};
+
+// One work item: crystal det_begin + di against one voxel brick of bx x by x bz voxels (brick
+// (gx, gy, gz) of the block's grid starting at z-plane iz0).  The block builds the cone
+// superset of the brick, then its warps take the brick's voxels in turn.
+template <int MODE, bool COUNT>
+__device__ __forceinline__ void pe_brick(const DevGeom& g, BlockSmem& bs, WarpSmem& ws, int lane, int wid,
+                                         const BrickOut& O, int di, int gx, int gy, int gz, int iz0, int iz1,
+                                         int bx, int by, int bz, float cr, float sr,
+                                         unsigned long long* counters)
+{
+    const int x0 = gx * bx, y0 = gy * by, z0 = iz0 + gz * bz;
+    const int x1 = min(x0 + bx, g.nx) - 1, y1 = min(y0 + by, g.ny) - 1, z1 = min(z0 + bz, iz1 + 1) - 1;
+    const int d = O.det_begin + di;
+    // brick centre and radius from its extreme voxel centres (rotation about z keeps lengths)
+    float ax, ay, az, bxx, byy, bzz;
+    voxel_centre(g, x0 + g.nx * ((long long)y0 + g.ny * z0), 1.0f, 0.0f, ax, ay, az);
+    voxel_centre(g, x1 + g.nx * ((long long)y1 + g.ny * z1), 1.0f, 0.0f, bxx, byy, bzz);
+    const float mx = 0.5f * (ax + bxx), my = 0.5f * (ay + byy), mz = 0.5f * (az + bzz);
+    const float rho = 0.5f * sqrtf((bxx - ax) * (bxx - ax) + (byy - ay) * (byy - ay) +
+                                   (bzz - az) * (bzz - az)) + 1e-3f;
+    build_superset(g, bs, d, mx * cr - my * sr, mx * sr + my * cr, mz, rho);
+    const int n_slots = bx * by * bz;
+    for (int slot = wid; slot < n_slots; slot += kWarps) {
+        const int ox = slot % bx, oy = (slot / bx) % by, oz = slot / (bx * by);
+        const int ix = x0 + ox, iy = y0 + oy, iz = z0 + oz;
+        if (ix >= g.nx || iy >= g.ny || iz > z1) continue;
+        const long long v = ix + g.nx * ((long long)iy + (long long)g.ny * iz);
+        if (v < O.vox_begin || v > O.vlast) continue;
+        const float val = (float)pe_element<MODE, COUNT>(g, bs, ws, d, v, cr, sr, lane, counters);
+        if (lane == 0) O.out[(long long)di * O.ld + (v - O.vox_begin)] = val;
+        __syncwarp();
+    }
+    __syncthreads();
+}
+
 template <int MODE, bool COUNT>
 __global__ void __launch_bounds__(kThreads, 2) pe_kernel(DevGeom g, PeLaunch L)
 {
@@ -731,10 +781,12 @@ __global__ void __launch_bounds__(kThreads, 2) pe_kernel(DevGeom g, PeLaunch L)
     const long long nxy = (long long)g.nx * g.ny;
     const long long vlast = L.vox_begin + L.vox_count - 1;
     const int iz0 = (int)(L.vox_begin / nxy), iz1 = (int)(vlast / nxy);
-    const int nbx = (g.nx + kBx - 1) / kBx, nby = (g.ny + kBy - 1) / kBy;
-    const int nbz = (iz1 - iz0 + 1 + kBz - 1) / kBz;
+    constexpr int bx = 4, by = 4, bz = 2;                 // voxel brick of one work item
+    const int nbx = (g.nx + bx - 1) / bx, nby = (g.ny + by - 1) / by;
+    const int nbz = (iz1 - iz0 + 1 + bz - 1) / bz;
     const long long n_bricks = (long long)nbx * nby * nbz;
     const long long total = n_bricks * L.det_count;
+    const BrickOut O{L.out, L.ld, L.vox_begin, vlast, L.det_begin};
     for (;;) {
         if (threadIdx.x == 0) bs.item = (long long)atomicAdd(L.work_counter, 1ull);
         __syncthreads();
@@ -743,33 +795,74 @@ __global__ void __launch_bounds__(kThreads, 2) pe_kernel(DevGeom g, PeLaunch L)
         if (item >= total) break;
         const int di = (int)(item / n_bricks);
         const long long b = item - (long long)di * n_bricks;
-        const int bz = (int)(b / ((long long)nbx * nby));
-        const int rem = (int)(b - (long long)bz * nbx * nby);
-        const int by = rem / nbx, bx = rem - by * nbx;
-        const int x0 = bx * kBx, y0 = by * kBy, z0 = iz0 + bz * kBz;
-        const int x1 = min(x0 + kBx, g.nx) - 1, y1 = min(y0 + kBy, g.ny) - 1, z1 = min(z0 + kBz, iz1 + 1) - 1;
-        const int d = L.det_begin + di;
-        // brick centre and radius from its extreme voxel centres (rotation about z keeps lengths)
-        float ax, ay, az, bxx, byy, bzz;
-        voxel_centre(g, x0 + g.nx * ((long long)y0 + g.ny * z0), 1.0f, 0.0f, ax, ay, az);
-        voxel_centre(g, x1 + g.nx * ((long long)y1 + g.ny * z1), 1.0f, 0.0f, bxx, byy, bzz);
-        const float mx = 0.5f * (ax + bxx), my = 0.5f * (ay + byy), mz = 0.5f * (az + bzz);
-        const float rho = 0.5f * sqrtf((bxx - ax) * (bxx - ax) + (byy - ay) * (byy - ay) +
-                                       (bzz - az) * (bzz - az)) + 1e-3f;
-        build_superset(g, bs, d, mx * cr - my * sr, mx * sr + my * cr, mz, rho);
-        for (int slot = wid; slot < kBx * kBy * kBz; slot += kWarps) {
-            const int ox = slot % kBx, oy = (slot / kBx) % kBy, oz = slot / (kBx * kBy);
-            const int ix = x0 + ox, iy = y0 + oy, iz = z0 + oz;
-            if (ix >= g.nx || iy >= g.ny || iz > z1) continue;
-            const long long v = ix + g.nx * ((long long)iy + (long long)g.ny * iz);
-            if (v < L.vox_begin || v > vlast) continue;
-            const float val = pe_element<MODE, COUNT>(g, bs, ws, d, v, cr, sr, lane, L.counters);
-            if (lane == 0) L.out[(long long)di * L.ld + (v - L.vox_begin)] = val;
-            __syncwarp();
-        }
-        __syncthreads();
+        const int gz = (int)(b / ((long long)nbx * nby));
+        const int rem = (int)(b - (long long)gz * nbx * nby);
+        const int gy = rem / nbx, gx = rem - gy * nbx;
+        pe_brick<MODE, COUNT>(g, bs, ws, lane, wid, O, di, gx, gy, gz, iz0, iz1, bx, by, bz, cr, sr,
+                              L.counters);
     }
 }
+
+// Shared memory of the batched kernel: the block's working set plus the geometry of the
+// task in hand (copied in when the block moves to a task of another geometry).
+struct BatchSmem {
+    BlockSmem bs;
+    DevGeom g;
+    int task;
+};
+
+// Batched launch: one persistent grid over the items of many (geometry, rotation, block)
+// tasks, taken from one work counter; a block finds its item's task by binary search over
+// the tasks' first item numbers.
+template <int MODE>
+__global__ void __launch_bounds__(kThreads, 2) pe_batch_kernel(BatchLaunch B)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    BatchSmem& sm = *reinterpret_cast<BatchSmem*>(smem_raw);
+    BlockSmem& bs = sm.bs;
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    WarpSmem& ws = bs.w[wid];
+    int cur_geom = -1;
+    for (;;) {
+        if (threadIdx.x == 0) {
+            const long long item = (long long)atomicAdd(B.work_counter, 1ull);
+            int lo = 0, hi = B.n_tasks - 1;
+            while (lo < hi) {                       // last task with item_begin <= item
+                const int mid = (lo + hi + 1) >> 1;
+                if (B.tasks[mid].item_begin <= item) lo = mid; else hi = mid - 1;
+            }
+            bs.item = item;
+            sm.task = lo;
+        }
+        __syncthreads();
+        const long long item = bs.item;
+        const BatchTask T = B.tasks[sm.task];
+        __syncthreads();
+        if (item >= B.total_items) break;
+        if (T.geom != cur_geom) {                   // block-uniform
+            const int* src = reinterpret_cast<const int*>(B.geoms + T.geom);
+            int* dst = reinterpret_cast<int*>(&sm.g);
+            for (int i = threadIdx.x; i < (int)(sizeof(DevGeom) / sizeof(int)); i += kThreads) dst[i] = src[i];
+            cur_geom = T.geom;
+            __syncthreads();
+        }
+        const DevGeom& g = sm.g;
+        const float ang = T.rotation * g.angle_step;       // :1006
+        const float cr = cosf(ang), sr = sinf(ang);
+        const long long n_bricks = (long long)T.nbx * T.nby * T.nbz;
+        const long long local = item - T.item_begin;
+        const int di = (int)(local / n_bricks);
+        const long long b = local - (long long)di * n_bricks;
+        const int gz = (int)(b / ((long long)T.nbx * T.nby));
+        const int rem = (int)(b - (long long)gz * T.nbx * T.nby);
+        const int gy = rem / T.nbx, gx = rem - gy * T.nbx;
+        const BrickOut O{T.out, T.ld, T.vox_begin, T.vox_begin + T.vox_count - 1, T.det_begin};
+        pe_brick<MODE, false>(g, bs, ws, lane, wid, O, di, gx, gy, gz, T.iz0, T.iz1, B.bx, B.by, B.bz, cr, sr,
+                              nullptr);
+    }
+}
+
+#include "pe_adjoint.cuh"
 
 }  // namespace
 
@@ -791,6 +884,70 @@ static int launch_mode(const DevGeom& g, const PeLaunch& L, int num_sms, cudaStr
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, pe_kernel<MODE, COUNT>, kThreads, smem);
     if (per_sm < 1) per_sm = 1;
     pe_kernel<MODE, COUNT><<<num_sms * per_sm, kThreads, smem, stream>>>(g, L);
+    return cudaGetLastError() == cudaSuccess ? 0 : -1;
+}
+
+template <int KIND>
+static int launch_adjoint_kind(const DevGeom& g, const AdjLaunch& L, int num_sms, cudaStream_t stream)
+{
+    const int smem = (int)sizeof(AdjSmem);
+    static unsigned long long configured = 0;   // one bit per device
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return -1;
+    const unsigned long long bit = 1ull << (dev & 63);
+    if (!(__atomic_load_n(&configured, __ATOMIC_ACQUIRE) & bit)) {
+        if (cudaFuncSetAttribute(pe_adjoint_kernel<KIND>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem) !=
+            cudaSuccess)
+            return -1;
+        __atomic_fetch_or(&configured, bit, __ATOMIC_RELEASE);
+    }
+    int per_sm = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, pe_adjoint_kernel<KIND>, kThreads, smem);
+    if (per_sm < 1) per_sm = 1;
+    pe_adjoint_kernel<KIND><<<num_sms * per_sm, kThreads, smem, stream>>>(g, L);
+    return cudaGetLastError() == cudaSuccess ? 0 : -1;
+}
+
+int launch_pe_adjoint(const DevGeom& g, const AdjLaunch& L, int kind, int num_sms, cudaStream_t stream)
+{
+    if (kind == 0) return launch_adjoint_kind<0>(g, L, num_sms, stream);
+    if (kind == 1) return launch_adjoint_kind<1>(g, L, num_sms, stream);
+    return launch_adjoint_kind<2>(g, L, num_sms, stream);
+}
+
+template <int MODE>
+static int configure_batch_mode(int* per_sm)
+{
+    const int smem = (int)sizeof(BatchSmem);
+    static unsigned long long configured = 0;   // one bit per device
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return -1;
+    const unsigned long long bit = 1ull << (dev & 63);
+    if (!(__atomic_load_n(&configured, __ATOMIC_ACQUIRE) & bit)) {
+        if (cudaFuncSetAttribute(pe_batch_kernel<MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem) !=
+            cudaSuccess)
+            return -1;
+        __atomic_fetch_or(&configured, bit, __ATOMIC_RELEASE);
+    }
+    *per_sm = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(per_sm, pe_batch_kernel<MODE>, kThreads, smem) !=
+        cudaSuccess)
+        return -1;
+    if (*per_sm < 1) *per_sm = 1;
+    return 0;
+}
+
+int configure_pe_batch(int mode, int* blocks_per_sm)
+{
+    return mode == 0 ? configure_batch_mode<0>(blocks_per_sm) : configure_batch_mode<1>(blocks_per_sm);
+}
+
+int launch_pe_batch(const BatchLaunch& B, int mode, int grid, cudaStream_t stream)
+{
+    if (B.n_tasks < 1 || B.total_items < 1) return 0;
+    const int smem = (int)sizeof(BatchSmem);
+    if (mode == 0) pe_batch_kernel<0><<<grid, kThreads, smem, stream>>>(B);
+    else pe_batch_kernel<1><<<grid, kThreads, smem, stream>>>(B);
     return cudaGetLastError() == cudaSuccess ? 0 : -1;
 }
 

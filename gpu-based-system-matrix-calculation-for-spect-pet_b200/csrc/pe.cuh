@@ -29,7 +29,50 @@ struct PeLaunch {
     unsigned long long* counters;
 };
 
+// One (geometry, rotation, detector x voxel block) task of a batched launch.  The host fills
+// the brick grid of the block (nbx x nby x nbz bricks over z-planes iz0..iz1) and the first
+// global item number of the task; items are (row, brick) pairs, row-major.
+struct BatchTask {
+    int geom;                              // index into the launch's geometry array
+    float rotation;                        // rotation index, as Params_Image[20]
+    int det_begin, det_count;
+    long long vox_begin, vox_count;
+    float* out;
+    long long ld;
+    long long item_begin;
+    int nbx, nby, nbz, iz0, iz1;
+};
+
+struct BatchLaunch {
+    const DevGeom* geoms;                  // device array
+    const BatchTask* tasks;                // device array, item_begin ascending
+    int n_tasks;
+    long long total_items;
+    int bx, by, bz;
+    unsigned long long* work_counter;      // zeroed before the launch
+};
+
+// Forward projection and its vector-Jacobian product over all voxels of one rotation and a
+// range of detector rows (pe_adjoint.cuh).
+struct AdjLaunch {
+    int det_begin, det_count;
+    float rotation;
+    int bx = 4, by = 4, bz = 2;
+    const float* x;                        // n_vox activity values
+    const float* u;                        // det_count cotangent values (vjp only)
+    double* p;                             // det_count projections (project only), zeroed
+    double* grad;                          // 8 values (vjp only), zeroed
+    double* q;                             // n_vox back projections (back projection only), zeroed
+    unsigned long long* work_counter;      // zeroed
+};
+
 int launch_pe(const DevGeom& g, const PeLaunch& L, int mode, int num_sms, cudaStream_t stream);
+// kind 0: projection, kind 1: vector-Jacobian product, kind 2: back projection.
+int launch_pe_adjoint(const DevGeom& g, const AdjLaunch& L, int kind, int num_sms, cudaStream_t stream);
+// Sets the batched kernel's shared-memory attribute on the current device (once) and returns
+// how many of its blocks fit on one SM.  Call before capturing a launch into a graph.
+int configure_pe_batch(int mode, int* blocks_per_sm);
+int launch_pe_batch(const BatchLaunch& B, int mode, int grid, cudaStream_t stream);
 
 __global__ void derive_crystals(const float* __restrict__ det, float fov, int n, float4* pos,
                                 float4* size, float4* mu, float4* trig);

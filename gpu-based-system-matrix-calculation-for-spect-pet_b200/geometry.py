@@ -259,6 +259,110 @@ def mini(seed: int = 0, rotated: bool = False, layers: int = 1, n_rot: int = 1,
     return Geometry(f"mini{seed}{'r' if rotated else ''}{layers}", cb.build(), det, img, _physics())
 
 
+def config4(n_instances: int = 64, seed: int = 4) -> list:
+    """Batched design sweep: `n_instances` systems with seeded hole diameter U[0.8, 2.0] mm and
+    tungsten plate thickness U[5, 25] mm (32x32 holes at 2.5 mm pitch, plate 84x84 mm, so
+    every diameter fits the pitch), each with its own number of rotations U{12..60} and
+    step 2*pi/n; 32x32x16 voxels of 2 mm, front face 50 mm from the FOV centre; NaI 32x32
+    crystals 2x5x2 mm at 2 mm pitch, 2 mm behind the plate.  Returns Geometry objects whose
+    image parameters carry n_rot and the step."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for k in range(n_instances):
+        dia = float(rng.uniform(0.8, 2.0))
+        t = float(rng.uniform(5.0, 25.0))
+        n_rot = int(rng.integers(12, 61))
+        cb = _CollimatorBuilder()
+        _w_layer(cb, 84.0, t, 84.0, _square_holes(32, 2.5, dia / 2.0))
+        det = _detector(_crystal_grid(32, 32, 2.0, t / 2 + 2.0 + 2.5), (2.0, 5.0, 2.0))
+        img = _image((32, 32, 16), (2, 2, 2), 50.0 + t / 2, n_rot=n_rot, dtheta=2 * math.pi / n_rot)
+        out.append(Geometry(f"config4_{k}", cb.build(), det, img, _physics(),
+                            dict(hole_diameter=dia, thickness=t, n_rot=n_rot)))
+    return out
+
+
+def apply_theta(geo: Geometry, theta) -> Geometry:
+    """The system at parameters theta = (mu_W, mu_crystal, hole radius, dx, dy, dz, tilt):
+    every layer's mu_total and every crystal's mu_total (mu_pe kept, mu_C = mu_total - mu_pe)
+    and every hole's radius are set; hole centres are rotated by `tilt` (radians) about the
+    y axis and shifted by (dx, dz); hole caps and layer planes are shifted by dy.  Coordinates
+    are computed in double and rounded to the float parameter format once."""
+    mu_w, mu_c, radius, dx, dy, dz, tilt = (float(t) for t in theta)
+    col = geo.collimator.astype(np.float64)
+    det = geo.detector.astype(np.float64)
+    n_layers = int(round(col[0]))
+    for m in range(n_layers):
+        base = (m + 1) * 10
+        col[base + 4] += dy
+        col[base + 5] = mu_w
+    n_holes = geo.n_holes
+    h = col[100:100 + 9 * n_holes].reshape(n_holes, 9)
+    x, z = h[:, 0].copy(), h[:, 3].copy()
+    c, s_ = math.cos(tilt), math.sin(tilt)
+    h[:, 0] = x * c - z * s_ + dx
+    h[:, 3] = x * s_ + z * c + dz
+    h[:, 1] += dy
+    h[:, 2] += dy
+    h[:, 4] = radius
+    col[100:100 + 9 * n_holes] = h.reshape(-1)
+    n_det = geo.n_det
+    d = det[1:1 + 12 * n_det].reshape(n_det, 12)
+    changed = d[:, 6] != np.float64(np.float32(mu_c))
+    d[changed, 8] = mu_c - d[changed, 7]
+    d[:, 6] = mu_c
+    det[1:1 + 12 * n_det] = d.reshape(-1)
+    return Geometry(geo.name, col.astype(np.float32), det.astype(np.float32), geo.image, geo.physics,
+                    dict(geo.meta, theta=tuple(float(t) for t in theta)))
+
+
+def theta_of(geo: Geometry) -> np.ndarray:
+    """Nominal theta of a system built here (layer 0 mu, crystal 0 mu, hole 0 radius, no
+    shift or tilt)."""
+    return np.array([float(geo.collimator[15]), float(geo.detector[7]), float(geo.collimator[104]),
+                     0.0, 0.0, 0.0, 0.0])
+
+
+def ellipsoid_phantom(n, width, n_ellipsoids=5, seed=5) -> np.ndarray:
+    """Seeded phantom of uniform ellipsoids (activity U[0.5, 4]) on an n = (nx, ny, nz) grid of
+    voxel size `width`, flattened as ix + nx*(iy + ny*iz)."""
+    rng = np.random.default_rng(seed)
+    nx, ny, nz = n
+    xs = (np.arange(nx) - nx / 2 + 0.5) * width[0]
+    ys = (np.arange(ny) - ny / 2 + 0.5) * width[1]
+    zs = (np.arange(nz) - nz / 2 + 0.5) * width[2]
+    Z, Y, X = np.meshgrid(zs, ys, xs, indexing="ij")
+    img = np.zeros((nz, ny, nx))
+    half = np.array([nx * width[0], ny * width[1], nz * width[2]]) / 2
+    for _ in range(n_ellipsoids):
+        c = rng.uniform(-0.5, 0.5, 3) * half
+        r = rng.uniform(0.15, 0.4, 3) * half
+        a = rng.uniform(0.5, 4.0)
+        inside = ((X - c[0]) / r[0]) ** 2 + ((Y - c[1]) / r[1]) ** 2 + ((Z - c[2]) / r[2]) ** 2 <= 1.0
+        img[inside] += a
+    return img.reshape(-1).astype(np.float32)
+
+
+def config5(seed: int = 5):
+    """Calibration problem: 64x64x16 voxels of 1 mm holding a seeded phantom of 5 uniform
+    ellipsoids; tungsten plate T = 10 mm (100x100 mm, a generator choice covering the
+    detector) with 32x32 holes of radius 0.75 mm at 2.0 mm pitch, front face 40 mm from the
+    FOV centre (clears the 32 mm half-depth); NaI 48x48 crystals 2x5x2 mm at 2 mm pitch, 2 mm
+    behind the plate.  Returns (geometry at nominal theta, phantom x, nominal theta, true
+    theta*) with theta* = nominal + offsets N(0, 0.1 mm) and tilt N(0, 0.2 deg)."""
+    t = 10.0
+    cb = _CollimatorBuilder()
+    _w_layer(cb, 100.0, t, 100.0, _square_holes(32, 2.0, 0.75))
+    det = _detector(_crystal_grid(48, 48, 2.0, t / 2 + 2.0 + 2.5), (2.0, 5.0, 2.0))
+    geo = Geometry("config5", cb.build(), det, _image((64, 64, 16), (1, 1, 1), 40.0 + t / 2), _physics())
+    x = ellipsoid_phantom((64, 64, 16), (1.0, 1.0, 1.0), 5, seed)
+    rng = np.random.default_rng(seed + 1)
+    theta0 = theta_of(geo)
+    theta_star = theta0.copy()
+    theta_star[3:6] += rng.normal(0.0, 0.1, 3)
+    theta_star[6] += math.radians(rng.normal(0.0, 0.2))
+    return geo, x, theta0, theta_star
+
+
 CONFIGS = {"config1": config1, "config2": config2, "config3": config3}
 
 

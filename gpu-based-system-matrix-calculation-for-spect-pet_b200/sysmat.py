@@ -21,6 +21,8 @@ ERRORS = {-1: "SYSMAT_ERR_ARG", -2: "SYSMAT_ERR_CUDA", -3: "SYSMAT_ERR_CAPACITY"
           -4: "SYSMAT_ERR_IO", -5: "SYSMAT_ERR_NOMEM", -6: "SYSMAT_ERR_TIMEOUT"}
 MODE_REFERENCE = 0
 MODE_PRECISE = 1
+THETA_N = 7
+THETA_NAMES = ("mu_w", "mu_crystal", "radius", "dx", "dy", "dz", "tilt")
 SCATTER_CRYSTAL = 1
 SCATTER_COLLIMATOR = 2
 HOLE_MODEL_COMBINED = 0
@@ -31,13 +33,22 @@ EXPORTS = ("PESysMatGen", "scatter", "scatter_collimator", "scatter_crystal", "s
            "sysmat_destroy", "sysmat_dims", "sysmat_pe", "sysmat_bitmap_crystal_words",
            "sysmat_bitmap_collimator_words", "sysmat_bitmap_crystal", "sysmat_bitmap_collimator",
            "sysmat_scatter_prepare", "sysmat_scatter", "sysmat_pe_noalloc", "sysmat_csr_count",
-           "sysmat_csr_fill", "sysmat_pe_work",
+           "sysmat_csr_fill", "sysmat_pe_work", "sysmat_batch_create", "sysmat_batch_set_tiles",
+           "sysmat_batch_get_tiles", "sysmat_batch_tune", "sysmat_batch_run", "sysmat_batch_destroy",
+           "sysmat_batch", "sysmat_project", "sysmat_vjp", "sysmat_backproject",
            "sysmat_measure_peaks",
            "sysmat_error_string", "sysmat_version")
 
 _fp = ctypes.POINTER(ctypes.c_float)
 _vp = ctypes.c_void_p
 _lib = None
+
+
+class BatchItem(ctypes.Structure):
+    """sysmat_batch_item: one (context, rotation, detector x voxel block) task of a batch."""
+    _fields_ = [("ctx", ctypes.c_int), ("rotation", ctypes.c_float), ("det_begin", ctypes.c_int),
+                ("det_count", ctypes.c_int), ("vox_begin", ctypes.c_longlong),
+                ("vox_count", ctypes.c_longlong), ("d_out", ctypes.c_void_p), ("ld", ctypes.c_longlong)]
 
 
 class SysmatError(RuntimeError):
@@ -88,6 +99,20 @@ def lib():
                                   _vp, _vp, _vp], ctypes.c_int),
             "sysmat_csr_fill": ([_vp, ctypes.c_int, ctypes.c_longlong, ctypes.c_longlong, ctypes.c_float,
                                  ctypes.c_longlong, _vp, _vp, _vp, _vp], ctypes.c_int),
+            "sysmat_batch_create": ([ctypes.POINTER(_vp), ctypes.POINTER(_vp), ctypes.c_int,
+                                     ctypes.POINTER(BatchItem), ctypes.c_int], ctypes.c_int),
+            "sysmat_batch_set_tiles": ([_vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int],
+                                       ctypes.c_int),
+            "sysmat_batch_get_tiles": ([_vp, ctypes.POINTER(ctypes.c_int)], ctypes.c_int),
+            "sysmat_batch_tune": ([_vp, ctypes.c_int, _vp, ctypes.POINTER(ctypes.c_int)], ctypes.c_int),
+            "sysmat_batch_run": ([_vp, ctypes.c_int, _vp], ctypes.c_int),
+            "sysmat_batch_destroy": ([_vp], ctypes.c_int),
+            "sysmat_batch": ([ctypes.POINTER(_vp), ctypes.c_int, ctypes.POINTER(BatchItem), ctypes.c_int,
+                              ctypes.c_int, _vp], ctypes.c_int),
+            "sysmat_project": ([_vp, ctypes.c_float, ctypes.c_int, ctypes.c_int, _vp, _vp, _vp], ctypes.c_int),
+            "sysmat_vjp": ([_vp, ctypes.c_float, ctypes.c_int, ctypes.c_int, _vp, _vp, _vp, _vp], ctypes.c_int),
+            "sysmat_backproject": ([_vp, ctypes.c_float, ctypes.c_int, ctypes.c_int, _vp, _vp, _vp],
+                                   ctypes.c_int),
             "sysmat_error_string": ([ctypes.c_int], ctypes.c_char_p),
             "sysmat_version": ([], ctypes.c_char_p),
         }
@@ -255,6 +280,100 @@ class Context:
                                     det_count, vox_begin, vox_count, _ptr(out), ld, _stream(stream)),
                "sysmat_scatter")
         return out
+
+
+def _context_project(self, x, p=None, rotation=0.0, det_begin=0, det_count=None, stream=None):
+    """p = A x over all voxels (x: CUDA float32 of n_vox); returns a float64 CUDA tensor."""
+    import torch
+    det_count = self.n_det - det_begin if det_count is None else det_count
+    p = torch.empty(det_count, dtype=torch.float64, device=x.device) if p is None else p
+    _check(lib().sysmat_project(self.handle, float(rotation), det_begin, det_count, _ptr(x), _ptr(p),
+                                _stream(stream)), "sysmat_project")
+    return p
+
+
+def _context_vjp(self, x, u, rotation=0.0, det_begin=0, det_count=None, stream=None):
+    """d(u^T A x)/d theta (float64 CUDA tensor of THETA_N + 1; the last entry is u^T A x)."""
+    import torch
+    det_count = self.n_det - det_begin if det_count is None else det_count
+    g = torch.empty(THETA_N + 1, dtype=torch.float64, device=x.device)
+    _check(lib().sysmat_vjp(self.handle, float(rotation), det_begin, det_count, _ptr(x), _ptr(u), _ptr(g),
+                            _stream(stream)), "sysmat_vjp")
+    return g
+
+
+def _context_backproject(self, u, rotation=0.0, det_begin=0, det_count=None, stream=None):
+    """q = A^T u (u: CUDA float32 of det_count); returns a float64 CUDA tensor of n_vox."""
+    import torch
+    det_count = self.n_det - det_begin if det_count is None else det_count
+    q = torch.empty(self.n_vox, dtype=torch.float64, device=u.device)
+    _check(lib().sysmat_backproject(self.handle, float(rotation), det_begin, det_count, _ptr(u), _ptr(q),
+                                    _stream(stream)), "sysmat_backproject")
+    return q
+
+
+Context.project = _context_project
+Context.vjp = _context_vjp
+Context.backproject = _context_backproject
+
+
+def _batch_items(contexts, items):
+    """items: iterables (ctx_index, rotation, det_begin, det_count, vox_begin, vox_count, out)
+    with `out` a CUDA float32 tensor of det_count rows (row-contiguous)."""
+    arr = (BatchItem * max(len(items), 1))()
+    for k, (c, rot, d0, nd, v0, nv, out) in enumerate(items):
+        ld = out.stride(0) if out.dim() == 2 else nv
+        arr[k] = BatchItem(int(c), float(rot), int(d0), int(nd), int(v0), int(nv), out.data_ptr(), int(ld))
+    ctxs = (_vp * len(contexts))(*[c.handle.value for c in contexts])
+    return ctxs, arr
+
+
+class BatchPlan:
+    """Many (system, rotation, block) PE tasks in one persistent launch (sysmat_batch_*).
+
+    The plan refers to the contexts' device tables and to the output tensors: keep them alive
+    while the plan is used."""
+
+    def __init__(self, contexts, items):
+        self._keep = (list(contexts), [it[-1] for it in items])
+        ctxs, arr = _batch_items(contexts, items)
+        h = ctypes.c_void_p()
+        _check(lib().sysmat_batch_create(ctypes.byref(h), ctxs, len(contexts), arr, len(items)),
+               "sysmat_batch_create")
+        self.handle = h
+
+    def set_tiles(self, bx, by, bz, blocks_per_sm=0):
+        _check(lib().sysmat_batch_set_tiles(self.handle, bx, by, bz, blocks_per_sm), "sysmat_batch_set_tiles")
+
+    def tiles(self):
+        t = (ctypes.c_int * 4)()
+        _check(lib().sysmat_batch_get_tiles(self.handle, t), "sysmat_batch_get_tiles")
+        return tuple(t)
+
+    def tune(self, mode=MODE_REFERENCE, stream=None):
+        t = (ctypes.c_int * 4)()
+        _check(lib().sysmat_batch_tune(self.handle, mode, _stream(stream), t), "sysmat_batch_tune")
+        return tuple(t)
+
+    def run(self, mode=MODE_REFERENCE, stream=None):
+        _check(lib().sysmat_batch_run(self.handle, mode, _stream(stream)), "sysmat_batch_run")
+
+    def close(self):
+        if self.handle:
+            lib().sysmat_batch_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def batch(contexts, items, mode=MODE_REFERENCE, stream=None):
+    """One-shot batched PE (sysmat_batch): create, run, synchronise, destroy."""
+    ctxs, arr = _batch_items(contexts, items)
+    _check(lib().sysmat_batch(ctxs, len(contexts), arr, len(items), mode, _stream(stream)), "sysmat_batch")
 
 
 def measure_peaks():

@@ -127,6 +127,76 @@ SYSMAT_API int sysmat_scatter(sysmat_ctx* ctx, int parts, int hole_model, float 
                               const float* d_pe, int det_begin, int det_count, long long vox_begin,
                               long long vox_count, float* d_out, long long ld, void* stream);
 
+/* ---- Batched photoelectric launches --------------------------------------------------------
+ * Many (system, rotation, block) tasks in one persistent launch over a device work queue.
+ * No reference counterpart: the reference computes one rotation of one system per call
+ * (PESysMatGen.cu:1368-1437).  Every context of a plan must live on the current device. */
+typedef struct sysmat_batch_item {
+    int ctx;                    /* index into the context array of the plan */
+    float rotation;             /* rotation index, as Params_Image[20] */
+    int det_begin, det_count;   /* detector rows */
+    long long vox_begin, vox_count;   /* voxels (flat index ix + Nx*(iy + Ny*iz)) */
+    float* d_out;               /* device block of det_count rows, row stride ld floats */
+    long long ld;
+} sysmat_batch_item;
+
+typedef struct sysmat_batch_plan sysmat_batch_plan;
+
+/* Validate the items (each block as sysmat_pe checks it) and upload the work queue.  The
+ * plan keeps pointers to the contexts' device tables: destroy it before them. */
+SYSMAT_API int sysmat_batch_create(sysmat_batch_plan** plan, sysmat_ctx* const* ctxs, int n_ctx,
+                                   const sysmat_batch_item* items, int n_items);
+/* Voxel brick of one work item (bx*by*bz <= 512) and resident blocks per SM (0 = all that fit). */
+SYSMAT_API int sysmat_batch_set_tiles(sysmat_batch_plan* plan, int bx, int by, int bz, int blocks_per_sm);
+/* tiles[4] = bx, by, bz, blocks_per_sm currently in use. */
+SYSMAT_API int sysmat_batch_get_tiles(const sysmat_batch_plan* plan, int* tiles);
+/* Time candidate bricks on a probe subset of the batch (synchronises `stream`), keep the
+ * fastest and return it in tiles[4] (may be NULL). */
+SYSMAT_API int sysmat_batch_tune(sysmat_batch_plan* plan, int mode, void* stream, int* tiles);
+/* Run the whole batch on `stream` (asynchronous).  The first run per mode captures the
+ * launch into a CUDA graph on a plan-owned stream; later runs replay it. */
+SYSMAT_API int sysmat_batch_run(sysmat_batch_plan* plan, int mode, void* stream);
+SYSMAT_API int sysmat_batch_destroy(sysmat_batch_plan* plan);
+/* One-shot: create, run once without a graph, synchronise `stream`, destroy. */
+SYSMAT_API int sysmat_batch(sysmat_ctx* const* ctxs, int n_ctx, const sysmat_batch_item* items, int n_items,
+                            int mode, void* stream);
+
+/* ---- Forward projection and its adjoint -----------------------------------------------------
+ * No reference counterpart: the reference only writes the dense matrix.  Both functions cover
+ * every voxel of rotation `rotation` and detector rows [det_begin, +det_count), recompute A
+ * brick by brick (nothing of A is stored) and skip voxels with x = 0.  Asynchronous on
+ * `stream`; calls on one context share its work counter, so issue them on one stream.
+ *
+ * theta, the parameters of the derivative, in this order:
+ *   0 mu_W        total attenuation of every collimator layer (Params_Collimator[(m+1)*10+5])
+ *   1 mu_crystal  total attenuation of every crystal (Params_Detector[12d+7]; mu_pe held fixed)
+ *   2 radius      radius of every hole (Params_Collimator[100+9h+4])
+ *   3 dx          shift of every hole centre along x
+ *   4 dy          shift of every hole's caps and every layer plane along y
+ *   5 dz          shift of every hole centre along z
+ *   6 tilt        rotation of the hole pattern about the y axis, radians
+ *                 (x' = x cos t - z sin t, z' = x sin t + z cos t)
+ * Thresholds of the reference's program (plate penalty, eps cut-offs) are piecewise constant
+ * and contribute nothing to the derivative. */
+#define SYSMAT_THETA_N 7
+
+/* d_p[i] = sum_v A[det_begin + i, v] * d_x[v] in double (precise-mode elements).
+ * d_x: n_vox floats; d_p: det_count doubles, overwritten. */
+SYSMAT_API int sysmat_project(sysmat_ctx* ctx, float rotation, int det_begin, int det_count,
+                              const float* d_x, double* d_p, void* stream);
+
+/* Vector-Jacobian product of the projection: with u = d_u (det_count floats, the cotangent of
+ * d_p), d_grad[k] = sum_{i,v} u[i] x[v] dA[det_begin + i, v]/dtheta_k for k < SYSMAT_THETA_N,
+ * and d_grad[SYSMAT_THETA_N] = u^T A x.  d_grad: SYSMAT_THETA_N + 1 doubles, overwritten.
+ * For loss = |A x - y|^2 pass u = 2 (A x - y). */
+SYSMAT_API int sysmat_vjp(sysmat_ctx* ctx, float rotation, int det_begin, int det_count, const float* d_x,
+                          const float* d_u, double* d_grad, void* stream);
+
+/* Back projection d_q[v] = sum_i A[det_begin + i, v] * d_u[i] (the gradient of u^T A x with
+ * respect to x).  d_u: det_count floats; d_q: n_vox doubles, overwritten. */
+SYSMAT_API int sysmat_backproject(sysmat_ctx* ctx, float rotation, int det_begin, int det_count,
+                                  const float* d_u, double* d_q, void* stream);
+
 /* Photoelectric block like sysmat_pe, for callers that cannot allocate device memory when
  * they call (for example a host that gives all device memory to its own pool at start-up,
  * or a plug-in host that forbids allocation after initialisation).  No counterpart in the
