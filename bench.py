@@ -437,6 +437,7 @@ def run_reference(args, rank, world, local):
     value = nel * args.steps / dt
     sample = (f"{strip} voxel rows x {int(g.image[0])} of z-plane {plane} x {g.n_det} crystals "
               f"({nel} elements) per step, one PESysMatGen call each")
+    scatter = None if args.no_scatter else run_reference_scatter(ref_lib, local)
     return {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": 1,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": dt * 1e3 / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
@@ -447,7 +448,30 @@ def run_reference(args, rank, world, local):
                              "sample": sample + "; the reference is a CUDA program: its host "
                                        "wrapper drives the GPU"},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
-            "gpu_launches": args.steps}
+            "gpu_launches": args.steps, "scatter": scatter}
+
+
+def run_reference_scatter(ref_lib, local):
+    """The reference's combined scatter program on 8 voxel rows (384 voxels) of configuration
+    3's z-plane 8 x 1024 crystals: a warm-up call computes and writes the relationship bitmaps,
+    the timed call reads them back (about 200 MB of files), as a rotation loop of the reference
+    program would."""
+    import tempfile
+    g = geometry.voxel_slab(geometry.config3(), 8, 20, 8)
+    pe = ref_lib.pe(g, cuda_id=local)
+    tmp = tempfile.mkdtemp(prefix="refscatter_")
+    ref_lib.scatter(g, pe, "combined", cuda_id=local, workdir=tmp)
+    t = time.perf_counter()
+    ref_lib.scatter(g, pe, "combined", cuda_id=local, workdir=tmp, load_bitmaps=True)
+    dt = time.perf_counter() - t
+    for f in os.listdir(tmp):
+        os.remove(os.path.join(tmp, f))
+    os.rmdir(tmp)
+    nel = g.n_det * g.n_vox
+    return {"value": nel / dt, "unit": UNIT, "ms_per_step": dt * 1e3,
+            "workload": "config3 primary Compton (crystal + collimator), reference combined program, "
+                        f"voxel rows 20-27 of z-plane 8: {g.n_det} crystals x {g.n_vox} voxels, bitmaps read "
+                        "from the files of a warm-up call"}
 
 
 def main():

@@ -77,16 +77,18 @@ def _geo_paths(tmp):
             os.path.join(tmp, "GeometryRelationShip_Collimator2Crystal").encode())
 
 
-def scatter(geo, pe_matrix, variant: str = "combined", cuda_id: int = 0, workdir=None):
+def scatter(geo, pe_matrix, variant: str = "combined", cuda_id: int = 0, workdir=None, load_bitmaps=False):
     """Reference scatter program.  variant: combined | collimator | crystal.
 
     The bitmaps are computed by the reference (physics[8] = physics[9] = 1) and read back
-    from the files it writes.  Returns (dst (D,V) float32, bitmaps dict of uint32 arrays)."""
+    from the files it writes; with load_bitmaps (and a workdir holding the files of an earlier
+    call) the reference reads them instead (physics[8] = physics[9] = 0).  Returns
+    (dst (D,V) float32, bitmaps dict of uint32 arrays)."""
     if geo.n_rot != 1 and variant == "combined":
         raise ValueError("the combined reference sums D*V*R elements on the host; use R = 1")
     phys = geo.physics.copy()
-    phys[8] = 1.0
-    phys[9] = 1.0
+    phys[8] = 0.0 if load_bitmaps else 1.0
+    phys[9] = 0.0 if load_bitmaps else 1.0
     D, V = geo.n_det, geo.n_vox
     c, pc = _f(geo.collimator.copy())
     d, pd = _f(geo.detector.copy())
@@ -113,7 +115,8 @@ def scatter(geo, pe_matrix, variant: str = "combined", cuda_id: int = 0, workdir
     bitmaps = {}
     for key, path in (("crystal", fcry), ("collimator", fcol)):
         if os.path.exists(path):
-            bitmaps[key] = np.fromfile(path.decode(), dtype=np.uint32)
+            if own or not load_bitmaps:
+                bitmaps[key] = np.fromfile(path.decode(), dtype=np.uint32)
             if own:
                 os.remove(path)
     if own:
