@@ -205,6 +205,7 @@ extern "C" SYSMAT_API int sysmat_destroy(sysmat_ctx* ctx)
     if (!ctx) return SYSMAT_OK;
     scatter_scratch_free(ctx->scratch);
     cudaFree(ctx->d_kn_tab);
+    cudaFree(ctx->d_shapes);
     cudaFree(ctx->d_det);
     cudaFree(ctx->d_col);
     cudaFree(ctx->d_img);
@@ -213,6 +214,50 @@ extern "C" SYSMAT_API int sysmat_destroy(sysmat_ctx* ctx)
     cudaFree(ctx->d_counter);
     cudaFree(ctx->d_status);
     delete ctx;
+    return SYSMAT_OK;
+}
+
+extern "C" SYSMAT_API int sysmat_set_hole_shapes(sysmat_ctx* ctx, const float* rho_x, const float* rho_z,
+                                                  const float* theta)
+{
+    if (!ctx || !same_device(ctx)) return SYSMAT_ERR_ARG;
+    if (!rho_x) {                                   // back to circular holes
+        cudaFree(ctx->d_shapes);
+        ctx->d_shapes = nullptr;
+        ctx->g.hole_shape = nullptr;
+        return SYSMAT_OK;
+    }
+    if (!rho_z || !theta) return SYSMAT_ERR_ARG;
+    const int n = ctx->g.n_holes;
+    std::vector<float> h(3 * (size_t)(n > 0 ? n : 1), 0.0f);
+    std::vector<float> col(kNCollimator);
+    CUDA_TRY(cudaMemcpy(col.data(), ctx->d_col, sizeof(float) * kNCollimator, cudaMemcpyDeviceToHost));
+    for (int i = 0; i < n; ++i) {
+        const float rx = rho_x[i], rz = rho_z[i], th = theta[i];
+        if (!std::isfinite(rx) || !std::isfinite(rz) || !std::isfinite(th)) return SYSMAT_ERR_ARG;
+        if (rx > 0.0f) {
+            // the hole's radius field bounds the ellipse: the cone test and the filters use it
+            const float r = col[100 + 9 * i + 4];
+            if (!(rz > 0.0f) || rx > r || rz > r) return SYSMAT_ERR_ARG;
+        }
+        h[3 * i] = rx > 0.0f ? rx : 0.0f;
+        h[3 * i + 1] = rz;
+        h[3 * i + 2] = th;
+    }
+    float* d_s = nullptr;
+    if (!ctx->d_shapes && cudaMalloc(&ctx->d_shapes, sizeof(float4) * (size_t)(n > 0 ? n : 1)) != cudaSuccess) {
+        ctx->d_shapes = nullptr;
+        return SYSMAT_ERR_NOMEM;
+    }
+    if (cudaMalloc(&d_s, sizeof(float) * h.size()) != cudaSuccess) return SYSMAT_ERR_NOMEM;
+    cudaError_t e = cudaMemcpy(d_s, h.data(), sizeof(float) * h.size(), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess && n > 0) {
+        derive_shapes<<<(n + 255) / 256, 256>>>(d_s, n, ctx->d_shapes);
+        e = cudaDeviceSynchronize();
+    }
+    cudaFree(d_s);
+    if (e != cudaSuccess) return SYSMAT_ERR_CUDA;
+    ctx->g.hole_shape = ctx->d_shapes;
     return SYSMAT_OK;
 }
 

@@ -127,8 +127,8 @@ extern "C" SYSMAT_API int sysmat_batch_create(sysmat_batch_plan** out, sysmat_ct
     if (!out || !ctxs || n_ctx < 1 || n_items < 0 || (n_items > 0 && !items)) return SYSMAT_ERR_ARG;
     *out = nullptr;
     const int device = ctxs[0] ? ctxs[0]->device : -1;
-    for (int c = 0; c < n_ctx; ++c)
-        if (!ctxs[c] || ctxs[c]->device != device) return SYSMAT_ERR_ARG;
+    for (int c = 0; c < n_ctx; ++c)   // elliptical holes are not supported by the batched kernel
+        if (!ctxs[c] || ctxs[c]->device != device || ctxs[c]->g.hole_shape) return SYSMAT_ERR_ARG;
     if (!device_is(device)) return SYSMAT_ERR_ARG;
     auto* p = new sysmat_batch_plan();
     p->device = device;

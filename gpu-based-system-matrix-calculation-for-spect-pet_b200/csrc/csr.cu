@@ -1,5 +1,5 @@
 // Dense block -> CSR on the device (entries with value > threshold), for streaming large
-// system matrices to the host in compressed form (SURVEY next-row: CSR at 1e-9).
+// system matrices to the host in compressed form (production matrices use 1e-9).
 //
 // Two passes over the dense block: a per-row count (one warp per row, ballot + popc), a
 // single-block exclusive scan of the counts into row pointers, then an ordered fill (one

@@ -31,6 +31,7 @@ struct sysmat_ctx {
     sysmat::PairRec* pairs = nullptr;
     sysmat::AttEntry* att = nullptr;
     double* d_kn_tab = nullptr;     // Klein-Nishina table for kn_e0
+    float4* d_shapes = nullptr;     // elliptical holes (sysmat_set_hole_shapes), or nullptr
     float kn_e0 = -1.0f;
 };
 

@@ -5,6 +5,7 @@
 // kernels use inline (PESysMatGen.cu:1058-1068, :1124-1135, :1159-1166;
 // scatter.cu:1465-1479), so they round exactly as the reference's own copies do.
 #include "pe.cuh"
+#include "../../include/sysmat.h"
 
 namespace sysmat {
 
@@ -37,4 +38,34 @@ __global__ void derive_holes(const float* __restrict__ col, float fov, int n, fl
     raw[h] = make_float4(p[0], p[1], p[2], p[3]);
 }
 
+// One thread per hole: (rho_x, rho_z, theta) -> (rho_x, rho_z, cos theta, sin theta), with the
+// float cos/sin the reference's elliptical chord evaluates (PESysMatGen.cu:832-836);
+// rho_x <= 0 marks a circular hole (stored as 0).
+__global__ void derive_shapes(const float* __restrict__ s, int n, float4* out)
+{
+    const int h = blockIdx.x * blockDim.x + threadIdx.x;
+    if (h >= n) return;
+    const float rx = s[3 * h], rz = s[3 * h + 1], th = s[3 * h + 2];
+    out[h] = rx > 0.0f ? make_float4(rx, rz, cosf(th), sinf(th)) : make_float4(0.0f, 0.0f, 1.0f, 0.0f);
+}
+
+// Diagnostic: the elliptical-cylinder chord on arrays of arguments (13 per item, as
+// sysmat_ell_chords documents), one thread per item.
+__global__ void ell_chords_kernel(const float* __restrict__ a, float* __restrict__ out, int n)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const float* p = a + 13 * (long long)i;
+    out[i] = ell_chord(p[0], p[1], p[2], p[3], p[4], p[5], p[6], p[7], p[8], p[9], p[10], p[11], cosf(p[12]),
+                       sinf(p[12]));
+}
+
 }  // namespace sysmat
+
+extern "C" SYSMAT_API int sysmat_ell_chords(const float* d_args, float* d_out, int n, void* stream)
+{
+    if (n < 0 || (n > 0 && (!d_args || !d_out))) return SYSMAT_ERR_ARG;
+    if (n == 0) return SYSMAT_OK;
+    sysmat::ell_chords_kernel<<<(n + 255) / 256, 256, 0, (cudaStream_t)stream>>>(d_args, d_out, n);
+    return cudaGetLastError() == cudaSuccess ? SYSMAT_OK : SYSMAT_ERR_CUDA;
+}

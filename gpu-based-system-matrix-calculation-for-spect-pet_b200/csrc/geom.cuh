@@ -62,6 +62,9 @@ struct DevGeom {
     const float* raw_det;   // Params_Detector as uploaded (bitmaps use raw, un-offset values)
     CrystalTables cry;
     HoleTables hole;
+    // optional elliptical holes (sysmat_set_hole_shapes): per hole (rho_x, rho_z, cos theta,
+    // sin theta), rho_x = 0 for a circular hole; nullptr when every hole is circular
+    const float4* hole_shape;
     LayerInfo layer[kMaxLayers];
 };
 
@@ -269,6 +272,67 @@ __device__ __forceinline__ float cyl_chord(float xi, float yi, float zi, float x
     if (eb <= 0.0001f || ea <= 0.0001f) return 0.0f;
     if (eb >= tio || ea >= tio) return 0.0f;
     return eb - ea;
+}
+
+// Chord through the y-parallel elliptical cylinder ((x'-xc)/rx)^2 + ((z'-zc)/rz)^2 <= 1,
+// y in [y1, y2], with the segment's points rotated by theta about the axis first
+// (PESysMatGen.cu:801-947, defined but not called by the reference kernels).  ct, st are
+// cos(theta), sin(theta) as the reference evaluates them; each expression is written as the
+// reference writes it, so nvcc contracts it the same way.
+__device__ __forceinline__ float ell_chord(float x_in, float y_in, float z_in, float x_out, float y_out,
+                                           float z_out, float xc, float y1, float y2, float zc, float rx,
+                                           float rz, float ct, float st)
+{
+    const float x_in_ = x_in - xc;
+    const float z_in_ = z_in - zc;
+    const float x_out_ = x_out - xc;
+    const float z_out_ = z_out - zc;
+    x_in = xc + x_in_ * ct + z_in_ * st;
+    z_in = zc - x_in_ * st + z_in_ * ct;
+    x_out = xc + x_out_ * ct + z_out_ * st;
+    z_out = zc - x_out_ * st + z_out_ * ct;
+    if (fabsf(y1 - y2) < 0.001f) return 0.0f;
+    const float tio = sqrtf((x_out - x_in) * (x_out - x_in) + (y_out - y_in) * (y_out - y_in) +
+                            (z_out - z_in) * (z_out - z_in));
+    const float kx = (x_out - x_in) / tio;
+    const float ky = (y_out - y_in) / tio;
+    const float kz = (z_out - z_in) / tio;
+    const float xl = x_in + kx / ky * (y1 - y_in);
+    const float xr = x_in + kx / ky * (y2 - y_in);
+    const float zl = z_in + kz / ky * (y1 - y_in);
+    const float zr = z_in + kz / ky * (y2 - y_in);
+    const float ta = (y1 - y_in) / ky;
+    const float tb = (y2 - y_in) / ky;
+    const bool fl = ((xl - xc) * (xl - xc) / rx / rx + (zl - zc) * (zl - zc) / rz / rz) <= 1.0f;
+    const bool fr = ((xr - xc) * (xr - xc) / rx / rx + (zr - zc) * (zr - zc) / rz / rz) <= 1.0f;
+    if (fr && fl) {
+        if (ta <= 0.0001f || tb <= 0.0001f) return 0.0f;
+        if (ta >= tio || tb >= tio) return 0.0f;
+        return fabsf(tb - ta);
+    }
+    const float x_ = x_in - xc;
+    const float z_ = z_in - zc;
+    const float a = (kx * kx * rz * rz + kz * kz * rx * rx);
+    const float b = kx * x_ * rz * rz + kz * z_ * rx * rx;
+    const float c = rz * rz * x_ * x_ + rx * rx * z_ * z_ - rx * rx * rz * rz;
+    const float delta = (b * b - a * c);
+    if (delta <= 0.00001f) return 0.0f;
+    const float t1 = (-b - sqrtf(delta)) / a;
+    const float t2 = (-b + sqrtf(delta)) / a;
+    if (!fr && !fl) {
+        if (!((t1 >= ta) && (t2 <= tb))) return 0.0f;
+        if (t2 <= 0.0001f || t1 <= 0.0001f) return 0.0f;
+        if (t2 >= tio || t1 >= tio) return 0.0f;
+        return t2 - t1;
+    }
+    if (fl && !fr) {
+        if (t2 <= 0.0001f || ta <= 0.0001f) return 0.0f;
+        if (t2 >= tio || ta >= tio) return 0.0f;
+        return t2 - ta;
+    }
+    if (tb <= 0.0001f || t1 <= 0.0001f) return 0.0f;
+    if (tb >= tio || t1 >= tio) return 0.0f;
+    return tb - t1;
 }
 
 // World point -> frame of a crystal rotated about y, given cos(-rot), sin(-rot)

@@ -333,6 +333,7 @@ __device__ __forceinline__ bool capsule_meets_box(float xo, float zo, float y0, 
 // the round buffer from position n, with their geometry (one entry per lane); returns the
 // new count.  Stops before the buffer could overflow; *next receives the first entry not
 // examined.
+template <bool ELL>
 __device__ __forceinline__ int fill_round(const DevGeom& g, WarpSmem& ws, const Elem& e, int k0, int k1,
                                           float4 box, int n, int lane, int* next, int* nh)
 {
@@ -370,6 +371,7 @@ __device__ __forceinline__ int fill_round(const DevGeom& g, WarpSmem& ws, const 
                 const float4 hb = __ldg(&g.hole.b[id]);
                 ws.ra[pos] = make_float4(ha.x, ha.w, hb.x, hb.y);
                 ws.rb[pos] = make_float4(ha.y, ha.z, 0.0f, 0.0f);
+                if constexpr (ELL) ws.rc[pos] = __ldg(&g.hole_shape[id]);   // rho_x, rho_z, cos, sin
                 ws.rl[pos] = layer_of_hole(g, id);
             } else {
                 const int o = id - g.n_holes;
@@ -395,6 +397,7 @@ __device__ __forceinline__ int fill_round(const DevGeom& g, WarpSmem& ws, const 
 // Walk round-buffer entries [0, nr) for one sub-element ray (voxel -> (xD, yD, zD)); holes
 // occupy [0, nh) and crystals [nh, nr), both in the reference's object order; the layer
 // terms are added when the walk leaves a layer.
+template <bool ELL>
 __device__ __forceinline__ void walk_round(const DevGeom& g, const WarpSmem& ws, int nh, int nr,
                                            float xD, float yD, float zD, float sa_a, float sa_b,
                                            float cosang, RayCyl& rc, Walk& s)
@@ -405,8 +408,19 @@ __device__ __forceinline__ void walk_round(const DevGeom& g, const WarpSmem& ws,
         if (!in_rect(ws.rr[j], sa_a, sa_b)) continue;
         const float4 A = ws.ra[j];
         const float4 B = ws.rb[j];
-        ray_cyl_caps(rc, B.x, B.y);
-        const float tmp = ray_cyl_chord(rc, A.x, A.y, A.z);
+        float tmp;
+        if constexpr (ELL) {
+            const float4 S = ws.rc[j];
+            if (S.x > 0.0f) {                                    // elliptical hole
+                tmp = ell_chord(rc.xi, rc.yi, rc.zi, xD, yD, zD, A.x, B.x, B.y, A.y, S.x, S.y, S.z, S.w);
+            } else {
+                ray_cyl_caps(rc, B.x, B.y);
+                tmp = ray_cyl_chord(rc, A.x, A.y, A.z);
+            }
+        } else {
+            ray_cyl_caps(rc, B.x, B.y);
+            tmp = ray_cyl_chord(rc, A.x, A.y, A.z);
+        }
         s.len = s.len + tmp;                                     // :1276-1278
         s.att = s.att + A.w * tmp;
         s.hole_hits += (tmp != 0.0f);
@@ -553,7 +567,7 @@ __device__ __forceinline__ bool init_element(const DevGeom& g, WarpSmem& ws, int
     return true;
 }
 
-template <int MODE, bool COUNT>
+template <int MODE, bool COUNT, bool ELL = false>
 __device__ double pe_element(const DevGeom& g, const BlockSmem& bs, WarpSmem& ws, int d,
                              long long v, float cr, float sr, int lane,
                              unsigned long long* counters)
@@ -608,9 +622,9 @@ __device__ double pe_element(const DevGeom& g, const BlockSmem& bs, WarpSmem& ws
             int k = 0;
             while (k < count) {
                 int next = count, nh = 0;
-                const int nr = fill_round(g, ws, e, k, count, box, 0, lane, &next, &nh);
+                const int nr = fill_round<ELL>(g, ws, e, k, count, box, 0, lane, &next, &nh);
                 if constexpr (COUNT) n_sub_entries += nr;
-                if (!skip) walk_round(g, ws, nh, nr, q.xD, q.yD, q.zD, q.sa_a, q.sa_b, q.cosang, rc, s);
+                if (!skip) walk_round<ELL>(g, ws, nh, nr, q.xD, q.yD, q.zD, q.sa_a, q.sa_b, q.cosang, rc, s);
                 __syncwarp();
                 k = next;
             }
@@ -738,7 +752,7 @@ struct BrickOut {
 // One work item: crystal det_begin + di against one voxel brick of bx x by x bz voxels (brick
 // (gx, gy, gz) of the block's grid starting at z-plane iz0).  The block builds the cone
 // superset of the brick, then its warps take the brick's voxels in turn.
-template <int MODE, bool COUNT>
+template <int MODE, bool COUNT, bool ELL = false>
 __device__ __forceinline__ void pe_brick(const DevGeom& g, BlockSmem& bs, WarpSmem& ws, int lane, int wid,
                                          const BrickOut& O, int di, int gx, int gy, int gz, int iz0, int iz1,
                                          int bx, int by, int bz, float cr, float sr,
@@ -762,14 +776,14 @@ __device__ __forceinline__ void pe_brick(const DevGeom& g, BlockSmem& bs, WarpSm
         if (ix >= g.nx || iy >= g.ny || iz > z1) continue;
         const long long v = ix + g.nx * ((long long)iy + (long long)g.ny * iz);
         if (v < O.vox_begin || v > O.vlast) continue;
-        const float val = (float)pe_element<MODE, COUNT>(g, bs, ws, d, v, cr, sr, lane, counters);
+        const float val = (float)pe_element<MODE, COUNT, ELL>(g, bs, ws, d, v, cr, sr, lane, counters);
         if (lane == 0) O.out[(long long)di * O.ld + (v - O.vox_begin)] = val;
         __syncwarp();
     }
     __syncthreads();
 }
 
-template <int MODE, bool COUNT>
+template <int MODE, bool COUNT, bool ELL>
 __global__ void __launch_bounds__(kThreads, 2) pe_kernel(DevGeom g, PeLaunch L)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -798,8 +812,8 @@ __global__ void __launch_bounds__(kThreads, 2) pe_kernel(DevGeom g, PeLaunch L)
         const int gz = (int)(b / ((long long)nbx * nby));
         const int rem = (int)(b - (long long)gz * nbx * nby);
         const int gy = rem / nbx, gx = rem - gy * nbx;
-        pe_brick<MODE, COUNT>(g, bs, ws, lane, wid, O, di, gx, gy, gz, iz0, iz1, bx, by, bz, cr, sr,
-                              L.counters);
+        pe_brick<MODE, COUNT, ELL>(g, bs, ws, lane, wid, O, di, gx, gy, gz, iz0, iz1, bx, by, bz, cr, sr,
+                                   L.counters);
     }
 }
 
@@ -866,7 +880,7 @@ __global__ void __launch_bounds__(kThreads, 2) pe_batch_kernel(BatchLaunch B)
 
 }  // namespace
 
-template <int MODE, bool COUNT>
+template <int MODE, bool COUNT, bool ELL>
 static int launch_mode(const DevGeom& g, const PeLaunch& L, int num_sms, cudaStream_t stream)
 {
     const int smem = (int)sizeof(BlockSmem);
@@ -875,15 +889,15 @@ static int launch_mode(const DevGeom& g, const PeLaunch& L, int num_sms, cudaStr
     if (cudaGetDevice(&dev) != cudaSuccess) return -1;
     const unsigned long long bit = 1ull << (dev & 63);
     if (!(__atomic_load_n(&configured, __ATOMIC_ACQUIRE) & bit)) {
-        if (cudaFuncSetAttribute(pe_kernel<MODE, COUNT>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem) !=
+        if (cudaFuncSetAttribute(pe_kernel<MODE, COUNT, ELL>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem) !=
             cudaSuccess)
             return -1;
         __atomic_fetch_or(&configured, bit, __ATOMIC_RELEASE);
     }
     int per_sm = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, pe_kernel<MODE, COUNT>, kThreads, smem);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, pe_kernel<MODE, COUNT, ELL>, kThreads, smem);
     if (per_sm < 1) per_sm = 1;
-    pe_kernel<MODE, COUNT><<<num_sms * per_sm, kThreads, smem, stream>>>(g, L);
+    pe_kernel<MODE, COUNT, ELL><<<num_sms * per_sm, kThreads, smem, stream>>>(g, L);
     return cudaGetLastError() == cudaSuccess ? 0 : -1;
 }
 
@@ -953,9 +967,14 @@ int launch_pe_batch(const BatchLaunch& B, int mode, int grid, cudaStream_t strea
 
 int launch_pe(const DevGeom& g, const PeLaunch& L, int mode, int num_sms, cudaStream_t stream)
 {
-    if (L.counters) return launch_mode<0, true>(g, L, num_sms, stream);
-    return mode == 0 ? launch_mode<0, false>(g, L, num_sms, stream)
-                     : launch_mode<1, false>(g, L, num_sms, stream);
+    if (g.hole_shape) {                   // systems with elliptical holes
+        if (L.counters) return launch_mode<0, true, true>(g, L, num_sms, stream);
+        return mode == 0 ? launch_mode<0, false, true>(g, L, num_sms, stream)
+                         : launch_mode<1, false, true>(g, L, num_sms, stream);
+    }
+    if (L.counters) return launch_mode<0, true, false>(g, L, num_sms, stream);
+    return mode == 0 ? launch_mode<0, false, false>(g, L, num_sms, stream)
+                     : launch_mode<1, false, false>(g, L, num_sms, stream);
 }
 
 }  // namespace sysmat

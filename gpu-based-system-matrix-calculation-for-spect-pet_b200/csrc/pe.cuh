@@ -78,5 +78,6 @@ __global__ void derive_crystals(const float* __restrict__ det, float fov, int n,
                                 float4* size, float4* mu, float4* trig);
 __global__ void derive_holes(const float* __restrict__ col, float fov, int n, float4* a, float4* b,
                              float4* raw);
+__global__ void derive_shapes(const float* __restrict__ s, int n, float4* out);
 
 }  // namespace sysmat

@@ -207,7 +207,7 @@ __device__ __forceinline__ void pe_element_grad(const DevGeom& g, const BlockSme
             int k = 0;
             while (k < count) {
                 int next = count, nh = 0;
-                const int nr = fill_round(g, ws, e, k, count, box, 0, lane, &next, &nh);
+                const int nr = fill_round<false>(g, ws, e, k, count, box, 0, lane, &next, &nh);
                 if (!skip) walk_round_grad(g, ws, nh, nr, q.xD, q.yD, q.zD, q.sa_a, q.sa_b, q.cosang, rc, s);
                 __syncwarp();
                 k = next;

@@ -35,8 +35,8 @@ EXPORTS = ("PESysMatGen", "scatter", "scatter_collimator", "scatter_crystal", "s
            "sysmat_scatter_prepare", "sysmat_scatter", "sysmat_pe_noalloc", "sysmat_csr_count",
            "sysmat_csr_fill", "sysmat_pe_work", "sysmat_batch_create", "sysmat_batch_set_tiles",
            "sysmat_batch_get_tiles", "sysmat_batch_tune", "sysmat_batch_run", "sysmat_batch_destroy",
-           "sysmat_batch", "sysmat_project", "sysmat_vjp", "sysmat_backproject",
-           "sysmat_measure_peaks",
+           "sysmat_batch", "sysmat_set_hole_shapes", "sysmat_pe_csr_file", "sysmat_project", "sysmat_vjp", "sysmat_backproject",
+           "sysmat_measure_peaks", "sysmat_ell_chords",
            "sysmat_error_string", "sysmat_version")
 
 _fp = ctypes.POINTER(ctypes.c_float)
@@ -109,10 +109,14 @@ def lib():
             "sysmat_batch_destroy": ([_vp], ctypes.c_int),
             "sysmat_batch": ([ctypes.POINTER(_vp), ctypes.c_int, ctypes.POINTER(BatchItem), ctypes.c_int,
                               ctypes.c_int, _vp], ctypes.c_int),
+            "sysmat_set_hole_shapes": ([_vp, _fp, _fp, _fp], ctypes.c_int),
+            "sysmat_pe_csr_file": ([_vp, ctypes.c_float, ctypes.c_char_p, ctypes.c_float, ctypes.c_int, ctypes.c_int,
+                                    ctypes.POINTER(ctypes.c_longlong), _vp], ctypes.c_int),
             "sysmat_project": ([_vp, ctypes.c_float, ctypes.c_int, ctypes.c_int, _vp, _vp, _vp], ctypes.c_int),
             "sysmat_vjp": ([_vp, ctypes.c_float, ctypes.c_int, ctypes.c_int, _vp, _vp, _vp, _vp], ctypes.c_int),
             "sysmat_backproject": ([_vp, ctypes.c_float, ctypes.c_int, ctypes.c_int, _vp, _vp, _vp],
                                    ctypes.c_int),
+            "sysmat_ell_chords": ([_vp, _vp, ctypes.c_int, _vp], ctypes.c_int),
             "sysmat_error_string": ([ctypes.c_int], ctypes.c_char_p),
             "sysmat_version": ([], ctypes.c_char_p),
         }
@@ -312,6 +316,63 @@ def _context_backproject(self, u, rotation=0.0, det_begin=0, det_count=None, str
     return q
 
 
+def _context_pe_csr_file(self, path, rotation=0.0, threshold=1e-9, mode=MODE_REFERENCE, rows_per_block=0,
+                         stream=None):
+    """Whole PE matrix of one rotation to a compressed file (sysmat_pe_csr_file); returns nnz."""
+    n = ctypes.c_longlong()
+    _check(lib().sysmat_pe_csr_file(self.handle, float(rotation), os.fsencode(path), float(threshold), mode,
+                                    int(rows_per_block), ctypes.byref(n), _stream(stream)), "sysmat_pe_csr_file")
+    return n.value
+
+
+def read_csr_file(path):
+    """Read a sysmat_pe_csr_file file: (rows, cols, threshold, mode, row_ptr int64, col int64,
+    val float32), rows assembled in order."""
+    with open(path, "rb") as f:
+        head = f.read(40)
+        if head[:8] != b"SMCSR001":
+            raise ValueError(f"{path}: not a sysmat CSR file")
+        rows, cols = np.frombuffer(head[8:24], dtype=np.int64)
+        threshold = float(np.frombuffer(head[24:28], dtype=np.float32)[0])
+        mode = int(np.frombuffer(head[28:32], dtype=np.int32)[0])
+        ptr = [np.zeros(1, dtype=np.int64)]
+        cols_l, vals_l = [], []
+        base = 0
+        next_row = 0
+        while True:
+            b = f.read(24)
+            if not b:
+                break
+            d0, n, nnz = np.frombuffer(b, dtype=np.int64)
+            if d0 != next_row:
+                raise ValueError(f"{path}: block starts at row {d0}, expected {next_row}")
+            rp = np.frombuffer(f.read(8 * (n + 1)), dtype=np.int64)
+            cols_l.append(np.frombuffer(f.read(8 * nnz), dtype=np.int64))
+            vals_l.append(np.frombuffer(f.read(4 * nnz), dtype=np.float32))
+            ptr.append(rp[1:] + base)
+            base += int(nnz)
+            next_row += int(n)
+    if next_row != rows:
+        raise ValueError(f"{path}: {next_row} rows of {rows}")
+    cat = (lambda xs, t: np.concatenate(xs) if xs else np.zeros(0, dtype=t))
+    return int(rows), int(cols), threshold, mode, np.concatenate(ptr), cat(cols_l, np.int64), cat(vals_l, np.float32)
+
+
+def _context_set_hole_shapes(self, shapes=None):
+    """shapes: (n_holes, 3) rows (rho_x, rho_z, theta), rho_x <= 0 for a circular hole; None
+    restores circular holes (sysmat_set_hole_shapes)."""
+    if shapes is None:
+        _check(lib().sysmat_set_hole_shapes(self.handle, None, None, None), "sysmat_set_hole_shapes")
+        return
+    a = np.ascontiguousarray(np.asarray(shapes, dtype=np.float32).reshape(-1, 3))
+    cols = [np.ascontiguousarray(a[:, k]) for k in range(3)]
+    self._shapes = cols
+    _check(lib().sysmat_set_hole_shapes(self.handle, *[c.ctypes.data_as(_fp) for c in cols]),
+           "sysmat_set_hole_shapes")
+
+
+Context.set_hole_shapes = _context_set_hole_shapes
+Context.pe_csr_file = _context_pe_csr_file
 Context.project = _context_project
 Context.vjp = _context_vjp
 Context.backproject = _context_backproject
@@ -374,6 +435,15 @@ def batch(contexts, items, mode=MODE_REFERENCE, stream=None):
     """One-shot batched PE (sysmat_batch): create, run, synchronise, destroy."""
     ctxs, arr = _batch_items(contexts, items)
     _check(lib().sysmat_batch(ctxs, len(contexts), arr, len(items), mode, _stream(stream)), "sysmat_batch")
+
+
+def ell_chords(args, stream=None):
+    """Device elliptical-cylinder chord on a CUDA float32 tensor of (n, 13) arguments."""
+    import torch
+    args = args.contiguous()
+    out = torch.empty(args.shape[0], dtype=torch.float32, device=args.device)
+    _check(lib().sysmat_ell_chords(_ptr(args), _ptr(out), args.shape[0], _stream(stream)), "sysmat_ell_chords")
+    return out
 
 
 def measure_peaks():

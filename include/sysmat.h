@@ -127,6 +127,27 @@ SYSMAT_API int sysmat_scatter(sysmat_ctx* ctx, int parts, int hole_model, float 
                               const float* d_pe, int det_begin, int det_count, long long vox_begin,
                               long long vox_count, float* d_out, long long ld, void* stream);
 
+/* Elliptical holes (an extension: the reference defines length_ellipticalcylinder_ray,
+ * PESysMatGen.cu:801-947, but its kernels never call it and its parameter files have no
+ * field for it).  Host arrays of n_holes values: hole h is the cylinder
+ * ((x'-x)/rho_x)^2 + ((z'-z)/rho_z)^2 <= 1 in its frame rotated by theta[h] (radians), with
+ * the reference's chord; rho_x[h] <= 0 keeps it circular.  The hole's radius field in
+ * Params_Collimator must bound both semi-axes (the reference cone test and the kernel's
+ * filters use it).  rho_x = NULL restores circular holes.  Applies to sysmat_pe (and the
+ * entry points built on it); the batched and adjoint paths reject such contexts. */
+SYSMAT_API int sysmat_set_hole_shapes(sysmat_ctx* ctx, const float* rho_x, const float* rho_z, const float* theta);
+
+/* Whole photoelectric matrix of rotation `rotation` written to `path` in compressed form
+ * (entries > threshold), computed and compressed on the device in blocks of rows_per_block
+ * detector rows (0: about 1 GB of dense block) and streamed to the file.  The reference CLI
+ * writes the dense D*V floats instead (PEGen_CircularHole.cpp:141-147).  File layout:
+ * "SMCSR001", int64 rows, int64 cols, float threshold, int32 mode, int64 reserved; then
+ * blocks of (int64 first_row, int64 n_rows, int64 nnz, int64 row_ptr[n_rows+1], int64
+ * col[nnz], float val[nnz]).  *nnz_total (may be NULL) receives the total.  Synchronous on
+ * `stream`; allocates its block buffers for the duration of the call. */
+SYSMAT_API int sysmat_pe_csr_file(sysmat_ctx* ctx, float rotation, const char* path, float threshold, int mode,
+                                  int rows_per_block, long long* nnz_total, void* stream);
+
 /* ---- Batched photoelectric launches --------------------------------------------------------
  * Many (system, rotation, block) tasks in one persistent launch over a device work queue.
  * No reference counterpart: the reference computes one rotation of one system per call
@@ -244,6 +265,11 @@ SYSMAT_API int sysmat_pe_work(sysmat_ctx* ctx, float rotation, int det_begin, in
 /* Measured FP32 FMA throughput (TFLOP/s, FMA = 2 flops) and MUFU throughput (Tops/s) of
  * the current device, from two short calibration kernels. */
 SYSMAT_API int sysmat_measure_peaks(double* fp32_tflops, double* mufu_tops);
+
+/* Diagnostic: the elliptical-cylinder chord used for elliptical holes, on n device items of
+ * 13 floats (x_in, y_in, z_in, x_out, y_out, z_out, x, y1, y2, z, rho_x, rho_z, theta), in
+ * the argument order of the reference's length_ellipticalcylinder_ray (PESysMatGen.cu:801). */
+SYSMAT_API int sysmat_ell_chords(const float* d_args, float* d_out, int n, void* stream);
 
 /* Text for a SYSMAT_ERR_* code. */
 SYSMAT_API const char* sysmat_error_string(int code);

@@ -46,7 +46,10 @@ def lib():
         L.oracle_bitmap_collimator_words.restype = ctypes.c_longlong
         L.oracle_bitmap_crystal.argtypes = [_fp, _u32p, ctypes.c_int]
         L.oracle_bitmap_collimator.argtypes = [_fp, _fp, _u32p, ctypes.c_int]
-        for name in ("oracle_box_chord", "oracle_box_chord_inside", "oracle_cyl_chord"):
+        L.oracle_pe_shapes.argtypes = [_fp, _fp, _fp, _fp, ctypes.c_int, _ip, ctypes.c_int, ctypes.c_longlong,
+                                       ctypes.c_longlong, _dp, _i64p, ctypes.c_int]
+        L.oracle_pe_shapes.restype = ctypes.c_int
+        for name in ("oracle_box_chord", "oracle_box_chord_inside", "oracle_cyl_chord", "oracle_ell_chord"):
             getattr(L, name).argtypes = [ctypes.c_int, _dp]
             getattr(L, name).restype = ctypes.c_double
         L.oracle_scatter_trace.argtypes = [_fp, _fp, _fp, _fp, _fp, _u32p, ctypes.c_int, ctypes.c_int,
@@ -70,9 +73,11 @@ def _dets(geo, dets):
     return d, d.ctypes.data_as(_ip)
 
 
-def pe(geo, prec=64, dets=None, v0=0, nv=None, threads=0, counts=False):
+def pe(geo, prec=64, dets=None, v0=0, nv=None, threads=0, counts=False, shapes=None):
     """PE elements (len(dets), nv) as float64; with counts=True also the per-element work
-    counts (subelements, hole hits, crystal hits, candidate crystals, candidate holes)."""
+    counts (subelements, hole hits, crystal hits, candidate crystals, candidate holes).
+    shapes: optional (n_holes, 3) float32 rows (rho_x, rho_z, theta); rho_x > 0 marks an
+    elliptical hole (the reference's length_ellipticalcylinder_ray)."""
     nv = geo.n_vox - v0 if nv is None else nv
     c, pc = _f32(geo.collimator)
     d, pd = _f32(geo.detector)
@@ -80,11 +85,22 @@ def pe(geo, prec=64, dets=None, v0=0, nv=None, threads=0, counts=False):
     dd, pdd = _dets(geo, dets)
     out = np.zeros((dd.size, nv), dtype=np.float64)
     cnt = np.zeros((dd.size, nv, 5), dtype=np.int64) if counts else None
-    rc = lib().oracle_pe(pc, pd, pi, prec, pdd, dd.size, v0, nv, out.ctypes.data_as(_dp),
-                         cnt.ctypes.data_as(_i64p) if counts else None, threads)
+    if shapes is not None:
+        sh, psh = _f32(np.asarray(shapes, dtype=np.float32).reshape(-1))
+        rc = lib().oracle_pe_shapes(pc, pd, pi, psh, prec, pdd, dd.size, v0, nv, out.ctypes.data_as(_dp),
+                                    cnt.ctypes.data_as(_i64p) if counts else None, threads)
+    else:
+        rc = lib().oracle_pe(pc, pd, pi, prec, pdd, dd.size, v0, nv, out.ctypes.data_as(_dp),
+                             cnt.ctypes.data_as(_i64p) if counts else None, threads)
     if rc:
         raise RuntimeError(f"oracle_pe failed ({rc})")
     return (out, cnt) if counts else out
+
+
+def ell_chord(args, prec=64):
+    """The reference's elliptical-cylinder chord on 13 arguments (see oracle_ell_chord)."""
+    a = np.ascontiguousarray(np.asarray(args, dtype=np.float64))
+    return lib().oracle_ell_chord(prec, a.ctypes.data_as(_dp))
 
 
 def bitmap_crystal(geo, threads=0):

@@ -161,6 +161,57 @@ static REAL FN(cyl_chord)(REAL xi, REAL yi, REAL zi, REAL xo, REAL yo, REAL zo,
     return eb - ea;
 }
 
+/* Chord through the y-parallel elliptical cylinder ((x'-xc)/rx)^2 + ((z'-zc)/rz)^2 <= 1,
+ * y in [y1, y2], where (x', z') are the ray's points rotated by theta about the axis
+ * (PESysMatGen.cu:801-947; defined there but not called by the reference kernels).
+ * ct, st: cos(theta), sin(theta). */
+static REAL FN(ell_chord)(REAL xi, REAL yi, REAL zi, REAL xo, REAL yo, REAL zo, REAL xc, REAL y1,
+                          REAL y2, REAL zc, REAL rx, REAL rz, REAL ct, REAL st)
+{
+    REAL xi_ = xi - xc, zi_ = zi - zc, xo_ = xo - xc, zo_ = zo - zc;
+    xi = xc + xi_ * ct + zi_ * st;
+    zi = zc - xi_ * st + zi_ * ct;
+    xo = xc + xo_ * ct + zo_ * st;
+    zo = zc - xo_ * st + zo_ * ct;
+    if ((double)FABS(y1 - y2) < 0.001) return 0;
+    REAL tio = SQRT((xo - xi) * (xo - xi) + (yo - yi) * (yo - yi) + (zo - zi) * (zo - zi));
+    REAL kx = (xo - xi) / tio, ky = (yo - yi) / tio, kz = (zo - zi) / tio;
+    REAL xl = xi + kx / ky * (y1 - yi);
+    REAL xr = xi + kx / ky * (y2 - yi);
+    REAL zl = zi + kz / ky * (y1 - yi);
+    REAL zr = zi + kz / ky * (y2 - yi);
+    REAL ta = (y1 - yi) / ky, tb = (y2 - yi) / ky;
+    int fl = ((xl - xc) * (xl - xc) / rx / rx + (zl - zc) * (zl - zc) / rz / rz) <= 1;
+    int fr = ((xr - xc) * (xr - xc) / rx / rx + (zr - zc) * (zr - zc) / rz / rz) <= 1;
+    if (fr && fl) {
+        if ((double)ta <= 0.0001 || (double)tb <= 0.0001) return 0;
+        if (ta >= tio || tb >= tio) return 0;
+        return FABS(tb - ta);
+    }
+    REAL x_ = xi - xc, z_ = zi - zc;
+    REAL a = kx * kx * rz * rz + kz * kz * rx * rx;
+    REAL b = kx * x_ * rz * rz + kz * z_ * rx * rx;
+    REAL c = rz * rz * x_ * x_ + rx * rx * z_ * z_ - rx * rx * rz * rz;
+    REAL delta = b * b - a * c;
+    if ((double)delta <= 0.00001) return 0;
+    REAL t1 = (-b - SQRT(delta)) / a;
+    REAL t2 = (-b + SQRT(delta)) / a;
+    if (!fr && !fl) {
+        if (!(t1 >= ta && t2 <= tb)) return 0;
+        if ((double)t2 <= 0.0001 || (double)t1 <= 0.0001) return 0;
+        if (t2 >= tio || t1 >= tio) return 0;
+        return t2 - t1;
+    }
+    if (fl && !fr) {
+        if ((double)t2 <= 0.0001 || (double)ta <= 0.0001) return 0;
+        if (t2 >= tio || ta >= tio) return 0;
+        return t2 - ta;
+    }
+    if ((double)tb <= 0.0001 || (double)t1 <= 0.0001) return 0;
+    if (tb >= tio || t1 >= tio) return 0;
+    return tb - t1;
+}
+
 /* ---------------------------------------------------------------------------------- */
 /* Geometry decoding shared by the element functions.                                  */
 
@@ -322,9 +373,18 @@ static REAL FN(pe_element)(const ogeo* g, int d, long long v, int* cand_c, int* 
             REAL mu_layer = (REAL)C[(m + 1) * 10 + 5];
             for (int j = 0; j < ncand_h[m]; ++j) {
                 int h = cand_h[hoff + j];
-                REAL tmp = FN(cyl_chord)(xI, yI, zI, xD, yD, zD, (REAL)C[h * 9 + 100],
-                                         (REAL)C[h * 9 + 101] + fov, (REAL)C[h * 9 + 102] + fov,
-                                         (REAL)C[h * 9 + 103], (REAL)C[h * 9 + 104]);
+                REAL tmp;
+                if (g->S && g->S[3 * h] > 0.0f) {               /* elliptical hole (extension) */
+                    const REAL th = (REAL)g->S[3 * h + 2];
+                    tmp = FN(ell_chord)(xI, yI, zI, xD, yD, zD, (REAL)C[h * 9 + 100],
+                                        (REAL)C[h * 9 + 101] + fov, (REAL)C[h * 9 + 102] + fov,
+                                        (REAL)C[h * 9 + 103], (REAL)g->S[3 * h], (REAL)g->S[3 * h + 1],
+                                        COS(th), SIN(th));
+                } else {
+                    tmp = FN(cyl_chord)(xI, yI, zI, xD, yD, zD, (REAL)C[h * 9 + 100],
+                                        (REAL)C[h * 9 + 101] + fov, (REAL)C[h * 9 + 102] + fov,
+                                        (REAL)C[h * 9 + 103], (REAL)C[h * 9 + 104]);
+                }
                 if (cnt && tmp != 0) cnt->hole_hits++;
                 len = len + tmp;
                 att = att + (REAL)C[h * 9 + 105] * tmp;

@@ -124,3 +124,16 @@ def scatter(geo, pe_matrix, variant: str = "combined", cuda_id: int = 0, workdir
     if ret not in (V, 0, None) and variant != "combined":
         pass
     return out.reshape(D, V), bitmaps
+
+
+def ell_chords(args, cuda_id: int = 0) -> np.ndarray:
+    """The reference's length_ellipticalcylinder_ray on rows of 13 arguments (x_in, y_in, z_in,
+    x_out, y_out, z_out, xc, y1, y2, zc, rho_x, rho_z, theta), evaluated by a test kernel
+    compiled with the unmodified reference source (oracle/ref/ref_ell.cu)."""
+    a, pa = _f(np.asarray(args, dtype=np.float32).reshape(-1, 13))
+    n = a.shape[0]
+    out = np.zeros(n, dtype=np.float32)
+    rc = _load("libref_ell.so").ref_ell_chords(pa, out.ctypes.data_as(_fp), ctypes.c_int(n), ctypes.c_int(cuda_id))
+    if rc != 0:
+        raise RuntimeError(f"ref_ell_chords failed ({rc})")
+    return out

@@ -29,6 +29,7 @@
 
 typedef struct {
     const float *C, *D, *I, *P;
+    const float* S;    /* optional hole shapes: rho_x, rho_z, theta per hole (rho_x <= 0: circle) */
     int L, ncry, nx, ny, nz, nh0, nholes;
     long long nvox;
     int nh[MAX_LAYERS];
@@ -99,11 +100,12 @@ static int parse(ogeo* g, const float* C, const float* D, const float* I, const 
 /* PE elements for detectors dets[0..ndet) and voxels [v0, v0+nv), row-major into out
  * (ndet x nv).  prec: 32 or 64.  counts (optional, ndet*nv*5 int64) receives the
  * instrumented work counts per element. */
-int oracle_pe(const float* C, const float* D, const float* I, int prec, const int* dets, int ndet,
-              long long v0, long long nv, double* out, long long* counts, int nthreads)
+int oracle_pe_shapes(const float* C, const float* D, const float* I, const float* S, int prec, const int* dets,
+                     int ndet, long long v0, long long nv, double* out, long long* counts, int nthreads)
 {
     ogeo g;
     if (parse(&g, C, D, I, NULL)) return -1;
+    g.S = S;
     if (nthreads > 0) omp_set_num_threads(nthreads);
     long long total = (long long)ndet * nv;
     int err = 0;
@@ -135,6 +137,12 @@ int oracle_pe(const float* C, const float* D, const float* I, int prec, const in
         free(ch);
     }
     return err ? -2 : 0;
+}
+
+int oracle_pe(const float* C, const float* D, const float* I, int prec, const int* dets, int ndet,
+              long long v0, long long nv, double* out, long long* counts, int nthreads)
+{
+    return oracle_pe_shapes(C, D, I, NULL, prec, dets, ndet, v0, nv, out, counts, nthreads);
 }
 
 /* Scatter elements.  part: 1 crystal scatter, 2 collimator scatter (combined program's
@@ -271,6 +279,17 @@ double oracle_cyl_chord(int prec, const double* a)
                              (float)a[5], (float)a[6], (float)a[7], (float)a[8], (float)a[9],
                              (float)a[10]);
     return cyl_chord_f64(a[0], a[1], a[2], a[3], a[4], a[5], a[6], a[7], a[8], a[9], a[10]);
+}
+
+/* a: 13 values (x_in, y_in, z_in, x_out, y_out, z_out, xc, y1, y2, zc, rho_x, rho_z, theta). */
+double oracle_ell_chord(int prec, const double* a)
+{
+    if (prec == 32)
+        return ell_chord_f32((float)a[0], (float)a[1], (float)a[2], (float)a[3], (float)a[4], (float)a[5],
+                             (float)a[6], (float)a[7], (float)a[8], (float)a[9], (float)a[10], (float)a[11],
+                             cosf((float)a[12]), sinf((float)a[12]));
+    return ell_chord_f64(a[0], a[1], a[2], a[3], a[4], a[5], a[6], a[7], a[8], a[9], a[10], a[11], cos(a[12]),
+                         sin(a[12]));
 }
 
 double oracle_kn_sum(int prec, double e0, double lo, double hi)

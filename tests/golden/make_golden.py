@@ -106,6 +106,31 @@ def cases():
     return out
 
 
+def ellipse_args(n=4000, seed=17):
+    """Seeded arguments for the elliptical-cylinder chord: rays from a voxel region to a
+    detector region crossing a plate at y in [40, 50], ellipses near the crossing (semi-axes
+    0.3-1.5 mm, any orientation), with a tenth of them circles."""
+    rng = np.random.default_rng(seed)
+    a = np.zeros((n, 13), dtype=np.float32)
+    xi, yi, zi = rng.uniform(-20, 20, n), rng.uniform(-30, 0, n), rng.uniform(-20, 20, n)
+    xo, yo, zo = rng.uniform(-30, 30, n), np.full(n, 60.0), rng.uniform(-30, 30, n)
+    yy = rng.uniform(40, 50, n)
+    s = (yy - yi) / (yo - yi)
+    rx, rz = rng.uniform(0.3, 1.5, n), rng.uniform(0.3, 1.5, n)
+    circ = rng.random(n) < 0.1
+    rz[circ] = rx[circ]
+    xc = xi + s * (xo - xi) + rng.normal(0, 1.0, n)
+    zc = zi + s * (zo - zi) + rng.normal(0, 1.0, n)
+    a[:] = np.stack([xi, yi, zi, xo, yo, zo, xc, np.full(n, 40.0), np.full(n, 50.0), zc, rx, rz,
+                     rng.uniform(0, np.pi, n)], 1)
+    return a
+
+
+def ellipse_case(outdir):
+    args = ellipse_args()
+    np.savez_compressed(os.path.join(outdir, "ellipse_chords.npz"), args=args, ref=ref_lib.ell_chords(args))
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--out", default="gpurun_out/golden")
@@ -119,6 +144,8 @@ def main():
         if args.only and name not in args.only.split(","):
             continue
         run_case(name, geo, variants, args.out, timings)
+    if not args.only or "ellipse" in args.only.split(","):
+        ellipse_case(args.out)
     with open(os.path.join(args.out, "timings.json"), "w") as f:
         json.dump(timings, f, indent=1)
     print(json.dumps(timings))

@@ -45,3 +45,32 @@ def test_csr_of_a_strided_pe_block_rebuilds_the_dense_block(gpu):
     ref = np.where(ref > 1e-9, ref, 0.0)
     assert np.array_equal(dense[:, 24:1024], ref)
     assert p[-1] > 0
+
+
+@pytest.mark.parametrize("rows_per_block,threshold", [(7, 1e-9), (0, 1e-9), (100, 0.0)])
+def test_pe_csr_file_rebuilds_the_thresholded_matrix(gpu, tmp_path, rows_per_block, threshold):
+    """The whole matrix of a rotation streamed to a compressed file, block by block, reads back
+    as the dense matrix with entries <= threshold dropped."""
+    geo, _ = golden("config1")
+    ctx = sysmat.Context(geo)
+    dense = gpu.empty((ctx.n_det, ctx.n_vox), dtype=gpu.float32, device="cuda")
+    ctx.pe(dense)
+    a = dense.cpu().numpy()
+    path = tmp_path / "pe.smcsr"
+    nnz = ctx.pe_csr_file(str(path), threshold=threshold, rows_per_block=rows_per_block)
+    rows, cols, thr, mode, ptr, col, val = sysmat.read_csr_file(str(path))
+    assert (rows, cols, mode) == (ctx.n_det, ctx.n_vox, sysmat.MODE_REFERENCE)
+    assert thr == np.float32(threshold) and nnz == len(val) == ptr[-1] == int((a > threshold).sum())
+    back = np.zeros_like(a)
+    for r in range(rows):
+        back[r, col[ptr[r]:ptr[r + 1]]] = val[ptr[r]:ptr[r + 1]]
+    assert np.array_equal(back, np.where(a > threshold, a, 0.0))
+
+
+def test_pe_csr_file_errors(gpu, tmp_path):
+    geo, _ = golden("mini0")
+    ctx = sysmat.Context(geo)
+    with pytest.raises(sysmat.SysmatError):
+        ctx.pe_csr_file(str(tmp_path / "no_such_dir" / "x.smcsr"))
+    with pytest.raises(sysmat.SysmatError):
+        ctx.pe_csr_file(str(tmp_path / "x.smcsr"), threshold=-1.0)

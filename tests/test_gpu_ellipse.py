@@ -1,0 +1,98 @@
+"""GPU tests of elliptical holes (sysmat_set_hole_shapes), through the C ABI.
+
+The device chord is pinned to the reference function's own outputs (golden vectors made by
+its unmodified source on a B200, tests/golden/make_golden.py).  The reference's float chord
+is ill-conditioned: c = rz^2 x^2 + rx^2 z^2 - rx^2 rz^2 and b^2 - a c cancel, so its value
+depends on the compiler's contractions (it differs from FP64 by up to 7e-3 mm on the golden
+items).  Built by the same compiler from the same expressions, the device chord reproduces
+it; the gcc-built CPU oracle agrees with it only to that conditioning, which bounds the
+matrix-level comparison below."""
+import os
+
+import numpy as np
+import pytest
+
+from conftest import geometry, oracle, rel_err, sysmat
+
+pytestmark = pytest.mark.gpu
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+
+
+def test_device_chord_tracks_reference_function(gpu):
+    """Measured: 92.7 % of the golden items bit-identical, the rest within 3.5e-3 mm (99th
+    percentile 4e-4 mm) where the cancelling expressions take another contraction; the
+    reference's own float chord is 6.7e-3 mm from FP64 on the same items."""
+    z = np.load(os.path.join(HERE, "golden", "ellipse_chords.npz"))
+    args = gpu.from_numpy(z["args"]).cuda()
+    got = sysmat.ell_chords(args).cpu().numpy().astype(np.float64)
+    ref = z["ref"].astype(np.float64)
+    o64 = np.array([oracle.ell_chord(a, 64) for a in z["args"].astype(np.float64)])
+    assert np.mean(got == ref) > 0.9, np.mean(got == ref)
+    assert np.abs(got - ref).max() <= np.abs(o64 - ref).max()
+    assert np.percentile(np.abs(got - ref), 99) < 1e-3
+
+
+def _system_and_shapes(seed):
+    geo = geometry.mini(seed=seed, rotated=True, layers=2, n_rot=8, nvox=(6, 5, 3), ncry=(5, 4))
+    H = geo.n_holes
+    rng = np.random.default_rng(seed)
+    r = geo.collimator[100:100 + 9 * H].reshape(H, 9)[:, 4].astype(np.float64)
+    shapes = np.stack([r * rng.uniform(0.5, 1.0, H), r * rng.uniform(0.5, 1.0, H),
+                       rng.uniform(0.0, np.pi, H)], 1).astype(np.float32)
+    shapes[rng.random(H) < 0.2, 0] = 0.0                 # some holes stay circular
+    return geo, shapes
+
+
+def _pe(torch, ctx, rotation, mode=sysmat.MODE_REFERENCE):
+    out = torch.empty((ctx.n_det, ctx.n_vox), dtype=torch.float32, device="cuda")
+    ctx.pe(out, rotation=rotation, mode=mode)
+    torch.cuda.synchronize()
+    return out.cpu().numpy()
+
+
+@pytest.mark.parametrize("seed", [51, 52])
+def test_elliptical_holes_match_oracle(gpu, seed):
+    geo, shapes = _system_and_shapes(seed)
+    ctx = sysmat.Context(geo)
+    circ = _pe(gpu, ctx, 2.0)
+    ctx.set_hole_shapes(shapes)
+    a = _pe(gpu, ctx, 2.0)
+    ref = oracle.pe(geo.with_rotation(2), prec=32, shapes=shapes)
+    r = rel_err(a, ref)
+    # measured: median 2e-7, 6-10 % of elements above 1e-5, none above 2e-4 (the float
+    # elliptical chord's conditioning, see the module docstring)
+    assert np.median(r) < 1e-6
+    assert r.max() < 1e-3
+    assert not np.array_equal(a, circ)                   # the shapes change the matrix
+    ctx.set_hole_shapes(None)                            # back to circles
+    assert np.array_equal(_pe(gpu, ctx, 2.0), circ)
+
+
+def test_all_circular_shape_table_is_bit_identical(gpu):
+    geo, shapes = _system_and_shapes(53)
+    ctx = sysmat.Context(geo)
+    plain = _pe(gpu, ctx, 1.0)
+    shapes[:, 0] = 0.0
+    ctx.set_hole_shapes(shapes)
+    assert np.array_equal(_pe(gpu, ctx, 1.0), plain)
+
+
+def test_invalid_shapes_and_unsupported_paths_raise(gpu):
+    geo, shapes = _system_and_shapes(54)
+    ctx = sysmat.Context(geo)
+    bad = shapes.copy()
+    bad[0, :2] = [10.0, 0.5]                             # semi-axis beyond the radius field
+    with pytest.raises(sysmat.SysmatError):
+        ctx.set_hole_shapes(bad)
+    bad = shapes.copy()
+    bad[1, 2] = np.nan
+    with pytest.raises(sysmat.SysmatError):
+        ctx.set_hole_shapes(bad)
+    ctx.set_hole_shapes(shapes)
+    out = gpu.empty((ctx.n_det, ctx.n_vox), dtype=gpu.float32, device="cuda")
+    with pytest.raises(sysmat.SysmatError):
+        sysmat.BatchPlan([ctx], [(0, 0.0, 0, ctx.n_det, 0, ctx.n_vox, out)])
+    x = gpu.ones(ctx.n_vox, dtype=gpu.float32, device="cuda")
+    with pytest.raises(sysmat.SysmatError):
+        ctx.project(x)

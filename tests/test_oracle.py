@@ -217,3 +217,30 @@ def test_oracle_fp32_vs_fp64_error_is_small():
     r = rel_err(oracle.pe(geo, prec=32), oracle.pe(geo, prec=64))
     assert np.median(r) < 2e-6
     assert r.max() < 1e-3
+
+
+def test_ellipse_chord_against_reference_golden():
+    """The oracle's restatement of length_ellipticalcylinder_ray (PESysMatGen.cu:801-947)
+    against the reference function's own outputs (tests/golden/ellipse_chords.npz, made on a
+    B200 by tests/golden/make_golden.py).  The reference's float chord cancels in
+    c = rz^2 x^2 + rx^2 z^2 - rx^2 rz^2 and in b^2 - a c, so a gcc build reproduces it only to
+    that conditioning: most items exactly, the rest within the reference's own error
+    against FP64."""
+    import os
+    z = np.load(os.path.join(os.path.dirname(__file__), "golden", "ellipse_chords.npz"))
+    args, ref = z["args"].astype(np.float64), z["ref"].astype(np.float64)
+    o32 = np.array([oracle.ell_chord(a, 32) for a in args])
+    o64 = np.array([oracle.ell_chord(a, 64) for a in args])
+    assert np.mean(o32 == ref) > 0.75
+    assert np.percentile(np.abs(o32 - ref), 95) < 1e-3
+    # the oracle's float error is of the size of the reference's own error against FP64
+    assert np.abs(o32 - ref).max() <= 2 * np.abs(o64 - ref).max() + 1e-3
+    # circles: the elliptical chord equals the circular chord away from the two functions'
+    # different tangency cut-offs (the elliptical discriminant carries a factor r^4)
+    rng = np.random.default_rng(3)
+    diff = []
+    for a in args[:500]:
+        r = float(rng.uniform(0.3, 1.5))
+        c = oracle.lib().oracle_cyl_chord(64, np.ascontiguousarray(np.r_[a[:10], r]).ctypes.data_as(oracle._dp))
+        diff.append(abs(c - oracle.ell_chord(np.r_[a[:10], r, r, a[12]], 64)))
+    assert np.mean(np.array(diff) < 1e-9) > 0.99
