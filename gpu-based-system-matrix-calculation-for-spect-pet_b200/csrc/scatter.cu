@@ -34,12 +34,13 @@ namespace sysmat {
 namespace {
 
 constexpr int kItemThreads = 128;
-constexpr int kPairChunk = 128;
+constexpr int kPairChunk = 512;
 
 // ---- reference helper formulas (scatter.cu:961-1038) ----
 
-__device__ __forceinline__ float cone_angle(float xs, float ys, float zs, float xa, float ya, float za,
-                                            float xd, float yd, float zd)
+// Clamped cosine of the scattering angle at a between the directions s -> a and a -> d.
+__device__ __forceinline__ float cone_cosine(float xs, float ys, float zs, float xa, float ya, float za,
+                                             float xd, float yd, float zd)
 {
     const float a0 = xa - xs, a1 = ya - ys, a2 = za - zs;
     const float b0 = xd - xa, b1 = yd - ya, b2 = zd - za;
@@ -49,7 +50,13 @@ __device__ __forceinline__ float cone_angle(float xs, float ys, float zs, float 
     float c = dot / (ma * mb);
     if (c > 1.0f) c = 1.0f;
     if (c < -1.0f) c = -1.0f;
-    return acosf(c);
+    return c;
+}
+
+__device__ __forceinline__ float cone_angle(float xs, float ys, float zs, float xa, float ya, float za,
+                                            float xd, float yd, float zd)
+{
+    return acosf(cone_cosine(xs, ys, zs, xa, ya, za, xd, yd, zd));
 }
 
 __device__ __forceinline__ float dist3(float x1, float y1, float z1, float x2, float y2, float z2)
@@ -414,22 +421,19 @@ __device__ float scatter_item(const ElemConst& e, const PairRec& pr, const AttEn
     const float yt = pr.yss + 1000.0f * (pr.yss - e.yIs) / dis;
     const float zt = pr.zss + 1000.0f * (pr.zss - e.zIs) / dis;
     const float lthr = box_chord(e.xIs, e.yIs, e.zIs, xt, yt, zt, e.ux1, e.uy1, e.uz1, e.ux2, e.uy2, e.uz2);
-    float tmin = 0.0f, tmax = 0.0f;
+    // The reference takes the extremes of the 8 corner angles acos(c_k); acos decreases, so
+    // they are acos(max c_k) and acos(min c_k): two arc cosines instead of eight (the same
+    // floats wherever acosf is monotone, which holds to within an ulp at ties).
+    float cmin = 2.0f, cmax = -2.0f;
 #pragma unroll
     for (int c = 0; c < 8; ++c) {
-        // corner order of the reference: (x1,y1,z1),(x2,y1,z1),(x1,y2,z1),(x1,y1,z2),
-        // (x2,y2,z1),(x2,y1,z2),(x1,y2,z2),(x2,y2,z2)
-        const int cx = (c == 1 || c == 4 || c == 5 || c == 7);
-        const int cy = (c == 2 || c == 4 || c == 6 || c == 7);
-        const int cz = (c == 3 || c == 5 || c == 6 || c == 7);
-        const float th = cone_angle(e.xIs, e.yIs, e.zIs, pr.xss, pr.yss, pr.zss, cx ? e.ux2 : e.ux1,
-                                    cy ? e.uy2 : e.uy1, cz ? e.uz2 : e.uz1);
-        if (c == 0) { tmin = th; tmax = th; }
-        else {
-            if (th > tmax) tmax = th;
-            if (th < tmin) tmin = th;
-        }
+        const int cx = c & 1, cy = (c >> 1) & 1, cz = c >> 2;
+        const float ck = cone_cosine(e.xIs, e.yIs, e.zIs, pr.xss, pr.yss, pr.zss, cx ? e.ux2 : e.ux1,
+                                     cy ? e.uy2 : e.uy1, cz ? e.uz2 : e.uz1);
+        cmin = fminf(cmin, ck);
+        cmax = fmaxf(cmax, ck);
     }
+    float tmin = acosf(cmax), tmax = acosf(cmin);
     if (lthr > 0.001f) tmin = 0.0f;
     const int n = (int)((tmax - tmin) / 0.01f);
     const float ratio = (float)kn_sum_tab(tmin, n, kn_tab) / integ;
@@ -506,12 +510,12 @@ scatter_kernel(DevGeom g, ScatterPhysics ph, ScatterLaunch L)
             const PairRec& pr = sp[k];
             if (!pr.valid) continue;
             float xs, ys, zs, w_s;
-            if (s < g.n_det) {
+            const bool crystal = s < g.n_det;
+            if (crystal) {
                 w_s = __ldg(&L.pe[(long long)s * g.nvox + v]) * e.mu_c / e.mu_pe;   // :1218-1219
                 if (w_s == 0.0f) continue;          // the item is exactly 0
                 const float4 ps = __ldg(&g.cry.pos[s]);
                 xs = ps.x; ys = ps.y; zs = ps.z;
-                acc_c += (double)scatter_item(e, pr, L.att, xs, ys, zs, w_s, ph.e0, ph.integ, L.kn_tab);
             } else {
                 const float4 hr = __ldg(&g.hole.raw[s - g.n_det]);
                 xs = hr.x;
@@ -529,8 +533,11 @@ scatter_kernel(DevGeom g, ScatterPhysics ph, ScatterLaunch L)
                     sa = (vr * vr + (hr.z - hr.y) * vr) / (4.0f * lih * lih);
                 }
                 w_s = sa / ph.col_mu_tot0 * ph.col_mu_c0;                // :1716
-                acc_h += (double)scatter_item(e, pr, L.att, xs, ys, zs, w_s, ph.e0, ph.integ, L.kn_tab);
             }
+            // one call site keeps a single copy of the item code
+            const double c = (double)scatter_item(e, pr, L.att, xs, ys, zs, w_s, ph.e0, ph.integ, L.kn_tab);
+            if (crystal) acc_c += c;
+            else acc_h += c;
         }
     }
     if (!active) return;
