@@ -328,14 +328,14 @@ def run_scatter(args, sysmat, torch):
                         "2304 voxels, 1024 layer-0 holes"}
 
 
-def run_batch(args, sysmat, torch, n_instances=64, rows=8):
+def run_batch(args, sysmat, torch, n_instances=64, rows=8, sweep=True):
     """Design sweep of configuration 4: every instance x every one of its rotations, each task
     a block of `rows` crystals (centre of the 32x32 array) x one z-plane (1024 voxels).  The
     batched form (one autotuned persistent launch, replayed as a CUDA graph) against the plain
     form (one sysmat_pe call per instance and rotation), same outputs."""
     geos = geometry.config4(n_instances=n_instances)
     ctxs = [sysmat.Context(gg) for gg in geos]
-    d0, v0, nv = 16 * 32 + 12, 1024 * 8, 1024
+    d0, v0, nv = 16 * 32 + 16 - rows // 2, 1024 * 8, 1024
     tasks = [(k, float(r), d0, rows, v0, nv) for k, gg in enumerate(geos) for r in range(gg.n_rot)]
     out = torch.empty((len(tasks), rows, nv), dtype=torch.float32, device="cuda")
     plan = sysmat.BatchPlan(ctxs, [t + (out[i],) for i, t in enumerate(tasks)])
@@ -368,11 +368,20 @@ def run_batch(args, sysmat, torch, n_instances=64, rows=8):
     same = bool(torch.equal(out, ref))
     plan.close()
     nel = len(tasks) * rows * nv
+    by_rows = None
+    if sweep:
+        # the batched form's gain against per-task calls as the tasks grow (16 designs)
+        by_rows = {}
+        for r in (2, 32):
+            sub = run_batch(args, sysmat, torch, n_instances=16, rows=r, sweep=False)
+            by_rows[str(r)] = {"speedup_vs_plain": sub["speedup_vs_plain"], "tasks": sub["tasks"],
+                               "elements_per_step": sub["elements_per_step"]}
     return {"value": nel / (batch_ms * 1e-3), "unit": UNIT, "ms_per_step": batch_ms,
             "plain_value": nel / (plain_ms * 1e-3), "plain_ms_per_step": plain_ms,
             "speedup_vs_plain": plain_ms / batch_ms, "outputs_identical": same,
             "tiles": list(tiles), "tasks": len(tasks), "elements_per_step": nel,
             "gpu_launches_per_step": {"batched": 1, "plain": len(tasks)},
+            "speedup_by_rows_per_task": by_rows,
             "workload": f"config4 design sweep: {n_instances} seeded collimators x their 12-60 rotations "
                         f"({len(tasks)} tasks), each crystals {d0}..{d0 + rows - 1} x z-plane 8 "
                         f"(1024 voxels)"}
