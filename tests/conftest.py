@@ -51,7 +51,7 @@ def rel_err(a, b, scale=None):
     return np.abs(a - b) / np.maximum(np.abs(b), tau)
 
 
-# Per-element tolerance of the system matrix against the reference (north star: 1e-5).
+# Per-element tolerance of the system matrix against the reference (1e-5).
 TOL = 1e-5
 
 

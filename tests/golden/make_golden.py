@@ -5,7 +5,7 @@ unmodified CUDA sources compiled for sm_100a (oracle/Makefile, target `ref`) and
 through the reference host entry points (PESysMatGen, the three `scatter` programs).
 Run on a machine with a GPU:
 
-    python tests/golden/make_golden.py --out gpurun_out/golden
+    python tests/golden/make_golden.py --out golden_out
 
 and copy the resulting .npz files into tests/golden/.  Each fixture stores the four
 parameter arrays it was made from, so it does not depend on the generator staying
@@ -133,7 +133,7 @@ def ellipse_case(outdir):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--out", default="gpurun_out/golden")
+    ap.add_argument("--out", default="golden_out")
     ap.add_argument("--only", default="")
     args = ap.parse_args()
     if not ref_lib.available():
