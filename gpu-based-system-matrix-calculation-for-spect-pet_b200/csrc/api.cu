@@ -88,6 +88,8 @@ int decode(const float* pC, const float* pD, const float* pI, DevGeom& g, int& n
             Ly.z2 = L[3] / 2.0f;
             Ly.thickness = L[2];
             Ly.mu_total = L[5];
+            Ly.mu_pe = L[6];
+            Ly.mu_c = L[7];
             if (!(L[5] >= 0.0f)) g.nonneg_mu = 0;
             Ly.hole_begin = h;
             Ly.hole_count = nh;
@@ -352,6 +354,24 @@ extern "C" SYSMAT_API int sysmat_scatter_prepare(sysmat_ctx* ctx, int parts, con
     if (rc == -2) return SYSMAT_ERR_NOMEM;
     if (rc) return SYSMAT_ERR_CUDA;
     ctx->prepared_parts = parts;
+    ctx->prepared_native = 0;
+    return SYSMAT_OK;
+}
+
+extern "C" SYSMAT_API int sysmat_scatter_prepare_native(sysmat_ctx* ctx, int parts, const uint32_t* d_bm_crystal,
+                                                        void* stream)
+{
+    if (!ctx || !same_device(ctx)) return SYSMAT_ERR_ARG;
+    if (parts < 1 || parts > 3) return SYSMAT_ERR_ARG;
+    if ((parts & SYSMAT_SCATTER_CRYSTAL) && !d_bm_crystal) return SYSMAT_ERR_ARG;
+    if ((parts & SYSMAT_SCATTER_COLLIMATOR) && (ctx->g.n_holes < 1 || ctx->g.n_layers < 1)) return SYSMAT_ERR_ARG;
+    ctx->prepared_parts = 0;
+    const int rc = build_scatter_pairs_native(ctx->g, parts, d_bm_crystal, ctx->scratch, &ctx->pairs, &ctx->att,
+                                              (cudaStream_t)stream);
+    if (rc == -2) return SYSMAT_ERR_NOMEM;
+    if (rc) return SYSMAT_ERR_CUDA;
+    ctx->prepared_parts = parts;
+    ctx->prepared_native = 1;
     return SYSMAT_OK;
 }
 
@@ -363,8 +383,11 @@ extern "C" SYSMAT_API int sysmat_scatter(sysmat_ctx* ctx, int parts, int hole_mo
     int rc = check_block(ctx, det_begin, det_count, vox_begin, vox_count, d_out, ld);
     if (rc) return rc;
     if (parts < 1 || parts > 3 || (parts & ~ctx->prepared_parts)) return SYSMAT_ERR_ARG;
-    if (hole_model != SYSMAT_HOLE_MODEL_COMBINED && hole_model != SYSMAT_HOLE_MODEL_VARIANT)
+    if (hole_model != SYSMAT_HOLE_MODEL_COMBINED && hole_model != SYSMAT_HOLE_MODEL_VARIANT &&
+        hole_model != SYSMAT_HOLE_MODEL_NATIVE)
         return SYSMAT_ERR_ARG;
+    // the pair tables' layout follows the model they were prepared for
+    if ((hole_model == SYSMAT_HOLE_MODEL_NATIVE) != (ctx->prepared_native != 0)) return SYSMAT_ERR_ARG;
     if ((parts & SYSMAT_SCATTER_CRYSTAL) && !d_pe) return SYSMAT_ERR_ARG;
     if (ctx->h_phys.size() != (size_t)kNPhysics) return SYSMAT_ERR_ARG;
     const float* P = ctx->h_phys.data();

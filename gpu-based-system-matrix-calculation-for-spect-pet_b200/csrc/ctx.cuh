@@ -28,6 +28,7 @@ struct sysmat_ctx {
     // scatter pair tables (sysmat_scatter_prepare)
     sysmat::ScatterScratch scratch{};
     int prepared_parts = 0;
+    int prepared_native = 0;        // the pair tables are the native model's
     sysmat::PairRec* pairs = nullptr;
     sysmat::AttEntry* att = nullptr;
     double* d_kn_tab = nullptr;     // Klein-Nishina table for kn_e0

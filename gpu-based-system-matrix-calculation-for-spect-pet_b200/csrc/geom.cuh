@@ -44,6 +44,7 @@ struct LayerInfo {
     float x1, x2, y1, y2, z1, z2;   // plate box (PESysMatGen.cu:1242-1249)
     float thickness;
     float mu_total;
+    float mu_pe, mu_c;               // photoelectric and Compton parts (native scatter model)
     int hole_begin, hole_count;
 };
 

@@ -243,6 +243,25 @@ __global__ void bitmap_crystal_kernel(const float* __restrict__ det, int n, long
     out[w] = word;
 }
 
+// Whether crystal k may attenuate the path from hole i (raw parameters hr) to crystal j:
+// k's bounding sphere within the angular cone of the hole-to-j segment, seen from the hole
+// (scatter.cu:1963-2006; raw y, no FOV offset).
+__device__ __forceinline__ bool collimator_related(const float* __restrict__ det, float4 hr, int j, int k)
+{
+    const float xi = hr.x, yi = (hr.y + hr.z) / 2.0f, zi = hr.w;
+    const float* pj = det + 12 * j;
+    const float* pk = det + 12 * k;
+    const float rj = sqrtf(pj[4] * pj[4] + pj[6] * pj[6] + pj[5] * pj[5]) / 2.0f;
+    const float lij = dist3(xi, yi, zi, pj[1], pj[2], pj[3]);
+    const float cji = rj / lij;
+    const float rk = sqrtf(pk[4] * pk[4] + pk[6] * pk[6] + pk[5] * pk[5]) / 2.0f;
+    const float lik = dist3(pk[1], pk[2], pk[3], xi, yi, zi);
+    const float cki = rk / lik;
+    const float dd = dist3((pk[1] - xi) / lik, (pk[2] - yi) / lik, (pk[3] - zi) / lik,
+                           (pj[1] - xi) / lij, (pj[2] - yi) / lij, (pj[3] - zi) / lij);
+    return dd <= cki + cji;
+}
+
 __global__ void bitmap_collimator_kernel(const float* __restrict__ det, const float4* __restrict__ hraw,
                                          int n, int nh, long long words, uint32_t* __restrict__ out)
 {
@@ -256,20 +275,7 @@ __global__ void bitmap_collimator_kernel(const float* __restrict__ det, const fl
         const long long ij = bit / n;
         const int j = (int)(ij % n);
         const int i = (int)(ij / n);
-        // scatter.cu:1963-2006 (raw y, no FOV offset)
-        const float4 hr = __ldg(&hraw[i]);
-        const float xi = hr.x, yi = (hr.y + hr.z) / 2.0f, zi = hr.w;
-        const float* pj = det + 12 * j;
-        const float* pk = det + 12 * k;
-        const float rj = sqrtf(pj[4] * pj[4] + pj[6] * pj[6] + pj[5] * pj[5]) / 2.0f;
-        const float lij = dist3(xi, yi, zi, pj[1], pj[2], pj[3]);
-        const float cji = rj / lij;
-        const float rk = sqrtf(pk[4] * pk[4] + pk[6] * pk[6] + pk[5] * pk[5]) / 2.0f;
-        const float lik = dist3(pk[1], pk[2], pk[3], xi, yi, zi);
-        const float cki = rk / lik;
-        const float dd = dist3((pk[1] - xi) / lik, (pk[2] - yi) / lik, (pk[3] - zi) / lik,
-                               (pj[1] - xi) / lij, (pj[2] - yi) / lij, (pj[3] - zi) / lij);
-        if (dd <= cki + cji) word |= 1u << b;
+        if (collimator_related(det, __ldg(&hraw[i]), j, k)) word |= 1u << b;
     }
     out[w] = word;
 }
@@ -297,7 +303,9 @@ __device__ __forceinline__ void scatter_point(const DevGeom& g, int s, float& xs
 }
 
 // Visit the attenuators of pair (s, d) with non-zero chords, in ascending crystal order.
-template <typename F>
+// NATIVE: hole scatterers s >= D are holes of any layer, their attenuators given by the
+// relationship predicate evaluated here instead of the layer-0 bitmap.
+template <bool NATIVE, typename F>
 __device__ void for_each_attenuator(const DevGeom& g, const uint32_t* bm_cry, const uint32_t* bm_col,
                                     int s, int d, float xs, float ys, float zs, const DetPoint& q, F&& f)
 {
@@ -310,9 +318,14 @@ __device__ void for_each_attenuator(const DevGeom& g, const uint32_t* bm_cry, co
         base = ((long long)(s - n) * n + d) * n;
     }
     const uint32_t* bm = s < n ? bm_cry : bm_col;
+    const float4 hr = (NATIVE && s >= n) ? __ldg(&g.hole.raw[s - n]) : make_float4(0.f, 0.f, 0.f, 0.f);
     for (int a = 0; a < n; ++a) {
         if (a == d || (s < n && a == s)) continue;
-        if (!test_bit(bm, base + a)) continue;
+        if (NATIVE && s >= n) {
+            if (!collimator_related(g.raw_det, hr, d, a)) continue;
+        } else if (!test_bit(bm, base + a)) {
+            continue;
+        }
         const float4 pa = __ldg(&g.cry.pos[a]);
         const float4 sa = __ldg(&g.cry.size[a]);
         const float4 ta = __ldg(&g.cry.trig[a]);
@@ -331,10 +344,72 @@ __device__ __forceinline__ bool pair_enabled(const DevGeom& g, int parts, int s,
     return (parts & 2) != 0;
 }
 
+// Layer of hole h (global numbering, layer by layer).
+__device__ __forceinline__ int hole_layer(const DevGeom& g, int h)
+{
+    int m = 0;
+    while (m + 1 < g.n_layers && h >= g.layer[m + 1].hole_begin) ++m;
+    return m;
+}
+
+// Distance from the centre (x, ym, z) of hole h along the unit direction k to where the
+// path leaves the hole (side wall or cap), capped at len.
+__device__ __forceinline__ float hole_exit(float4 a, float r, float ym, float kx, float ky, float kz, float len)
+{
+    const float kk = kx * kx + kz * kz;
+    float t = len;
+    if (kk > 0.0f) t = fminf(t, r / sqrtf(kk));
+    if (ky > 0.0f) t = fminf(t, (a.z - ym) / ky);
+    else if (ky < 0.0f) t = fminf(t, (a.y - ym) / ky);
+    return t;
+}
+
+// Native model: tungsten crossed by the scattered photon from the centre S of hole h to the
+// detector point D, as sum_m mu_pe,m L_m and sum_m mu_C,m L_m, L_m = plate chord of layer m
+// minus the hole chords of layer m (the reference chords; the scatter hole's own part is its
+// exit distance from S, and in its own layer the plate chord runs from the plate entry seen
+// from D to S).
+__device__ void tungsten_path(const DevGeom& g, int h, float sx, float sy, float sz, float dx, float dy, float dz,
+                              float& w_pe, float& w_c)
+{
+    w_pe = 0.0f;
+    w_c = 0.0f;
+    const int mh = hole_layer(g, h);
+    const float ex = dx - sx, ey = dy - sy, ez = dz - sz;
+    const float len = sqrtf(ex * ex + ey * ey + ez * ez);
+    const float kx = ex / len, ky = ey / len, kz = ez / len;
+    const float n2 = ex * ex + ez * ez;
+    for (int m = 0; m < g.n_layers; ++m) {
+        const LayerInfo& Ly = g.layer[m];
+        const float box = (m == mh) ? box_chord_inside(dx, dy, dz, sx, sy, sz, Ly.x1, Ly.y1, Ly.z1, Ly.x2, Ly.y2, Ly.z2)
+                                    : box_chord(sx, sy, sz, dx, dy, dz, Ly.x1, Ly.y1, Ly.z1, Ly.x2, Ly.y2, Ly.z2);
+        if (box == 0.0f) continue;
+        float holes = 0.0f;
+        for (int j = Ly.hole_begin; j < Ly.hole_begin + Ly.hole_count; ++j) {
+            const float4 a = __ldg(&g.hole.a[j]);
+            const float r = __ldg(&g.hole.b[j].x);
+            if (j == h) {
+                holes = holes + hole_exit(a, r, sy, kx, ky, kz, len);
+                continue;
+            }
+            // the line keeps further than r from the axis: the chord is 0 (exact-safe reject)
+            const float cr = ex * (a.w - sz) - ez * (a.x - sx);
+            if (cr * cr > r * r * n2 * 1.001f + 1e-12f) continue;
+            holes = holes + cyl_chord(sx, sy, sz, dx, dy, dz, a.x, a.y, a.z, a.w, r);
+        }
+        const float L = box - holes;
+        if (L > 0.0f) {
+            w_pe = w_pe + Ly.mu_pe * L;
+            w_c = w_c + Ly.mu_c * L;
+        }
+    }
+}
+
+template <bool NATIVE>
 __global__ void pair_count_kernel(DevGeom g, int parts, const uint32_t* bm_cry, const uint32_t* bm_col,
                                   int* counts)
 {
-    const int ns = g.n_det + g.n_holes0;
+    const int ns = g.n_det + (NATIVE ? g.n_holes : g.n_holes0);
     const long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (p >= (long long)g.n_det * ns) return;
     const int d = (int)(p / ns), s = (int)(p - (long long)d * ns);
@@ -343,15 +418,16 @@ __global__ void pair_count_kernel(DevGeom g, int parts, const uint32_t* bm_cry, 
         float xs, ys, zs;
         scatter_point(g, s, xs, ys, zs);
         const DetPoint q = det_point(__ldg(&g.cry.pos[d]), __ldg(&g.cry.size[d]), __ldg(&g.cry.trig[d]));
-        for_each_attenuator(g, bm_cry, bm_col, s, d, xs, ys, zs, q, [&](int, float) { ++c; });
+        for_each_attenuator<NATIVE>(g, bm_cry, bm_col, s, d, xs, ys, zs, q, [&](int, float) { ++c; });
     }
     counts[p] = c;
 }
 
+template <bool NATIVE>
 __global__ void pair_fill_kernel(DevGeom g, int parts, const uint32_t* bm_cry, const uint32_t* bm_col,
                                  const int* offsets, PairRec* pairs, AttEntry* att)
 {
-    const int ns = g.n_det + g.n_holes0;
+    const int ns = g.n_det + (NATIVE ? g.n_holes : g.n_holes0);
     const long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (p >= (long long)g.n_det * ns) return;
     const int d = (int)(p / ns), s = (int)(p - (long long)d * ns);
@@ -374,12 +450,19 @@ __global__ void pair_fill_kernel(DevGeom g, int parts, const uint32_t* bm_cry, c
         r.labs = box_chord(r.xss, r.yss, r.zss, xt, yt, zt, ux1, uy1, uz1, ux2, uy2, uz2);
         r.att_begin = offsets[p];
         int k = 0;
-        for_each_attenuator(g, bm_cry, bm_col, s, d, xs, ys, zs, q, [&](int a, float len) {
+        for_each_attenuator<NATIVE>(g, bm_cry, bm_col, s, d, xs, ys, zs, q, [&](int a, float len) {
             const float4 mu = __ldg(&g.cry.mu[a]);
             att[r.att_begin + k] = AttEntry{len, mu.y, mu.z};
             ++k;
         });
         r.att_count = k;
+        if (NATIVE && s >= g.n_det) {
+            const int h = s - g.n_det;
+            tungsten_path(g, h, xs, ys, zs, q.xD, q.yD, q.zD, r.w_pe, r.w_c);
+            const LayerInfo& Ly = g.layer[hole_layer(g, h)];
+            r.mu_tot_h = Ly.mu_total;
+            r.mu_c_h = Ly.mu_c;
+        }
     }
     pairs[p] = r;
 }
@@ -453,6 +536,11 @@ __device__ float scatter_item(const ElemConst& e, const PairRec& pr, const AttEn
         }
         a_sum = a_sum + ae.len * mt;
     }
+    if (pr.w_pe != 0.0f || pr.w_c != 0.0f) {             // native model: tungsten at E'
+        const float mpe_w = pr.w_pe * e0 * e0 * e0 / es / es / es;
+        const float mc_w = pr.w_c * e0 / es;
+        a_sum = a_sum + (mpe_w + mc_w);
+    }
     const float mpe_s = e.mu_pe * e0 * e0 * e0 / es / es / es;              // :1411-1417
     const float mc_s = e.mu_c * e0 / es;
     const float mt_s = mpe_s + mc_s;
@@ -471,7 +559,7 @@ scatter_kernel(DevGeom g, ScatterPhysics ph, ScatterLaunch L)
     const long long vi = (long long)blockIdx.x * kItemThreads + threadIdx.x;
     const bool active = vi < L.vox_count;
     const long long v = L.vox_begin + (active ? vi : 0);
-    const int ns = g.n_det + g.n_holes0;
+    const int ns = g.n_det + (L.hole_model == 2 ? g.n_holes : g.n_holes0);
 
     const float4 P = __ldg(&g.cry.pos[d]), S = __ldg(&g.cry.size[d]);
     const float4 M = __ldg(&g.cry.mu[d]), T = __ldg(&g.cry.trig[d]);
@@ -523,7 +611,7 @@ scatter_kernel(DevGeom g, ScatterPhysics ph, ScatterLaunch L)
                 zs = hr.w;
                 const float lih = dist3(e.xI, e.yI, e.zI, xs, ys, zs);
                 float sa;
-                if (L.hole_model == 0) {                                  // :1711-1715
+                if (L.hole_model != 1) {                                  // :1711-1715
                     const float vr = 0.1f;
                     sa = (float)(((double)(vr * vr) * 3.14159265358979323846 + (double)((hr.z - hr.y) * vr)) /
                                  (4.0f * 3.14159265358979323846 * (double)lih * (double)lih) *
@@ -532,7 +620,8 @@ scatter_kernel(DevGeom g, ScatterPhysics ph, ScatterLaunch L)
                     const float vr = 0.2f;
                     sa = (vr * vr + (hr.z - hr.y) * vr) / (4.0f * lih * lih);
                 }
-                w_s = sa / ph.col_mu_tot0 * ph.col_mu_c0;                // :1716
+                if (L.hole_model == 2) w_s = sa / pr.mu_tot_h * pr.mu_c_h;     // the hole's own layer
+                else w_s = sa / ph.col_mu_tot0 * ph.col_mu_c0;            // :1716
             }
             // one call site keeps a single copy of the item code
             const double c = (double)scatter_item(e, pr, L.att, xs, ys, zs, w_s, ph.e0, ph.integ, L.kn_tab);
@@ -580,10 +669,11 @@ int launch_bitmap_collimator(const DevGeom& g, uint32_t* words, cudaStream_t s)
     return cudaGetLastError() == cudaSuccess ? 0 : -1;
 }
 
-int build_scatter_pairs(const DevGeom& g, int parts, const uint32_t* bm_cry, const uint32_t* bm_col,
-                        ScatterScratch& scratch, PairRec** pairs, AttEntry** att, cudaStream_t s)
+template <bool NATIVE>
+static int build_pairs(const DevGeom& g, int parts, const uint32_t* bm_cry, const uint32_t* bm_col,
+                       ScatterScratch& scratch, PairRec** pairs, AttEntry** att, cudaStream_t s)
 {
-    const int ns = g.n_det + g.n_holes0;
+    const int ns = g.n_det + (NATIVE ? g.n_holes : g.n_holes0);
     const long long np = (long long)g.n_det * ns;
     // layout: [counts/offsets (np+1 ints)][cub temp][pairs][att]
     size_t temp_bytes = 0;
@@ -603,7 +693,7 @@ int build_scatter_pairs(const DevGeom& g, int parts, const uint32_t* bm_cry, con
     int* counts = (int*)(base + off_counts);
     int* offsets = (int*)(base + off_offsets);
     const unsigned blocks = (unsigned)((np + 255) / 256);
-    pair_count_kernel<<<blocks, 256, 0, s>>>(g, parts, bm_cry, bm_col, counts);
+    pair_count_kernel<NATIVE><<<blocks, 256, 0, s>>>(g, parts, bm_cry, bm_col, counts);
     if (cudaMemsetAsync(counts + np, 0, sizeof(int), s) != cudaSuccess) return -1;
     cub::DeviceScan::ExclusiveSum(base + off_temp, temp_bytes, counts, offsets, (int)(np + 1), s);
     int total = 0;
@@ -618,14 +708,26 @@ int build_scatter_pairs(const DevGeom& g, int parts, const uint32_t* bm_cry, con
         base = (char*)scratch.base;
         counts = (int*)(base + off_counts);
         offsets = (int*)(base + off_offsets);
-        pair_count_kernel<<<blocks, 256, 0, s>>>(g, parts, bm_cry, bm_col, counts);
+        pair_count_kernel<NATIVE><<<blocks, 256, 0, s>>>(g, parts, bm_cry, bm_col, counts);
         if (cudaMemsetAsync(counts + np, 0, sizeof(int), s) != cudaSuccess) return -1;
         cub::DeviceScan::ExclusiveSum(base + off_temp, temp_bytes, counts, offsets, (int)(np + 1), s);
     }
     *pairs = (PairRec*)(base + off_pairs);
     *att = (AttEntry*)(base + fixed);
-    pair_fill_kernel<<<blocks, 256, 0, s>>>(g, parts, bm_cry, bm_col, offsets, *pairs, *att);
+    pair_fill_kernel<NATIVE><<<blocks, 256, 0, s>>>(g, parts, bm_cry, bm_col, offsets, *pairs, *att);
     return cudaGetLastError() == cudaSuccess ? 0 : -1;
+}
+
+int build_scatter_pairs(const DevGeom& g, int parts, const uint32_t* bm_cry, const uint32_t* bm_col,
+                        ScatterScratch& scratch, PairRec** pairs, AttEntry** att, cudaStream_t s)
+{
+    return build_pairs<false>(g, parts, bm_cry, bm_col, scratch, pairs, att, s);
+}
+
+int build_scatter_pairs_native(const DevGeom& g, int parts, const uint32_t* bm_cry, ScatterScratch& scratch,
+                               PairRec** pairs, AttEntry** att, cudaStream_t s)
+{
+    return build_pairs<true>(g, parts, bm_cry, nullptr, scratch, pairs, att, s);
 }
 
 int launch_scatter(const DevGeom& g, const ScatterPhysics& ph, const ScatterLaunch& L, cudaStream_t s)

@@ -24,7 +24,8 @@ inline void scatter_scratch_free(ScatterScratch& s)
 }
 
 // Pair record of scatterer s (crystal k = s, or hole h = s - D) and detector crystal d,
-// stored at index d * (D + H0) + s.
+// stored at index d * (D + H0) + s (reference hole models: layer-0 holes) or d * (D + H) + s
+// (native model: the holes of every layer).
 struct PairRec {
     float xss, yss, zss;   // scatter point in crystal d's frame
     float lsd;             // |scatter point - crystal d centre| (world)
@@ -32,6 +33,10 @@ struct PairRec {
     int att_begin;         // first entry in the attenuator list
     int att_count;         // number of attenuators with a non-zero chord
     int valid;             // 0 for the excluded pair s == d
+    // native model only (0 otherwise): tungsten on the way from a hole scatter point to d,
+    // sum_m mu_pe,m L_m and sum_m mu_C,m L_m at the photopeak, and the scatter hole's layer
+    // mu_total and mu_C (its interaction weight)
+    float w_pe, w_c, mu_tot_h, mu_c_h;
 };
 
 // Attenuator entry: chord length and the attenuator's photoelectric and Compton
@@ -52,7 +57,7 @@ struct ScatterPhysics {
 
 struct ScatterLaunch {
     int parts;             // bit 0 crystal, bit 1 collimator
-    int hole_model;        // 0 combined program, 1 collimator-only program
+    int hole_model;        // 0 combined program, 1 collimator-only program, 2 native
     int det_begin, det_count;
     long long vox_begin, vox_count, ld;
     float rotation;
@@ -80,6 +85,12 @@ int launch_bitmap_collimator(const DevGeom& g, uint32_t* words, cudaStream_t s);
 int build_scatter_pairs(const DevGeom& g, int parts, const uint32_t* bm_crystal,
                         const uint32_t* bm_collimator, ScatterScratch& scratch, PairRec** pairs,
                         AttEntry** att, cudaStream_t s);
+
+// Native model: scatter points at the holes of every layer, each with its layer's mu; the
+// collimator-scatter attenuators from the relationship predicate evaluated directly (no
+// bitmap); tungsten attenuation of the scattered photon on its way to the crystal.
+int build_scatter_pairs_native(const DevGeom& g, int parts, const uint32_t* bm_crystal,
+                               ScatterScratch& scratch, PairRec** pairs, AttEntry** att, cudaStream_t s);
 
 int launch_scatter(const DevGeom& g, const ScatterPhysics& ph, const ScatterLaunch& L,
                    cudaStream_t s);

@@ -27,6 +27,7 @@ SCATTER_CRYSTAL = 1
 SCATTER_COLLIMATOR = 2
 HOLE_MODEL_COMBINED = 0
 HOLE_MODEL_VARIANT = 1
+HOLE_MODEL_NATIVE = 2
 
 # Every symbol declared in include/sysmat.h.
 EXPORTS = ("PESysMatGen", "scatter", "scatter_collimator", "scatter_crystal", "sysmat_create",
@@ -35,7 +36,7 @@ EXPORTS = ("PESysMatGen", "scatter", "scatter_collimator", "scatter_crystal", "s
            "sysmat_scatter_prepare", "sysmat_scatter", "sysmat_pe_noalloc", "sysmat_csr_count",
            "sysmat_csr_fill", "sysmat_pe_work", "sysmat_batch_create", "sysmat_batch_set_tiles",
            "sysmat_batch_get_tiles", "sysmat_batch_tune", "sysmat_batch_run", "sysmat_batch_destroy",
-           "sysmat_batch", "sysmat_set_hole_shapes", "sysmat_pe_csr_file", "sysmat_project", "sysmat_vjp", "sysmat_backproject",
+           "sysmat_batch", "sysmat_scatter_prepare_native", "sysmat_set_hole_shapes", "sysmat_pe_csr_file", "sysmat_project", "sysmat_vjp", "sysmat_backproject",
            "sysmat_measure_peaks", "sysmat_ell_chords",
            "sysmat_error_string", "sysmat_version")
 
@@ -109,6 +110,7 @@ def lib():
             "sysmat_batch_destroy": ([_vp], ctypes.c_int),
             "sysmat_batch": ([ctypes.POINTER(_vp), ctypes.c_int, ctypes.POINTER(BatchItem), ctypes.c_int,
                               ctypes.c_int, _vp], ctypes.c_int),
+            "sysmat_scatter_prepare_native": ([_vp, ctypes.c_int, _vp, _vp], ctypes.c_int),
             "sysmat_set_hole_shapes": ([_vp, _fp, _fp, _fp], ctypes.c_int),
             "sysmat_pe_csr_file": ([_vp, ctypes.c_float, ctypes.c_char_p, ctypes.c_float, ctypes.c_int, ctypes.c_int,
                                     ctypes.POINTER(ctypes.c_longlong), _vp], ctypes.c_int),
@@ -272,6 +274,14 @@ class Context:
                                             _ptr(bm_crystal) if bm_crystal is not None else nullp,
                                             _ptr(bm_collimator) if bm_collimator is not None else nullp,
                                             _stream(stream)), "sysmat_scatter_prepare")
+
+    def scatter_prepare_native(self, bm_crystal=None, parts=SCATTER_CRYSTAL | SCATTER_COLLIMATOR, stream=None):
+        """Pair tables of the native model (sysmat_scatter_prepare_native); then call scatter with
+        hole_model=HOLE_MODEL_NATIVE."""
+        nullp = ctypes.c_void_p(0)
+        _check(lib().sysmat_scatter_prepare_native(self.handle, parts,
+                                                   _ptr(bm_crystal) if bm_crystal is not None else nullp,
+                                                   _stream(stream)), "sysmat_scatter_prepare_native")
 
     def scatter(self, out, pe=None, parts=SCATTER_CRYSTAL | SCATTER_COLLIMATOR,
                 hole_model=HOLE_MODEL_COMBINED, rotation=0.0, det_begin=0, det_count=None,

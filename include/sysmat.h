@@ -51,6 +51,8 @@ extern "C" {
 #define SYSMAT_SCATTER_COLLIMATOR 2
 #define SYSMAT_HOLE_MODEL_COMBINED 0   /* ScatterGen_RayTracing_CircularHole/scatter.cu:1711-1716 */
 #define SYSMAT_HOLE_MODEL_VARIANT 1    /* ScatterGen_Collimator/scatter.cu:1212-1215 */
+/* Native collimator scatter (no reference counterpart; see sysmat_scatter_prepare_native). */
+#define SYSMAT_HOLE_MODEL_NATIVE 2
 
 /* ---------------------------------------------------------------------------------- */
 /* Reference-compatible entry points (host buffers in, host buffers out, synchronous). */
@@ -118,6 +120,17 @@ SYSMAT_API int sysmat_bitmap_collimator(sysmat_ctx* ctx, uint32_t* d_words, void
  * The tables stay valid until the next prepare or sysmat_destroy. */
 SYSMAT_API int sysmat_scatter_prepare(sysmat_ctx* ctx, int parts, const uint32_t* d_bm_crystal,
                                       const uint32_t* d_bm_collimator, void* stream);
+
+/* Pair tables of the native scatter model, which fixes three simplifications of the reference's
+ * collimator scatter (scatter.cu:1544-1936): the holes of every layer are scatter points (the
+ * reference uses layer 0 only, H0 = Params_Collimator[10]), each weighted with its own layer's
+ * mu_C / mu_total (the reference uses layer 0's, scatter.cu:1716), and the scattered photon is
+ * attenuated by the tungsten between the hole and the crystal (plate chords minus hole chords
+ * per layer, mu_pe and mu_C rescaled to the scattered energy as for crystals; the reference
+ * ignores it).  The crystal part is the reference's.  The collimator-scatter attenuators come
+ * from the reference's relationship predicate evaluated for every hole (no bitmap file).
+ * Use with hole_model SYSMAT_HOLE_MODEL_NATIVE; synchronises `stream` once. */
+SYSMAT_API int sysmat_scatter_prepare_native(sysmat_ctx* ctx, int parts, const uint32_t* d_bm_crystal, void* stream);
 
 /* Primary-Compton scatter block (parts must have been prepared).  d_pe: the D x V
  * photoelectric matrix (row stride V) the crystal part reads.  hole_model:

@@ -120,12 +120,14 @@ def bitmap_collimator(geo, threads=0):
     return out
 
 
-PART = {"crystal": 1, "collimator": 2, "collimator_variant": 3}
+PART = {"crystal": 1, "collimator": 2, "collimator_variant": 3, "collimator_native": 4}
 
 
 def scatter(geo, pe_matrix, part, bitmap, prec=64, dets=None, v0=0, nv=None, threads=0):
-    """Scatter elements for part 'crystal', 'collimator' (combined program) or
-    'collimator_variant' (collimator-only program); float64 (len(dets), nv)."""
+    """Scatter elements for part 'crystal', 'collimator' (combined program),
+    'collimator_variant' (collimator-only program) or 'collimator_native' (the library's
+    native model: holes of every layer, their layer's mu, tungsten attenuation of the
+    scattered photon; `bitmap` is not read); float64 (len(dets), nv)."""
     nv = geo.n_vox - v0 if nv is None else nv
     c, pc = _f32(geo.collimator)
     d, pd = _f32(geo.detector)
@@ -169,7 +171,7 @@ def scatter_trace(geo, pe_matrix, part, bitmap, d, v, prec=64):
     p, pp = _f32(geo.physics)
     m, pm = _f32(np.asarray(pe_matrix, dtype=np.float32).reshape(-1))
     b = np.ascontiguousarray(bitmap, dtype=np.uint32)
-    n = geo.n_det if part == "crystal" else geo.n_holes_layer0
+    n = geo.n_det if part == "crystal" else (geo.n_holes if part == "collimator_native" else geo.n_holes_layer0)
     tr = np.full((n, 9), np.nan)
     val = lib().oracle_scatter_trace(pc, pd, pi, pp, pm, b.ctypes.data_as(_u32p), PART[part], prec, d, v,
                                      tr.ctypes.data_as(_dp))

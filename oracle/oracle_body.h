@@ -486,6 +486,89 @@ static inline REAL FN(dist3)(REAL x1, REAL y1, REAL z1, REAL x2, REAL y2, REAL z
  * (scatter.cu:1728-1924).  `kind` 1 = crystal k is the scatterer (attenuators skip d and
  * k, crystal bitmap), 2 = hole k (attenuators skip d, collimator bitmap).  Returns the
  * contribution rounded as the reference's float atomicAdd does. */
+/* ---- native collimator-scatter model (an extension, no reference counterpart) ---- */
+
+static int FN(hole_layer)(const ogeo* g, int h, int* begin)
+{
+    int b = 0;
+    for (int m = 0; m < g->L; ++m) {
+        if (h < b + g->nh[m]) { if (begin) *begin = b; return m; }
+        b += g->nh[m];
+    }
+    if (begin) *begin = b;
+    return g->L - 1;
+}
+
+/* The reference's crystal-relationship predicate for hole i and crystals j, k
+ * (scatter.cu:1963-2006, raw coordinates), for any hole. */
+static int FN(collimator_related)(const ogeo* g, int i, int j, int k)
+{
+    const float* C = g->C;
+    const float* D = g->D;
+    float xi = C[100 + 9 * i], yi = (C[101 + 9 * i] + C[102 + 9 * i]) / 2.0f, zi = C[103 + 9 * i];
+    const float *pj = D + 12 * j, *pk = D + 12 * k;
+    float rj = sqrtf(pj[4] * pj[4] + pj[6] * pj[6] + pj[5] * pj[5]) / 2.0f;
+    float lij = sqrtf((xi - pj[1]) * (xi - pj[1]) + (yi - pj[2]) * (yi - pj[2]) + (zi - pj[3]) * (zi - pj[3]));
+    float cji = rj / lij;
+    float rk = sqrtf(pk[4] * pk[4] + pk[6] * pk[6] + pk[5] * pk[5]) / 2.0f;
+    float lik = sqrtf((pk[1] - xi) * (pk[1] - xi) + (pk[2] - yi) * (pk[2] - yi) + (pk[3] - zi) * (pk[3] - zi));
+    float cki = rk / lik;
+    float ax = (pk[1] - xi) / lik, ay = (pk[2] - yi) / lik, az = (pk[3] - zi) / lik;
+    float bx = (pj[1] - xi) / lij, by = (pj[2] - yi) / lij, bz = (pj[3] - zi) / lij;
+    float dd = sqrtf((ax - bx) * (ax - bx) + (ay - by) * (ay - by) + (az - bz) * (az - bz));
+    return dd <= cki + cji;
+}
+
+/* Tungsten from the centre S of hole h to the detector point: sum_m mu_pe,m L_m and
+ * sum_m mu_C,m L_m with L_m = plate chord of layer m minus its hole chords (the scatter hole's
+ * own part is its exit distance from S; in its own layer the plate chord runs from the plate
+ * entry seen from the detector point to S). */
+static void FN(tungsten_path)(const ogeo* g, int h, REAL sx, REAL sy, REAL sz, REAL dx, REAL dy, REAL dz,
+                              REAL* w_pe, REAL* w_c)
+{
+    const float* C = g->C;
+    const REAL fov = (REAL)g->I[11];
+    *w_pe = 0;
+    *w_c = 0;
+    int hb;
+    const int mh = FN(hole_layer)(g, h, &hb);
+    REAL ex = dx - sx, ey = dy - sy, ez = dz - sz;
+    REAL len = SQRT(ex * ex + ey * ey + ez * ez);
+    REAL kx = ex / len, ky = ey / len, kz = ez / len;
+    int begin = 0;
+    for (int m = 0; m < g->L; ++m) {
+        const float* Lh = C + (m + 1) * 10;
+        REAL x1 = -(REAL)Lh[1] / (REAL)2.0f, x2 = (REAL)Lh[1] / (REAL)2.0f;
+        REAL y1 = -(REAL)Lh[2] / (REAL)2.0f + fov + (REAL)Lh[4];
+        REAL y2 = (REAL)Lh[2] / (REAL)2.0f + fov + (REAL)Lh[4];
+        REAL z1 = -(REAL)Lh[3] / (REAL)2.0f, z2 = (REAL)Lh[3] / (REAL)2.0f;
+        REAL box = (m == mh) ? FN(box_chord_inside)(dx, dy, dz, sx, sy, sz, x1, y1, z1, x2, y2, z2)
+                             : FN(box_chord)(sx, sy, sz, dx, dy, dz, x1, y1, z1, x2, y2, z2);
+        if (box != 0) {
+            REAL holes = 0;
+            for (int j = begin; j < begin + g->nh[m]; ++j) {
+                REAL hx = (REAL)C[100 + 9 * j], hy1 = (REAL)C[101 + 9 * j] + fov, hy2 = (REAL)C[102 + 9 * j] + fov;
+                REAL hz = (REAL)C[103 + 9 * j], r = (REAL)C[104 + 9 * j];
+                if (j == h) {
+                    REAL kk = kx * kx + kz * kz, t = len;
+                    if (kk > 0) t = FN(rmin)(t, r / SQRT(kk));
+                    if (ky > 0) t = FN(rmin)(t, (hy2 - sy) / ky);
+                    else if (ky < 0) t = FN(rmin)(t, (hy1 - sy) / ky);
+                    holes = holes + t;
+                } else {
+                    holes = holes + FN(cyl_chord)(sx, sy, sz, dx, dy, dz, hx, hy1, hy2, hz, r);
+                }
+            }
+            REAL L = box - holes;
+            if (L > 0) {
+                *w_pe = *w_pe + (REAL)Lh[6] * L;
+                *w_c = *w_c + (REAL)Lh[7] * L;
+            }
+        }
+        begin += g->nh[m];
+    }
+}
+
 static REAL FN(scatter_item)(const ogeo* g, int kind, int d, int k, REAL xs, REAL ys, REAL zs,
                              REAL w_s, const FN(crystal)* cd, REAL xI, REAL yI, REAL zI,
                              REAL xIs, REAL yIs, REAL zIs, REAL e0, REAL lo_w, REAL hi_w,
@@ -551,15 +634,19 @@ static REAL FN(scatter_item)(const ogeo* g, int kind, int d, int k, REAL xs, REA
     for (int a = 0; a < g->ncry; ++a) {
         if (a == d) continue;
         if (kind == 1 && a == k) continue;
-        long long bit;
-        if (kind == 1) {
-            long long i = k < d ? k : d, j = k < d ? d : k;
-            long long pair = i * g->ncry - (i * (i + 1)) / 2 + j;
-            bit = pair * g->ncry + a;
+        if (kind == 3) {                                       /* native: predicate, any layer */
+            if (!FN(collimator_related)(g, k, d, a)) continue;
         } else {
-            bit = ((long long)k * g->ncry + d) * g->ncry + a;
+            long long bit;
+            if (kind == 1) {
+                long long i = k < d ? k : d, j = k < d ? d : k;
+                long long pair = i * g->ncry - (i * (i + 1)) / 2 + j;
+                bit = pair * g->ncry + a;
+            } else {
+                bit = ((long long)k * g->ncry + d) * g->ncry + a;
+            }
+            if (!((bitmap[bit >> 5] >> (bit & 31)) & 1u)) continue;
         }
-        if (!((bitmap[bit >> 5] >> (bit & 31)) & 1u)) continue;
         FN(crystal) ca;
         FN(load_crystal)(g, a, &ca);
         REAL mpe = ca.mu_pe * e0 * e0 * e0 / es / es / es;
@@ -572,6 +659,15 @@ static REAL FN(scatter_item)(const ogeo* g, int kind, int d, int k, REAL xs, REA
                                 (REAL)-0.5f * ca.h, (REAL)0.5f * ca.w, (REAL)0.5f * ca.t,
                                 (REAL)0.5f * ca.h);
         att = att + la * mt;
+    }
+    if (kind == 3) {                                           /* native: tungsten at E' */
+        REAL w_pe, w_c;
+        FN(tungsten_path)(g, k, xs, ys, zs, xD, yD, zD, &w_pe, &w_c);
+        if (w_pe != 0 || w_c != 0) {
+            REAL mpe_w = w_pe * e0 * e0 * e0 / es / es / es;
+            REAL mc_w = w_c * e0 / es;
+            att = att + (mpe_w + mc_w);
+        }
     }
     const REAL bx1 = -cd->w / (REAL)2.0f, bx2 = cd->w / (REAL)2.0f;
     const REAL by1 = -cd->t / (REAL)2.0f, by2 = cd->t / (REAL)2.0f;
@@ -632,6 +728,22 @@ static REAL FN(scatter_element)(const ogeo* g, int part, int d, long long v, con
             sum = sum + FN(scatter_item)(g, 1, d, k, ck.x, ck.y, ck.z, prob, &cd, xI, yI, zI,
                                          xIs, yIs, zIs, e0, lo_w, hi_w, integ, bitmap,
                                          trace ? trace + 9 * k : NULL);
+        }
+    } else if (part == 4) {                                    /* native collimator model */
+        for (int h = 0; h < g->nholes; ++h) {
+            const int m = FN(hole_layer)(g, h, NULL);
+            REAL hx = (REAL)C[h * 9 + 100];
+            REAL hy = ((REAL)C[h * 9 + 101] + (REAL)C[h * 9 + 102]) / (REAL)2.0f + fov;
+            REAL hz = (REAL)C[h * 9 + 103];
+            REAL lih = FN(dist3)(xI, yI, zI, hx, hy, hz);
+            REAL T = (REAL)C[h * 9 + 102] - (REAL)C[h * 9 + 101];
+            REAL vr = (REAL)0.1f;
+            REAL sa = (REAL)(((double)(vr * vr) * M_PI + (double)(T * vr)) /
+                             (4.0f * M_PI * (double)lih * (double)lih) * (double)FABS(hy - yI) / (double)lih);
+            REAL prob = sa / (REAL)C[(m + 1) * 10 + 5] * (REAL)C[(m + 1) * 10 + 7];
+            sum = sum + FN(scatter_item)(g, 3, d, h, hx, hy, hz, prob, &cd, xI, yI, zI,
+                                         xIs, yIs, zIs, e0, lo_w, hi_w, integ, bitmap,
+                                         trace ? trace + 9 * h : NULL);
         }
     } else {
         for (int h = 0; h < g->nh0; ++h) {

@@ -92,6 +92,39 @@ def test_scatter_vs_fp64_oracle_fresh_system(gpu):
             assert flip_explained(geo, pe_h, part, bm, int(d), int(v))
 
 
+def test_native_scatter_vs_fp64_oracle(gpu):
+    """Native model (holes of every layer, their layer's mu, tungsten attenuation of the
+    scattered photon) against the oracle's restatement, on a two-layer system."""
+    geo = geometry.mini(seed=22, rotated=True, layers=2, nvox=(6, 6, 2), ncry=(5, 5))
+    ctx = sysmat.Context(geo)
+    pe = _pe(gpu, ctx, geo)
+    bc = ctx.bitmap_crystal()
+    out = gpu.empty_like(pe)
+    ctx.scatter_prepare(bc, ctx.bitmap_collimator())
+    ctx.scatter(out, pe, parts=1)
+    crystal_ref = out.cpu().numpy()
+    ctx.scatter_prepare_native(bc)
+    with pytest.raises(sysmat.SysmatError):               # tables prepared for another model
+        ctx.scatter(out, pe, parts=2)
+    ctx.scatter(out, pe, parts=1, hole_model=sysmat.HOLE_MODEL_NATIVE)
+    assert np.array_equal(out.cpu().numpy(), crystal_ref)  # the crystal part is the reference's
+    ctx.scatter(out, pe, parts=2, hole_model=sysmat.HOLE_MODEL_NATIVE)
+    a = out.cpu().numpy()
+    pe_h = pe.cpu().numpy()
+    bch = bc.cpu().numpy().view(np.uint32)
+    o32 = oracle.scatter(geo, pe_h, "collimator_native", bch, prec=32)
+    o64 = oracle.scatter(geo, pe_h, "collimator_native", bch, prec=64)
+    assert a.max() > 0
+    r = rel_err(a, o32)
+    assert np.mean(r > TOL) <= 0.01
+    for d, v in np.argwhere(r > 1e-4):
+        assert flip_explained(geo, pe_h, "collimator_native", bch, int(d), int(v))
+    # against FP64: the tungsten length is a plate chord minus nearly equal hole chords, so
+    # float cancellation puts FP32 about 1e-5 (relative) from FP64
+    r64 = rel_err(a, o64)
+    assert np.median(r64) < 1e-5 and np.mean(r64 > 1e-4) <= 0.01
+
+
 def test_scatter_block_decomposition_is_exact(gpu):
     geo, z, ctx, bc, bh, pe = _setup(gpu, "config3_z8")
     full = gpu.empty_like(pe)

@@ -244,3 +244,18 @@ def test_ellipse_chord_against_reference_golden():
         c = oracle.lib().oracle_cyl_chord(64, np.ascontiguousarray(np.r_[a[:10], r]).ctypes.data_as(oracle._dp))
         diff.append(abs(c - oracle.ell_chord(np.r_[a[:10], r, r, a[12]], 64)))
     assert np.mean(np.array(diff) < 1e-9) > 0.99
+
+
+def test_native_collimator_scatter_only_adds_attenuation_on_one_layer():
+    """With one layer the native model has the reference combined model's scatter points and
+    weights (layer 0 is every layer) and its attenuators (the predicate is the bitmap's), plus
+    the tungsten between hole and crystal: every element is at most the combined model's, and
+    the tungsten removes a visible part."""
+    geo = geometry.mini(seed=7, layers=1, nvox=(5, 4, 2), ncry=(4, 4))
+    pe = oracle.pe(geo, prec=64).astype(np.float32)
+    bh = oracle.bitmap_collimator(geo)
+    comb = oracle.scatter(geo, pe, "collimator", bh, prec=64)
+    nat = oracle.scatter(geo, pe, "collimator_native", bh, prec=64)
+    assert comb.max() > 0 and nat.max() > 0
+    assert np.all(nat <= comb * (1 + 1e-12) + 1e-30)
+    assert nat.sum() < 0.99 * comb.sum()
