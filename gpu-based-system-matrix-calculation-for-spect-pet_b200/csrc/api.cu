@@ -366,8 +366,8 @@ extern "C" SYSMAT_API int sysmat_scatter_prepare_native(sysmat_ctx* ctx, int par
     if ((parts & SYSMAT_SCATTER_CRYSTAL) && !d_bm_crystal) return SYSMAT_ERR_ARG;
     if ((parts & SYSMAT_SCATTER_COLLIMATOR) && (ctx->g.n_holes < 1 || ctx->g.n_layers < 1)) return SYSMAT_ERR_ARG;
     ctx->prepared_parts = 0;
-    const int rc = build_scatter_pairs_native(ctx->g, parts, d_bm_crystal, ctx->scratch, &ctx->pairs, &ctx->att,
-                                              (cudaStream_t)stream);
+    const int rc = build_scatter_pairs_native(ctx->g, parts, d_bm_crystal, ctx->scratch, &ctx->pairs,
+                                              &ctx->pairs_native, &ctx->att, (cudaStream_t)stream);
     if (rc == -2) return SYSMAT_ERR_NOMEM;
     if (rc) return SYSMAT_ERR_CUDA;
     ctx->prepared_parts = parts;
@@ -415,6 +415,7 @@ extern "C" SYSMAT_API int sysmat_scatter(sysmat_ctx* ctx, int parts, int hole_mo
     L.rotation = rotation;
     L.pe = d_pe;
     L.pairs = ctx->pairs;
+    L.native = ctx->pairs_native;
     L.att = ctx->att;
     L.out = d_out;
     if (!ctx->d_kn_tab || ctx->kn_e0 != ph.e0) {     // (re)build the FP64 Klein-Nishina table

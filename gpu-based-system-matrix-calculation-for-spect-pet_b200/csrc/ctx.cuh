@@ -30,6 +30,7 @@ struct sysmat_ctx {
     int prepared_parts = 0;
     int prepared_native = 0;        // the pair tables are the native model's
     sysmat::PairRec* pairs = nullptr;
+    sysmat::PairNative* pairs_native = nullptr;   // native model's extra pair fields
     sysmat::AttEntry* att = nullptr;
     double* d_kn_tab = nullptr;     // Klein-Nishina table for kn_e0
     float4* d_shapes = nullptr;     // elliptical holes (sysmat_set_hole_shapes), or nullptr

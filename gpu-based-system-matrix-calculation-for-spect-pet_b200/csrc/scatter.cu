@@ -425,7 +425,7 @@ __global__ void pair_count_kernel(DevGeom g, int parts, const uint32_t* bm_cry, 
 
 template <bool NATIVE>
 __global__ void pair_fill_kernel(DevGeom g, int parts, const uint32_t* bm_cry, const uint32_t* bm_col,
-                                 const int* offsets, PairRec* pairs, AttEntry* att)
+                                 const int* offsets, PairRec* pairs, PairNative* nat, AttEntry* att)
 {
     const int ns = g.n_det + (NATIVE ? g.n_holes : g.n_holes0);
     const long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -458,11 +458,17 @@ __global__ void pair_fill_kernel(DevGeom g, int parts, const uint32_t* bm_cry, c
         r.att_count = k;
         if (NATIVE && s >= g.n_det) {
             const int h = s - g.n_det;
-            tungsten_path(g, h, xs, ys, zs, q.xD, q.yD, q.zD, r.w_pe, r.w_c);
+            PairNative n{};
+            tungsten_path(g, h, xs, ys, zs, q.xD, q.yD, q.zD, n.w_pe, n.w_c);
             const LayerInfo& Ly = g.layer[hole_layer(g, h)];
-            r.mu_tot_h = Ly.mu_total;
-            r.mu_c_h = Ly.mu_c;
+            n.mu_tot_h = Ly.mu_total;
+            n.mu_c_h = Ly.mu_c;
+            nat[p] = n;
+        } else if (NATIVE) {
+            nat[p] = PairNative{};
         }
+    } else if (NATIVE) {
+        nat[p] = PairNative{};
     }
     pairs[p] = r;
 }
@@ -481,7 +487,9 @@ struct ElemConst {
 
 // One (d, v, s) item; w_s is the interaction weight (PE * muC/muPE or hole solid angle *
 // muC/mu of layer 0).  Returns the float the reference would atomically add.
-__device__ float scatter_item(const ElemConst& e, const PairRec& pr, const AttEntry* __restrict__ att,
+template <bool NATIVE>
+__device__ float scatter_item(const ElemConst& e, const PairRec& pr, const PairNative& pn,
+                              const AttEntry* __restrict__ att,
                               float xs, float ys, float zs, float w_s, float e0, float integ,
                               const double* __restrict__ kn_tab)
 {
@@ -536,9 +544,9 @@ __device__ float scatter_item(const ElemConst& e, const PairRec& pr, const AttEn
         }
         a_sum = a_sum + ae.len * mt;
     }
-    if (pr.w_pe != 0.0f || pr.w_c != 0.0f) {             // native model: tungsten at E'
-        const float mpe_w = pr.w_pe * e0 * e0 * e0 / es / es / es;
-        const float mc_w = pr.w_c * e0 / es;
+    if (NATIVE && (pn.w_pe != 0.0f || pn.w_c != 0.0f)) {  // native model: tungsten at E'
+        const float mpe_w = pn.w_pe * e0 * e0 * e0 / es / es / es;
+        const float mc_w = pn.w_c * e0 / es;
         a_sum = a_sum + (mpe_w + mc_w);
     }
     const float mpe_s = e.mu_pe * e0 * e0 * e0 / es / es / es;              // :1411-1417
@@ -550,16 +558,18 @@ __device__ float scatter_item(const ElemConst& e, const PairRec& pr, const AttEn
     return (float)c;
 }
 
+template <bool NATIVE>
 __global__ void __launch_bounds__(kItemThreads)
 scatter_kernel(DevGeom g, ScatterPhysics ph, ScatterLaunch L)
 {
     __shared__ PairRec sp[kPairChunk];
+    __shared__ PairNative spn[NATIVE ? kPairChunk : 1];
     const int di = blockIdx.y;
     const int d = L.det_begin + di;
     const long long vi = (long long)blockIdx.x * kItemThreads + threadIdx.x;
     const bool active = vi < L.vox_count;
     const long long v = L.vox_begin + (active ? vi : 0);
-    const int ns = g.n_det + (L.hole_model == 2 ? g.n_holes : g.n_holes0);
+    const int ns = g.n_det + (NATIVE ? g.n_holes : g.n_holes0);
 
     const float4 P = __ldg(&g.cry.pos[d]), S = __ldg(&g.cry.size[d]);
     const float4 M = __ldg(&g.cry.mu[d]), T = __ldg(&g.cry.trig[d]);
@@ -590,7 +600,10 @@ scatter_kernel(DevGeom g, ScatterPhysics ph, ScatterLaunch L)
     for (int s0 = s_begin; s0 < s_end; s0 += kPairChunk) {
         const int cnt = min(kPairChunk, s_end - s0);
         __syncthreads();
-        for (int k = threadIdx.x; k < cnt; k += kItemThreads) sp[k] = prow[s0 + k];
+        for (int k = threadIdx.x; k < cnt; k += kItemThreads) {
+            sp[k] = prow[s0 + k];
+            if constexpr (NATIVE) spn[k] = L.native[(long long)d * ns + s0 + k];
+        }
         __syncthreads();
         if (!run || !active) continue;
         for (int k = 0; k < cnt; ++k) {
@@ -620,11 +633,12 @@ scatter_kernel(DevGeom g, ScatterPhysics ph, ScatterLaunch L)
                     const float vr = 0.2f;
                     sa = (vr * vr + (hr.z - hr.y) * vr) / (4.0f * lih * lih);
                 }
-                if (L.hole_model == 2) w_s = sa / pr.mu_tot_h * pr.mu_c_h;     // the hole's own layer
+                if (NATIVE) w_s = sa / spn[k].mu_tot_h * spn[k].mu_c_h;        // the hole's own layer
                 else w_s = sa / ph.col_mu_tot0 * ph.col_mu_c0;            // :1716
             }
             // one call site keeps a single copy of the item code
-            const double c = (double)scatter_item(e, pr, L.att, xs, ys, zs, w_s, ph.e0, ph.integ, L.kn_tab);
+            const double c = (double)scatter_item<NATIVE>(e, pr, spn[NATIVE ? k : 0], L.att, xs, ys, zs, w_s,
+                                                          ph.e0, ph.integ, L.kn_tab);
             if (crystal) acc_c += c;
             else acc_h += c;
         }
@@ -671,7 +685,7 @@ int launch_bitmap_collimator(const DevGeom& g, uint32_t* words, cudaStream_t s)
 
 template <bool NATIVE>
 static int build_pairs(const DevGeom& g, int parts, const uint32_t* bm_cry, const uint32_t* bm_col,
-                       ScatterScratch& scratch, PairRec** pairs, AttEntry** att, cudaStream_t s)
+                       ScatterScratch& scratch, PairRec** pairs, PairNative** native, AttEntry** att, cudaStream_t s)
 {
     const int ns = g.n_det + (NATIVE ? g.n_holes : g.n_holes0);
     const long long np = (long long)g.n_det * ns;
@@ -683,7 +697,8 @@ static int build_pairs(const DevGeom& g, int parts, const uint32_t* bm_cry, cons
     const size_t off_offsets = align(off_counts + sizeof(int) * (np + 1));
     const size_t off_temp = align(off_offsets + sizeof(int) * (np + 1));
     const size_t off_pairs = align(off_temp + temp_bytes);
-    const size_t fixed = align(off_pairs + sizeof(PairRec) * np);
+    const size_t off_native = align(off_pairs + sizeof(PairRec) * np);
+    const size_t fixed = align(off_native + (NATIVE ? sizeof(PairNative) * np : 0));
     if (scratch.bytes < fixed) {
         scatter_scratch_free(scratch);
         if (cudaMalloc(&scratch.base, fixed) != cudaSuccess) { scratch.base = nullptr; return -2; }
@@ -713,28 +728,31 @@ static int build_pairs(const DevGeom& g, int parts, const uint32_t* bm_cry, cons
         cub::DeviceScan::ExclusiveSum(base + off_temp, temp_bytes, counts, offsets, (int)(np + 1), s);
     }
     *pairs = (PairRec*)(base + off_pairs);
+    PairNative* nat = NATIVE ? (PairNative*)(base + off_native) : nullptr;
+    if (native) *native = nat;
     *att = (AttEntry*)(base + fixed);
-    pair_fill_kernel<NATIVE><<<blocks, 256, 0, s>>>(g, parts, bm_cry, bm_col, offsets, *pairs, *att);
+    pair_fill_kernel<NATIVE><<<blocks, 256, 0, s>>>(g, parts, bm_cry, bm_col, offsets, *pairs, nat, *att);
     return cudaGetLastError() == cudaSuccess ? 0 : -1;
 }
 
 int build_scatter_pairs(const DevGeom& g, int parts, const uint32_t* bm_cry, const uint32_t* bm_col,
                         ScatterScratch& scratch, PairRec** pairs, AttEntry** att, cudaStream_t s)
 {
-    return build_pairs<false>(g, parts, bm_cry, bm_col, scratch, pairs, att, s);
+    return build_pairs<false>(g, parts, bm_cry, bm_col, scratch, pairs, nullptr, att, s);
 }
 
 int build_scatter_pairs_native(const DevGeom& g, int parts, const uint32_t* bm_cry, ScatterScratch& scratch,
-                               PairRec** pairs, AttEntry** att, cudaStream_t s)
+                               PairRec** pairs, PairNative** native, AttEntry** att, cudaStream_t s)
 {
-    return build_pairs<true>(g, parts, bm_cry, nullptr, scratch, pairs, att, s);
+    return build_pairs<true>(g, parts, bm_cry, nullptr, scratch, pairs, native, att, s);
 }
 
 int launch_scatter(const DevGeom& g, const ScatterPhysics& ph, const ScatterLaunch& L, cudaStream_t s)
 {
     if (L.det_count == 0 || L.vox_count == 0) return 0;
     dim3 grid((unsigned)((L.vox_count + kItemThreads - 1) / kItemThreads), (unsigned)L.det_count);
-    scatter_kernel<<<grid, kItemThreads, 0, s>>>(g, ph, L);
+    if (L.hole_model == 2) scatter_kernel<true><<<grid, kItemThreads, 0, s>>>(g, ph, L);
+    else scatter_kernel<false><<<grid, kItemThreads, 0, s>>>(g, ph, L);
     return cudaGetLastError() == cudaSuccess ? 0 : -1;
 }
 

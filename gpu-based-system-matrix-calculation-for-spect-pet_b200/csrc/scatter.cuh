@@ -33,9 +33,12 @@ struct PairRec {
     int att_begin;         // first entry in the attenuator list
     int att_count;         // number of attenuators with a non-zero chord
     int valid;             // 0 for the excluded pair s == d
-    // native model only (0 otherwise): tungsten on the way from a hole scatter point to d,
-    // sum_m mu_pe,m L_m and sum_m mu_C,m L_m at the photopeak, and the scatter hole's layer
-    // mu_total and mu_C (its interaction weight)
+};
+
+// Native model only, beside each PairRec: tungsten on the way from a hole scatter point to d,
+// sum_m mu_pe,m L_m and sum_m mu_C,m L_m at the photopeak, and the scatter hole's layer
+// mu_total and mu_C (its interaction weight); zero for crystal scatterers.
+struct PairNative {
     float w_pe, w_c, mu_tot_h, mu_c_h;
 };
 
@@ -63,6 +66,7 @@ struct ScatterLaunch {
     float rotation;
     const float* pe;       // D x V photoelectric matrix (crystal part)
     const PairRec* pairs;
+    const PairNative* native;   // hole_model 2 only
     const AttEntry* att;
     const double* kn_tab;  // Klein-Nishina table (kn_table_build), kKnTable + 1 nodes on [0, pi]
     float* out;
@@ -90,7 +94,8 @@ int build_scatter_pairs(const DevGeom& g, int parts, const uint32_t* bm_crystal,
 // collimator-scatter attenuators from the relationship predicate evaluated directly (no
 // bitmap); tungsten attenuation of the scattered photon on its way to the crystal.
 int build_scatter_pairs_native(const DevGeom& g, int parts, const uint32_t* bm_crystal,
-                               ScatterScratch& scratch, PairRec** pairs, AttEntry** att, cudaStream_t s);
+                               ScatterScratch& scratch, PairRec** pairs, PairNative** native, AttEntry** att,
+                               cudaStream_t s);
 
 int launch_scatter(const DevGeom& g, const ScatterPhysics& ph, const ScatterLaunch& L,
                    cudaStream_t s);
