@@ -14,7 +14,9 @@ Reported: `value` = device-timed elements/s over all ranks (inputs resident in H
 device parameter copy and device to host matrix copy inside the timed region), `roofline`
 of the PE kernel against measured FP32 / MUFU peaks, `cpu_baseline` = the CPU oracle (the
 reference's float arithmetic restated in C, OpenMP) on a bounded sample, and `scatter` =
-the primary-Compton rate on a configuration-3 plane.
+the primary-Compton rate on a configuration-3 plane, `batch` = the configuration-4 design
+sweep in one batched launch against one launch per task, `sampled` = configuration 2 with
+the sampling it states (2x2x2 voxel sub-samples, 2x8x2 crystal sub-elements).
 
 `--impl reference` times the reference's own CUDA program (its source compiled for sm_100a
 by oracle/Makefile into oracle/_ref) through its own host entry point PESysMatGen on a
@@ -265,6 +267,10 @@ def run_sysmat(args, rank, world, local):
     if not args.no_batch and world == 1:
         batch = run_batch(args, sysmat, torch)
 
+    sampled = None
+    if not args.no_sampled and world == 1:
+        sampled = run_sampled(args, sysmat, torch)
+
     result = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": region_ms / args.steps, "higher_is_better": True,
@@ -274,7 +280,7 @@ def run_sysmat(args, rank, world, local):
                    "elements_per_step_per_gpu": D * nxy, "summation": "reference order (float chain)",
                    "l2": "flushed between steps (256 MB write)"},
         "clocks": clk.summary(), "gpu_launches": args.steps,
-        "roofline": roof, "e2e": e2e, "scatter": scatter, "batch": batch,
+        "roofline": roof, "e2e": e2e, "scatter": scatter, "batch": batch, "sampled": sampled,
     }
     return result
 
@@ -326,6 +332,36 @@ def run_scatter(args, sysmat, torch):
     return {"value": ctx.n_det * ctx.n_vox / (ms * 1e-3), "unit": UNIT, "ms_per_step": ms,
             "workload": "config3 primary Compton (crystal + collimator) on z-plane 8: 1024 crystals x "
                         "2304 voxels, 1024 layer-0 holes"}
+
+
+def run_sampled(args, sysmat, torch, rows=512):
+    """Configuration 2 with the sampling it states (no reference counterpart): each voxel
+    sampled at 2x2x2 source points, each crystal divided 2x8x2 (x, depth, z), every
+    contribution summed in FP64 (sysmat_pe_sampled).  `rows` crystals of the array's centre x
+    z-plane 16 (9216 voxels) per step."""
+    g = geometry.config2()
+    ctx = sysmat.Context(g)
+    nxy = int(g.image[0]) * int(g.image[1])
+    d0 = ctx.n_det // 2 - rows // 2
+    out = torch.empty((rows, nxy), dtype=torch.float32, device="cuda")
+
+    def step():
+        ctx.pe_sampled(out, (2, 8, 2), (2, 2, 2), det_begin=d0, det_count=rows, vox_begin=16 * nxy, vox_count=nxy)
+
+    step()
+    torch.cuda.synchronize()
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    n = 2
+    a.record()
+    for _ in range(n):
+        step()
+    b.record()
+    torch.cuda.synchronize()
+    ms = a.elapsed_time(b) / n
+    return {"value": rows * nxy / (ms * 1e-3), "unit": UNIT, "ms_per_step": ms, "rays_per_element": 8 * 32,
+            "summation": "FP64",
+            "workload": f"config2 as stated: 2x2x2 voxel sub-samples, 2x8x2 crystal sub-elements; crystals "
+                        f"{d0}..{d0 + rows - 1} x z-plane 16 ({rows * nxy} elements)"}
 
 
 def run_batch(args, sysmat, torch, n_instances=64, rows=8, sweep=True):
@@ -496,6 +532,7 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-scatter", action="store_true")
     ap.add_argument("--no-batch", action="store_true")
+    ap.add_argument("--no-sampled", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
     if args.warmup < 3 and args.impl == "sysmat":

@@ -318,6 +318,47 @@ extern "C" SYSMAT_API int sysmat_pe(sysmat_ctx* ctx, float rotation, int det_beg
     return SYSMAT_OK;
 }
 
+extern "C" SYSMAT_API int sysmat_pe_sampled(sysmat_ctx* ctx, float rotation, int det_begin, int det_count,
+                                            long long vox_begin, long long vox_count, const int* crystal_div,
+                                            const int* voxel_sub, float* d_out, long long ld, void* stream)
+{
+    int rc = check_block(ctx, det_begin, det_count, vox_begin, vox_count, d_out, ld);
+    if (rc) return rc;
+    if (!crystal_div || !voxel_sub) return SYSMAT_ERR_ARG;
+    Sampling smp;
+    smp.nx = crystal_div[0]; smp.ny = crystal_div[1]; smp.nz = crystal_div[2];
+    smp.sx = voxel_sub[0]; smp.sy = voxel_sub[1]; smp.sz = voxel_sub[2];
+    const int div[3] = {smp.nx, smp.ny, smp.nz}, sub[3] = {smp.sx, smp.sy, smp.sz};
+    for (int k = 0; k < 3; ++k) {
+        if (div[k] < 1 || div[k] > SYSMAT_SAMPLED_MAX_DIV) return SYSMAT_ERR_ARG;
+        if (sub[k] < 1 || sub[k] > SYSMAT_SAMPLED_MAX_SUB) return SYSMAT_ERR_ARG;
+    }
+    if (smp.nx * smp.ny * smp.nz > SYSMAT_SAMPLED_MAX_SUBELEMENTS) return SYSMAT_ERR_ARG;
+    if (smp.sx * smp.sy * smp.sz > SYSMAT_SAMPLED_MAX_POINTS) return SYSMAT_ERR_ARG;
+    if (det_count == 0 || vox_count == 0) return SYSMAT_OK;
+    cudaStream_t s = (cudaStream_t)stream;
+    CUDA_TRY(cudaMemsetAsync(ctx->d_counter, 0, sizeof(unsigned long long), s));
+    CUDA_TRY(cudaMemsetAsync(ctx->d_status, 0, sizeof(int), s));
+    PeLaunch L;
+    L.det_begin = det_begin;
+    L.det_count = det_count;
+    L.vox_begin = vox_begin;
+    L.vox_count = vox_count;
+    L.ld = ld;
+    L.rotation = rotation;
+    L.out = d_out;
+    L.work_counter = ctx->d_counter;
+    L.status = ctx->d_status;
+    L.counters = nullptr;
+    L.smp = smp;
+    if (launch_pe_sampled(ctx->g, L, ctx->num_sms, s)) return SYSMAT_ERR_CUDA;
+    int status = 0;
+    CUDA_TRY(cudaMemcpyAsync(&status, ctx->d_status, sizeof(int), cudaMemcpyDeviceToHost, s));
+    CUDA_TRY(cudaStreamSynchronize(s));
+    if (status & kStatusCapacity) return SYSMAT_ERR_CAPACITY;
+    return SYSMAT_OK;
+}
+
 extern "C" SYSMAT_API long long sysmat_bitmap_crystal_words(const sysmat_ctx* ctx)
 {
     return ctx ? bitmap_crystal_words(ctx->g.n_det) : SYSMAT_ERR_ARG;

@@ -348,17 +348,20 @@ __device__ __forceinline__ void to_crystal_frame(float cx, float cy, float cz, f
 }
 
 // Voxel centre of flat index v, rotated about z (PESysMatGen.cu:1031-1052).
+// Point of voxel v at fractions (fx, fy, fz) of its extent (1/2: the centre the reference
+// uses), rotated about z (PESysMatGen.cu:1031-1052).
 __device__ __forceinline__ void voxel_centre(const DevGeom& g, long long v, float cr, float sr,
-                                             float& x, float& y, float& z)
+                                             float& x, float& y, float& z, float fx = 0.5f,
+                                             float fy = 0.5f, float fz = 0.5f)
 {
     const long long nxy = (long long)g.nx * g.ny;
     const int iz = (int)(v / nxy);
     const long long r = v - (long long)iz * nxy;
     const int iy = (int)(r / g.nx);
     const int ix = (int)(r - (long long)iy * g.nx);
-    float xv = ((float)ix - (float)g.nx / 2.0f + 0.5f) * g.wx;
-    float yv = ((float)iy - (float)g.ny / 2.0f + 0.5f) * g.wy;
-    float zv = ((float)iz - (float)g.nz / 2.0f + 0.5f) * g.wz;
+    float xv = ((float)ix - (float)g.nx / 2.0f + fx) * g.wx;
+    float yv = ((float)iy - (float)g.ny / 2.0f + fy) * g.wy;
+    float zv = ((float)iz - (float)g.nz / 2.0f + fz) * g.wz;
     xv = xv + g.shx;
     yv = yv + g.shy;
     zv = zv + g.shz;

@@ -448,15 +448,17 @@ struct SubElem {
     float xDs, yDs, zDs, xD, yD, zD, dsq, sq, cosang, sa_a, sa_b;
 };
 
-__device__ __forceinline__ SubElem sub_element(const Elem& e, int s)
+// Sub-element (ix, iy, iz) of a crystal divided into fx x fy x fz (x, depth, z) parts.
+__device__ __forceinline__ SubElem sub_element_at(const Elem& e, int ix, int iy, int iz, float fx, float fy,
+                                                  float fz)
 {
     SubElem q;
-    q.iz = s >> 7;
-    q.ix = (s >> 4) & 7;
-    q.iy = s & 15;
-    q.xDs = -e.w / 2.0f + ((float)q.ix + 0.5f) / 8.0f * e.w;   // :1207-1217
-    q.zDs = -e.h / 2.0f + ((float)q.iz + 0.5f) / 8.0f * e.h;
-    q.yDs = -e.t / 2.0f + ((float)q.iy + 0.5f) / 16.0f * e.t;
+    q.iz = iz;
+    q.ix = ix;
+    q.iy = iy;
+    q.xDs = -e.w / 2.0f + ((float)q.ix + 0.5f) / fx * e.w;   // :1207-1217
+    q.zDs = -e.h / 2.0f + ((float)q.iz + 0.5f) / fz * e.h;
+    q.yDs = -e.t / 2.0f + ((float)q.iy + 0.5f) / fy * e.t;
     q.xD = e.xd + (q.xDs * e.cosr - q.zDs * e.sinr);
     q.zD = e.zd + (q.xDs * e.sinr + q.zDs * e.cosr);
     q.yD = e.yd + q.yDs;
@@ -474,6 +476,12 @@ __device__ __forceinline__ SubElem sub_element(const Elem& e, int s)
     return q;
 }
 
+// Reference sub-element s = 128 iz + 16 ix + iy of the 8 x 16 x 8 division.
+__device__ __forceinline__ SubElem sub_element(const Elem& e, int s)
+{
+    return sub_element_at(e, (s >> 4) & 7, s & 15, s >> 7, 8.0f, 16.0f, 8.0f);
+}
+
 // Plate penalty (:1240-1254); true if any layer fired.
 __device__ __forceinline__ bool plate_penalty(const DevGeom& g, const WarpSmem& ws, const Elem& e,
                                               const SubElem& q, float& att)
@@ -489,17 +497,18 @@ __device__ __forceinline__ bool plate_penalty(const DevGeom& g, const WarpSmem& 
     return blocked;
 }
 
-// Self attenuation, absorption and solid angle for a sub-element, given the attenuation
-// accumulated outside crystal d (:1223-1231, :1329-1357).
-__device__ __forceinline__ float finish_sub_element(const Elem& e, const SubElem& q, float att)
+// Self attenuation, absorption and solid angle for a sub-element of an fx x fy x fz
+// division, given the attenuation accumulated outside crystal d (:1223-1231, :1329-1357).
+__device__ __forceinline__ float finish_sub_element_at(const Elem& e, const SubElem& q, float att, float fx,
+                                                       float fy, float fz)
 {
     const float w = e.w, t = e.t, h = e.h;
-    const float ux1 = ((float)q.ix / 8.0f - 0.5f) * w;
-    const float ux2 = (((float)q.ix + 1.0f) / 8.0f - 0.5f) * w;
-    const float uy1 = ((float)q.iy / 16.0f - 0.5f) * t;
-    const float uy2 = (((float)q.iy + 1.0f) / 16.0f - 0.5f) * t;
-    const float uz1 = ((float)q.iz / 8.0f - 0.5f) * h;
-    const float uz2 = (((float)q.iz + 1.0f) / 8.0f - 0.5f) * h;
+    const float ux1 = ((float)q.ix / fx - 0.5f) * w;
+    const float ux2 = (((float)q.ix + 1.0f) / fx - 0.5f) * w;
+    const float uy1 = ((float)q.iy / fy - 0.5f) * t;
+    const float uy2 = (((float)q.iy + 1.0f) / fy - 0.5f) * t;
+    const float uz1 = ((float)q.iz / fz - 0.5f) * h;
+    const float uz2 = (((float)q.iz + 1.0f) / fz - 0.5f) * h;
     const float cbox[6] = {-w / 2.0f, -t / 2.0f, -h / 2.0f, w / 2.0f, t / 2.0f, h / 2.0f};
     const float ubox[6] = {ux1, uy1, uz1, ux2, uy2, uz2};
     float l1, l2;
@@ -514,7 +523,7 @@ __device__ __forceinline__ float finish_sub_element(const Elem& e, const SubElem
     // solid angle in double, as the reference's 4*M_PI promotion makes it; one shared
     // reciprocal (the float results round identically except in double-rounding ties)
     const double rq = 1.0 / ((4.0 * 3.14159265358979323846) * (double)q.dsq * (double)q.sq);
-    const float ax = t * h / 8.0f / 16.0f, az = w * t / 8.0f / 16.0f, ay = w * h / 8.0f / 8.0f;
+    const float ax = t * h / fz / fy, az = w * t / fx / fy, ay = w * h / fx / fz;
     const float sax = (float)((double)ax * (double)fabsf((q.xD - e.xI) * e.cosr - (q.zD - e.zI) * e.sinr) * rq);
     const float saz = (float)((double)az * (double)fabsf((q.xD - e.xI) * e.sinr + (q.zD - e.zI) * e.cosr) * rq);
     const float say = (float)((double)ay * (double)fabsf(q.yD - e.yI) * rq);
@@ -523,13 +532,19 @@ __device__ __forceinline__ float finish_sub_element(const Elem& e, const SubElem
     return eff * sa * absf;
 }
 
+__device__ __forceinline__ float finish_sub_element(const Elem& e, const SubElem& q, float att)
+{
+    return finish_sub_element_at(e, q, att, 8.0f, 16.0f, 8.0f);
+}
+
 // Per-element set-up shared by the lanes of a warp: voxel centre, crystal d, reference cone
 // constants, slope rectangle and the plate "through both faces" rectangles.  False when the
 // crystal's attenuation is too low for the reference to compute the element (it is 0).
 __device__ __forceinline__ bool init_element(const DevGeom& g, WarpSmem& ws, int d, long long v, float cr,
-                                             float sr, int lane, Elem& e)
+                                             float sr, int lane, Elem& e, float fx = 0.5f, float fy = 0.5f,
+                                             float fz = 0.5f)
 {
-    voxel_centre(g, v, cr, sr, e.xI, e.yI, e.zI);
+    voxel_centre(g, v, cr, sr, e.xI, e.yI, e.zI, fx, fy, fz);   // the source point in the voxel
     const float4 P = __ldg(&g.cry.pos[d]);
     const float4 S = __ldg(&g.cry.size[d]);
     const float4 M = __ldg(&g.cry.mu[d]);
@@ -567,6 +582,75 @@ __device__ __forceinline__ bool init_element(const DevGeom& g, WarpSmem& ws, int
     return true;
 }
 
+// Kept-list state of one element (source point) of a warp: the first chunk's end, whether the
+// whole list fits one chunk, and the current chunk's entry count.
+struct KeptList {
+    int n_src, cursor, count;
+    bool from_super, single;
+};
+
+__device__ __forceinline__ KeptList start_kept_list(const DevGeom& g, const BlockSmem& bs, WarpSmem& ws,
+                                                    const Elem& e, int d, int lane)
+{
+    KeptList k;
+    k.from_super = bs.s_count >= 0;
+    k.n_src = k.from_super ? bs.s_count : g.n_holes + g.n_det;
+    k.count = 0;
+    k.cursor = build_chunk(g, bs, ws, e, d, 0, k.n_src, k.from_super, lane, &k.count);
+    k.single = k.cursor >= k.n_src;
+    return k;
+}
+
+// Attenuation outside crystal d along the ray of sub-element q, into s: plate penalty, then
+// the kept objects that meet the round's slope box, walked in round buffers (an overfull
+// round in pieces: each lane's walk state carries over, so the attenuation order is kept).
+// Returns whether the lane skips the sub-element: `dead`, or blocked with every mu >= 0 (the
+// contribution is then exactly 0).
+template <bool COUNT, bool ELL>
+__device__ __forceinline__ bool walk_sub_element(const DevGeom& g, const BlockSmem& bs, WarpSmem& ws,
+                                                 const Elem& e, int d, const SubElem& q, bool dead,
+                                                 bool first_round, KeptList& kl, int lane, Walk& s,
+                                                 long long& n_sub_entries)
+{
+    RayCyl rc;
+    ray_cyl_init(rc, e.xI, e.yI, e.zI, q.xD, q.yD, q.zD);
+    const bool blocked = plate_penalty(g, ws, e, q, s.att);
+    const bool skip = dead || (blocked && g.nonneg_mu);
+    // slope box of the rays that still need the walk in this round
+    float4 box = make_float4(skip ? INFINITY : q.sa_a, skip ? -INFINITY : q.sa_a,
+                             skip ? INFINITY : q.sa_b, skip ? -INFINITY : q.sa_b);
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) {
+        box.x = fminf(box.x, __shfl_xor_sync(0xffffffffu, box.x, off));
+        box.y = fmaxf(box.y, __shfl_xor_sync(0xffffffffu, box.y, off));
+        box.z = fminf(box.z, __shfl_xor_sync(0xffffffffu, box.z, off));
+        box.w = fmaxf(box.w, __shfl_xor_sync(0xffffffffu, box.w, off));
+    }
+    int cur = 0;
+    bool first_chunk = true;
+    while (true) {
+        if (!kl.single && !first_chunk) {
+            cur = build_chunk(g, bs, ws, e, d, cur, kl.n_src, kl.from_super, lane, &kl.count);
+        } else if (!kl.single) {
+            if (!first_round) cur = build_chunk(g, bs, ws, e, d, 0, kl.n_src, kl.from_super, lane, &kl.count);
+            else cur = kl.cursor;
+        }
+        first_chunk = false;
+        int k = 0;
+        while (k < kl.count) {
+            int next = kl.count, nh = 0;
+            const int nr = fill_round<ELL>(g, ws, e, k, kl.count, box, 0, lane, &next, &nh);
+            if constexpr (COUNT) n_sub_entries += nr;
+            if (!skip) walk_round<ELL>(g, ws, nh, nr, q.xD, q.yD, q.zD, q.sa_a, q.sa_b, q.cosang, rc, s);
+            __syncwarp();
+            k = next;
+        }
+        if (kl.single || cur >= kl.n_src) break;
+    }
+    if (!skip && s.lay < g.n_layers) close_layers(g, s, g.n_layers, q.cosang);
+    return skip;
+}
+
 template <int MODE, bool COUNT, bool ELL = false>
 __device__ double pe_element(const DevGeom& g, const BlockSmem& bs, WarpSmem& ws, int d,
                              long long v, float cr, float sr, int lane,
@@ -574,11 +658,7 @@ __device__ double pe_element(const DevGeom& g, const BlockSmem& bs, WarpSmem& ws
 {
     Elem e;
     if (!init_element(g, ws, d, v, cr, sr, lane, e)) return 0.0;
-    const bool from_super = bs.s_count >= 0;
-    const int n_src = from_super ? bs.s_count : g.n_holes + g.n_det;
-    int count = 0;
-    int cursor = build_chunk(g, bs, ws, e, d, 0, n_src, from_super, lane, &count);
-    const bool single = cursor >= n_src;
+    KeptList kl = start_kept_list(g, bs, ws, e, d, lane);
 
     float chain = 0.0f;
     double dacc = 0.0;
@@ -592,49 +672,9 @@ __device__ double pe_element(const DevGeom& g, const BlockSmem& bs, WarpSmem& ws
                          (lane & 1);
         const SubElem q = sub_element(e, sidx);
         Walk s{0.0f, 0.0f, 0, 0, 0, 0, 0};
-        RayCyl rc;
-        ray_cyl_init(rc, e.xI, e.yI, e.zI, q.xD, q.yD, q.zD);
-        const bool blocked = plate_penalty(g, ws, e, q, s.att);
-        const bool skip = blocked && g.nonneg_mu;
-        // slope box of the rays that still need the walk in this round
-        float4 box = make_float4(skip ? INFINITY : q.sa_a, skip ? -INFINITY : q.sa_a,
-                                 skip ? INFINITY : q.sa_b, skip ? -INFINITY : q.sa_b);
-#pragma unroll
-        for (int off = 16; off > 0; off >>= 1) {
-            box.x = fminf(box.x, __shfl_xor_sync(0xffffffffu, box.x, off));
-            box.y = fmaxf(box.y, __shfl_xor_sync(0xffffffffu, box.y, off));
-            box.z = fminf(box.z, __shfl_xor_sync(0xffffffffu, box.z, off));
-            box.w = fmaxf(box.w, __shfl_xor_sync(0xffffffffu, box.w, off));
-        }
-        // walk this round's objects: kept entries meeting the round box, copied with their
-        // geometry into the round buffer; an overfull round is walked in pieces (the walk
-        // state of each lane carries over, so the attenuation order is unchanged)
-        int cur = 0;
-        bool first_chunk = true;
-        while (true) {
-            if (!single && !first_chunk) {
-                cur = build_chunk(g, bs, ws, e, d, cur, n_src, from_super, lane, &count);
-            } else if (!single) {
-                if (r > 0) cur = build_chunk(g, bs, ws, e, d, 0, n_src, from_super, lane, &count);
-                else cur = cursor;
-            }
-            first_chunk = false;
-            int k = 0;
-            while (k < count) {
-                int next = count, nh = 0;
-                const int nr = fill_round<ELL>(g, ws, e, k, count, box, 0, lane, &next, &nh);
-                if constexpr (COUNT) n_sub_entries += nr;
-                if (!skip) walk_round<ELL>(g, ws, nh, nr, q.xD, q.yD, q.zD, q.sa_a, q.sa_b, q.cosang, rc, s);
-                __syncwarp();
-                k = next;
-            }
-            if (single || cur >= n_src) break;
-        }
-        float contrib = 0.0f;
-        if (!skip) {
-            if (s.lay < g.n_layers) close_layers(g, s, g.n_layers, q.cosang);
-            contrib = finish_sub_element(e, q, s.att);
-        }
+        const bool skip = walk_sub_element<COUNT, ELL>(g, bs, ws, e, d, q, false, r == 0, kl, lane, s,
+                                                       n_sub_entries);
+        const float contrib = skip ? 0.0f : finish_sub_element(e, q, s.att);
         if constexpr (COUNT) {
             n_hole_hits += s.hole_hits;
             n_cry_hits += s.cry_hits;
@@ -669,8 +709,8 @@ __device__ double pe_element(const DevGeom& g, const BlockSmem& bs, WarpSmem& ws
             atomicAdd(&counters[2], (unsigned long long)n_cry_hits);
             atomicAdd(&counters[3], 1ull);
             atomicAdd(&counters[4], (unsigned long long)n_blocked);
-            atomicAdd(&counters[5], single ? 0ull : 1ull);                 // chunked elements
-            atomicAdd(&counters[6], (unsigned long long)count);            // kept objects (1st chunk)
+            atomicAdd(&counters[5], kl.single ? 0ull : 1ull);              // chunked elements
+            atomicAdd(&counters[6], (unsigned long long)kl.count);         // kept objects (last chunk)
             atomicAdd(&counters[7], (unsigned long long)n_sub_entries);    // round sub-list entries
             atomicAdd(&counters[8], bs.s_count < 0 ? 1ull : 0ull);         // superset overflow
             atomicAdd(&counters[9], (unsigned long long)(bs.s_count < 0 ? 0 : bs.s_count));
@@ -685,6 +725,45 @@ __device__ double pe_element(const DevGeom& g, const BlockSmem& bs, WarpSmem& ws
         for (int off = 16; off > 0; off >>= 1) dacc += __shfl_xor_sync(0xffffffffu, dacc, off);
         return dacc;
     }
+}
+
+// Element of the sampled form: the mean over the voxel's sx x sy x sz source points (centres of
+// a grid over the voxel) of the reference's element with crystal d divided into nx x ny x nz
+// sub-elements (x, depth, z), every contribution summed in FP64.  Each source point has its
+// own cone test and kept list; its sub-elements are taken 32 at a time in (z, depth, x) order,
+// x fastest, so a round is a compact patch of the crystal.  With 8 x 16 x 8 and 1 x 1 x 1 it
+// computes the same contributions as pe_element<1> (sums in another order, in FP64).
+template <bool ELL>
+__device__ double pe_element_sampled(const DevGeom& g, const BlockSmem& bs, WarpSmem& ws, int d, long long v,
+                                     float cr, float sr, int lane, const Sampling& sm)
+{
+    const int n_sub = sm.nx * sm.ny * sm.nz, nxy = sm.nx * sm.ny;
+    const int n_pts = sm.sx * sm.sy * sm.sz;
+    const float fx = (float)sm.nx, fy = (float)sm.ny, fz = (float)sm.nz;
+    double dacc = 0.0;
+    long long unused = 0;
+    for (int p = 0; p < n_pts; ++p) {
+        const int jx = p % sm.sx, jy = (p / sm.sx) % sm.sy, jz = p / (sm.sx * sm.sy);
+        __syncwarp();                     // the previous point's lists are no longer read
+        Elem e;
+        if (!init_element(g, ws, d, v, cr, sr, lane, e, ((float)jx + 0.5f) / (float)sm.sx,
+                          ((float)jy + 0.5f) / (float)sm.sy, ((float)jz + 0.5f) / (float)sm.sz))
+            return 0.0;                   // the crystal's mu does not depend on the point
+        KeptList kl = start_kept_list(g, bs, ws, e, d, lane);
+        for (int base = 0; base < n_sub; base += 32) {
+            const int sidx = min(base + lane, n_sub - 1);
+            const int iz = sidx / nxy, rem = sidx - iz * nxy;
+            const int iy = rem / sm.nx, ix = rem - iy * sm.nx;
+            const SubElem q = sub_element_at(e, ix, iy, iz, fx, fy, fz);
+            Walk s{0.0f, 0.0f, 0, 0, 0, 0, 0};
+            const bool skip = walk_sub_element<false, ELL>(g, bs, ws, e, d, q, base + lane >= n_sub, base == 0,
+                                                           kl, lane, s, unused);
+            if (!skip) dacc += (double)finish_sub_element_at(e, q, s.att, fx, fy, fz);
+        }
+    }
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) dacc += __shfl_xor_sync(0xffffffffu, dacc, off);
+    return dacc / (double)n_pts;
 }
 
 // Block superset of the reference cone test over all voxels within radius rho of
@@ -752,11 +831,13 @@ struct BrickOut {
 // One work item: crystal det_begin + di against one voxel brick of bx x by x bz voxels (brick
 // (gx, gy, gz) of the block's grid starting at z-plane iz0).  The block builds the cone
 // superset of the brick, then its warps take the brick's voxels in turn.
-template <int MODE, bool COUNT, bool ELL = false>
+// SAMPLED: elements of the sampled form `smp` (source points anywhere in the voxels: the
+// superset radius grows by half a voxel diagonal).
+template <int MODE, bool COUNT, bool ELL = false, bool SAMPLED = false>
 __device__ __forceinline__ void pe_brick(const DevGeom& g, BlockSmem& bs, WarpSmem& ws, int lane, int wid,
                                          const BrickOut& O, int di, int gx, int gy, int gz, int iz0, int iz1,
                                          int bx, int by, int bz, float cr, float sr,
-                                         unsigned long long* counters)
+                                         unsigned long long* counters, const Sampling* smp = nullptr)
 {
     const int x0 = gx * bx, y0 = gy * by, z0 = iz0 + gz * bz;
     const int x1 = min(x0 + bx, g.nx) - 1, y1 = min(y0 + by, g.ny) - 1, z1 = min(z0 + bz, iz1 + 1) - 1;
@@ -766,8 +847,9 @@ __device__ __forceinline__ void pe_brick(const DevGeom& g, BlockSmem& bs, WarpSm
     voxel_centre(g, x0 + g.nx * ((long long)y0 + g.ny * z0), 1.0f, 0.0f, ax, ay, az);
     voxel_centre(g, x1 + g.nx * ((long long)y1 + g.ny * z1), 1.0f, 0.0f, bxx, byy, bzz);
     const float mx = 0.5f * (ax + bxx), my = 0.5f * (ay + byy), mz = 0.5f * (az + bzz);
-    const float rho = 0.5f * sqrtf((bxx - ax) * (bxx - ax) + (byy - ay) * (byy - ay) +
-                                   (bzz - az) * (bzz - az)) + 1e-3f;
+    float rho = 0.5f * sqrtf((bxx - ax) * (bxx - ax) + (byy - ay) * (byy - ay) +
+                             (bzz - az) * (bzz - az)) + 1e-3f;
+    if constexpr (SAMPLED) rho += 0.5f * sqrtf(g.wx * g.wx + g.wy * g.wy + g.wz * g.wz);
     build_superset(g, bs, d, mx * cr - my * sr, mx * sr + my * cr, mz, rho);
     const int n_slots = bx * by * bz;
     for (int slot = wid; slot < n_slots; slot += kWarps) {
@@ -776,14 +858,16 @@ __device__ __forceinline__ void pe_brick(const DevGeom& g, BlockSmem& bs, WarpSm
         if (ix >= g.nx || iy >= g.ny || iz > z1) continue;
         const long long v = ix + g.nx * ((long long)iy + (long long)g.ny * iz);
         if (v < O.vox_begin || v > O.vlast) continue;
-        const float val = (float)pe_element<MODE, COUNT, ELL>(g, bs, ws, d, v, cr, sr, lane, counters);
+        float val;
+        if constexpr (SAMPLED) val = (float)pe_element_sampled<ELL>(g, bs, ws, d, v, cr, sr, lane, *smp);
+        else val = (float)pe_element<MODE, COUNT, ELL>(g, bs, ws, d, v, cr, sr, lane, counters);
         if (lane == 0) O.out[(long long)di * O.ld + (v - O.vox_begin)] = val;
         __syncwarp();
     }
     __syncthreads();
 }
 
-template <int MODE, bool COUNT, bool ELL>
+template <int MODE, bool COUNT, bool ELL, bool SAMPLED = false>
 __global__ void __launch_bounds__(kThreads, 2) pe_kernel(DevGeom g, PeLaunch L)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -812,8 +896,8 @@ __global__ void __launch_bounds__(kThreads, 2) pe_kernel(DevGeom g, PeLaunch L)
         const int gz = (int)(b / ((long long)nbx * nby));
         const int rem = (int)(b - (long long)gz * nbx * nby);
         const int gy = rem / nbx, gx = rem - gy * nbx;
-        pe_brick<MODE, COUNT, ELL>(g, bs, ws, lane, wid, O, di, gx, gy, gz, iz0, iz1, bx, by, bz, cr, sr,
-                                   L.counters);
+        pe_brick<MODE, COUNT, ELL, SAMPLED>(g, bs, ws, lane, wid, O, di, gx, gy, gz, iz0, iz1, bx, by, bz, cr, sr,
+                                            L.counters, &L.smp);
     }
 }
 
@@ -880,7 +964,7 @@ __global__ void __launch_bounds__(kThreads, 2) pe_batch_kernel(BatchLaunch B)
 
 }  // namespace
 
-template <int MODE, bool COUNT, bool ELL>
+template <int MODE, bool COUNT, bool ELL, bool SAMPLED = false>
 static int launch_mode(const DevGeom& g, const PeLaunch& L, int num_sms, cudaStream_t stream)
 {
     const int smem = (int)sizeof(BlockSmem);
@@ -889,15 +973,16 @@ static int launch_mode(const DevGeom& g, const PeLaunch& L, int num_sms, cudaStr
     if (cudaGetDevice(&dev) != cudaSuccess) return -1;
     const unsigned long long bit = 1ull << (dev & 63);
     if (!(__atomic_load_n(&configured, __ATOMIC_ACQUIRE) & bit)) {
-        if (cudaFuncSetAttribute(pe_kernel<MODE, COUNT, ELL>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem) !=
+        if (cudaFuncSetAttribute(pe_kernel<MODE, COUNT, ELL, SAMPLED>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 smem) !=
             cudaSuccess)
             return -1;
         __atomic_fetch_or(&configured, bit, __ATOMIC_RELEASE);
     }
     int per_sm = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, pe_kernel<MODE, COUNT, ELL>, kThreads, smem);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, pe_kernel<MODE, COUNT, ELL, SAMPLED>, kThreads, smem);
     if (per_sm < 1) per_sm = 1;
-    pe_kernel<MODE, COUNT, ELL><<<num_sms * per_sm, kThreads, smem, stream>>>(g, L);
+    pe_kernel<MODE, COUNT, ELL, SAMPLED><<<num_sms * per_sm, kThreads, smem, stream>>>(g, L);
     return cudaGetLastError() == cudaSuccess ? 0 : -1;
 }
 
@@ -975,6 +1060,12 @@ int launch_pe(const DevGeom& g, const PeLaunch& L, int mode, int num_sms, cudaSt
     if (L.counters) return launch_mode<0, true, false>(g, L, num_sms, stream);
     return mode == 0 ? launch_mode<0, false, false>(g, L, num_sms, stream)
                      : launch_mode<1, false, false>(g, L, num_sms, stream);
+}
+
+int launch_pe_sampled(const DevGeom& g, const PeLaunch& L, int num_sms, cudaStream_t stream)
+{
+    if (g.hole_shape) return launch_mode<1, false, true, true>(g, L, num_sms, stream);
+    return launch_mode<1, false, false, true>(g, L, num_sms, stream);
 }
 
 }  // namespace sysmat

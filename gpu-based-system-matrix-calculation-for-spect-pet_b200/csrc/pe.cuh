@@ -15,6 +15,14 @@ constexpr int kPeEffHoles = 192;
 // Bits of the device status word.
 constexpr int kStatusCapacity = 1;
 
+// Sampled form of the photoelectric element (no reference counterpart): crystal sub-elements
+// along x, depth and z, and source points per voxel along x, y and z.  The reference fixes
+// 8 x 16 x 8 and 1 x 1 x 1 (PESysMatGen.cu:1196-1217, :1031-1034).
+struct Sampling {
+    int nx = 8, ny = 16, nz = 8;
+    int sx = 1, sy = 1, sz = 1;
+};
+
 struct PeLaunch {
     int det_begin, det_count;
     long long vox_begin, vox_count;
@@ -27,6 +35,7 @@ struct PeLaunch {
     // [1] non-zero hole chords, [2] non-zero crystal chords, [3] elements, [4] plate-blocked
     // sub-elements, [5] cone-test candidates (holes + crystals)
     unsigned long long* counters;
+    Sampling smp;                          // read by the sampled instance only
 };
 
 // One (geometry, rotation, detector x voxel block) task of a batched launch.  The host fills
@@ -67,6 +76,8 @@ struct AdjLaunch {
 };
 
 int launch_pe(const DevGeom& g, const PeLaunch& L, int mode, int num_sms, cudaStream_t stream);
+// The sampled form (L.smp), accumulated in FP64.
+int launch_pe_sampled(const DevGeom& g, const PeLaunch& L, int num_sms, cudaStream_t stream);
 // kind 0: projection, kind 1: vector-Jacobian product, kind 2: back projection.
 int launch_pe_adjoint(const DevGeom& g, const AdjLaunch& L, int kind, int num_sms, cudaStream_t stream);
 // Sets the batched kernel's shared-memory attribute on the current device (once) and returns

@@ -107,6 +107,23 @@ SYSMAT_API int sysmat_dims(const sysmat_ctx* ctx, int* n_det, long long* n_vox, 
 SYSMAT_API int sysmat_pe(sysmat_ctx* ctx, float rotation, int det_begin, int det_count, long long vox_begin,
               long long vox_count, float* d_out, long long ld, int mode, void* stream);
 
+/* Photoelectric block in the sampled form.  No reference counterpart: the reference divides
+ * every crystal into 8 x 16 x 8 sub-elements and uses one source point, the voxel centre
+ * (PESysMatGen.cu:1196-1217, :1031-1034).  crystal_div[3]: sub-elements along x, depth (y)
+ * and z (each 1..SYSMAT_SAMPLED_MAX_DIV, product <= SYSMAT_SAMPLED_MAX_SUBELEMENTS);
+ * voxel_sub[3]: source points along x, y and z on the centres of a grid over the voxel (each
+ * 1..SYSMAT_SAMPLED_MAX_SUB, product <= SYSMAT_SAMPLED_MAX_POINTS).  The element is the mean
+ * over the source points of the reference's element at that point with that division, every
+ * sub-element contribution summed in FP64; {8,16,8} with {1,1,1} is SYSMAT_MODE_PRECISE's
+ * sysmat_pe up to the order of the FP64 sum.  Blocks, strides and errors as sysmat_pe. */
+#define SYSMAT_SAMPLED_MAX_DIV 64
+#define SYSMAT_SAMPLED_MAX_SUBELEMENTS 4096
+#define SYSMAT_SAMPLED_MAX_SUB 8
+#define SYSMAT_SAMPLED_MAX_POINTS 64
+SYSMAT_API int sysmat_pe_sampled(sysmat_ctx* ctx, float rotation, int det_begin, int det_count,
+                                 long long vox_begin, long long vox_count, const int* crystal_div,
+                                 const int* voxel_sub, float* d_out, long long ld, void* stream);
+
 /* Relationship bitmaps in the reference's word layout (scatter.cu:1040-1074).
  * Word counts: crystal ceil(D(D+1)/2*D/32), collimator ceil(H0*D*D/32). */
 SYSMAT_API long long sysmat_bitmap_crystal_words(const sysmat_ctx* ctx);

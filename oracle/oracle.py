@@ -49,6 +49,9 @@ def lib():
         L.oracle_pe_shapes.argtypes = [_fp, _fp, _fp, _fp, ctypes.c_int, _ip, ctypes.c_int, ctypes.c_longlong,
                                        ctypes.c_longlong, _dp, _i64p, ctypes.c_int]
         L.oracle_pe_shapes.restype = ctypes.c_int
+        L.oracle_pe_sampled.argtypes = [_fp, _fp, _fp, _fp, _ip, _ip, ctypes.c_int, _ip, ctypes.c_int,
+                                        ctypes.c_longlong, ctypes.c_longlong, _dp, ctypes.c_int]
+        L.oracle_pe_sampled.restype = ctypes.c_int
         for name in ("oracle_box_chord", "oracle_box_chord_inside", "oracle_cyl_chord", "oracle_ell_chord"):
             getattr(L, name).argtypes = [ctypes.c_int, _dp]
             getattr(L, name).restype = ctypes.c_double
@@ -95,6 +98,26 @@ def pe(geo, prec=64, dets=None, v0=0, nv=None, threads=0, counts=False, shapes=N
     if rc:
         raise RuntimeError(f"oracle_pe failed ({rc})")
     return (out, cnt) if counts else out
+
+
+def pe_sampled(geo, crystal_div, voxel_sub, prec=64, dets=None, v0=0, nv=None, threads=0, shapes=None):
+    """PE elements of the sampled form (len(dets), nv) as float64: crystal_div sub-elements of
+    each crystal along x, depth, z and voxel_sub source points per voxel along x, y, z, the
+    element being the mean over the source points (see oracle_pe_sampled).  shapes as for pe()."""
+    nv = geo.n_vox - v0 if nv is None else nv
+    c, pc = _f32(geo.collimator)
+    d, pd = _f32(geo.detector)
+    i, pi = _f32(geo.image)
+    dd, pdd = _dets(geo, dets)
+    dv = np.ascontiguousarray(np.asarray(crystal_div, dtype=np.int32).reshape(3))
+    sv = np.ascontiguousarray(np.asarray(voxel_sub, dtype=np.int32).reshape(3))
+    out = np.zeros((dd.size, nv), dtype=np.float64)
+    sh, psh = _f32(np.asarray(shapes, dtype=np.float32).reshape(-1)) if shapes is not None else (None, None)
+    rc = lib().oracle_pe_sampled(pc, pd, pi, psh, dv.ctypes.data_as(_ip), sv.ctypes.data_as(_ip), prec, pdd, dd.size,
+                                 v0, nv, out.ctypes.data_as(_dp), threads)
+    if rc:
+        raise RuntimeError(f"oracle_pe_sampled failed ({rc})")
+    return out
 
 
 def ell_chord(args, prec=64):

@@ -219,8 +219,10 @@ typedef struct {
     REAL x, y, z;
 } FN(vec3);
 
-/* Voxel centre of flat index v, rotated about z by I[20]*I[7] (PESysMatGen.cu:1031-1052). */
-static void FN(voxel_centre)(const ogeo* g, long long v, REAL* xo, REAL* yo, REAL* zo)
+/* Point of voxel v at fractions (fx, fy, fz) of its extent, rotated about z by I[20]*I[7]
+ * (PESysMatGen.cu:1031-1052, where the fractions are 1/2: the voxel centre). */
+static void FN(voxel_point)(const ogeo* g, long long v, REAL fx, REAL fy, REAL fz, REAL* xo, REAL* yo,
+                            REAL* zo)
 {
     const float* I = g->I;
     long long nxy = (long long)g->nx * g->ny;
@@ -229,15 +231,20 @@ static void FN(voxel_centre)(const ogeo* g, long long v, REAL* xo, REAL* yo, REA
     int iy = (int)(r / g->nx);
     int ix = (int)(r % g->nx);
     REAL ang = (REAL)I[20] * (REAL)I[7];
-    REAL x = ((REAL)ix - (REAL)g->nx / (REAL)2.0f + (REAL)0.5f) * (REAL)I[3];
-    REAL y = ((REAL)iy - (REAL)g->ny / (REAL)2.0f + (REAL)0.5f) * (REAL)I[4];
-    REAL z = ((REAL)iz - (REAL)g->nz / (REAL)2.0f + (REAL)0.5f) * (REAL)I[5];
+    REAL x = ((REAL)ix - (REAL)g->nx / (REAL)2.0f + fx) * (REAL)I[3];
+    REAL y = ((REAL)iy - (REAL)g->ny / (REAL)2.0f + fy) * (REAL)I[4];
+    REAL z = ((REAL)iz - (REAL)g->nz / (REAL)2.0f + fz) * (REAL)I[5];
     x = x + (REAL)I[8];
     y = y + (REAL)I[9];
     z = z + (REAL)I[10];
     *xo = x * COS(ang) - y * SIN(ang);
     *yo = x * SIN(ang) + y * COS(ang);
     *zo = z;
+}
+
+static void FN(voxel_centre)(const ogeo* g, long long v, REAL* xo, REAL* yo, REAL* zo)
+{
+    FN(voxel_point)(g, v, (REAL)0.5f, (REAL)0.5f, (REAL)0.5f, xo, yo, zo);
 }
 
 typedef struct {
@@ -273,15 +280,15 @@ static inline void FN(to_frame)(const FN(crystal)* c, REAL x, REAL y, REAL z,
 }
 
 /* ---------------------------------------------------------------------------------- */
-/* Photoelectric matrix element A[d][v] (PESysMatGen.cu:951-1364).                      */
+/* Photoelectric matrix element A[d][v] (PESysMatGen.cu:951-1364) for a source at
+ * (xI, yI, zI), with g->div[0..2] sub-elements of crystal d along x, depth and z (the
+ * reference's 8 x 16 x 8).                                                              */
 
-static REAL FN(pe_element)(const ogeo* g, int d, long long v, int* cand_c, int* cand_h,
-                           int* ncand_h, pe_counts* cnt)
+static REAL FN(pe_element_at)(const ogeo* g, int d, REAL xI, REAL yI, REAL zI, int* cand_c, int* cand_h,
+                              int* ncand_h, pe_counts* cnt)
 {
     const float* C = g->C;
     const REAL fov = (REAL)g->I[11];
-    REAL xI, yI, zI;
-    FN(voxel_centre)(g, v, &xI, &yI, &zI);
     FN(crystal) cd;
     FN(load_crystal)(g, d, &cd);
     REAL xIs, yIs, zIs;
@@ -330,7 +337,7 @@ static REAL FN(pe_element)(const ogeo* g, int d, long long v, int* cand_c, int* 
     if (cnt) { cnt->cand_crystals = nc; cnt->cand_holes = hoff; }
 
     /* ---- sub-element loop, order z, x, y (:1196-1362) ---- */
-    const unsigned NXS = 8, NYS = 16, NZS = 8;
+    const unsigned NXS = (unsigned)g->div[0], NYS = (unsigned)g->div[1], NZS = (unsigned)g->div[2];
     const REAL cr = COS(cd.rot), sr = SIN(cd.rot);
     REAL sum = 0;
     for (unsigned iz = 0; iz < NZS; ++iz)
@@ -426,6 +433,29 @@ static REAL FN(pe_element)(const ogeo* g, int d, long long v, int* cand_c, int* 
         sum = sum + eff * sa * absf;
     }
     return sum;
+}
+
+/* Element of voxel v: the reference's voxel-centre source when g->vsub is 1 x 1 x 1, else
+ * the mean over the centres of a vsub[0] x vsub[1] x vsub[2] grid of source points over the
+ * voxel (an extension: the reference has one source point per voxel), summed in double. */
+static REAL FN(pe_element)(const ogeo* g, int d, long long v, int* cand_c, int* cand_h,
+                           int* ncand_h, pe_counts* cnt)
+{
+    const int sx = g->vsub[0], sy = g->vsub[1], sz = g->vsub[2];
+    REAL xI, yI, zI;
+    if (sx == 1 && sy == 1 && sz == 1) {
+        FN(voxel_centre)(g, v, &xI, &yI, &zI);
+        return FN(pe_element_at)(g, d, xI, yI, zI, cand_c, cand_h, ncand_h, cnt);
+    }
+    double acc = 0.0;
+    for (int jz = 0; jz < sz; ++jz)
+    for (int jy = 0; jy < sy; ++jy)
+    for (int jx = 0; jx < sx; ++jx) {
+        FN(voxel_point)(g, v, ((REAL)jx + (REAL)0.5f) / (REAL)sx, ((REAL)jy + (REAL)0.5f) / (REAL)sy,
+                        ((REAL)jz + (REAL)0.5f) / (REAL)sz, &xI, &yI, &zI);
+        acc += (double)FN(pe_element_at)(g, d, xI, yI, zI, cand_c, cand_h, ncand_h, cnt);
+    }
+    return (REAL)(acc / (double)(sx * sy * sz));
 }
 
 /* ---------------------------------------------------------------------------------- */

@@ -31,6 +31,8 @@ typedef struct {
     const float *C, *D, *I, *P;
     const float* S;    /* optional hole shapes: rho_x, rho_z, theta per hole (rho_x <= 0: circle) */
     int L, ncry, nx, ny, nz, nh0, nholes;
+    int div[3];        /* PE crystal sub-elements along x, depth, z (reference: 8, 16, 8) */
+    int vsub[3];       /* PE source points per voxel along x, y, z (reference: 1, 1, 1) */
     long long nvox;
     int nh[MAX_LAYERS];
 } ogeo;
@@ -94,18 +96,18 @@ static int parse(ogeo* g, const float* C, const float* D, const float* I, const 
         g->nholes += g->nh[m];
     }
     g->nh0 = C ? (int)floorf(C[10] + 0.000001f) : 0;
+    g->div[0] = 8; g->div[1] = 16; g->div[2] = 8;
+    g->vsub[0] = g->vsub[1] = g->vsub[2] = 1;
     return 0;
 }
 
 /* PE elements for detectors dets[0..ndet) and voxels [v0, v0+nv), row-major into out
  * (ndet x nv).  prec: 32 or 64.  counts (optional, ndet*nv*5 int64) receives the
  * instrumented work counts per element. */
-int oracle_pe_shapes(const float* C, const float* D, const float* I, const float* S, int prec, const int* dets,
-                     int ndet, long long v0, long long nv, double* out, long long* counts, int nthreads)
+static int run_pe(const ogeo* gp, int prec, const int* dets, int ndet, long long v0, long long nv, double* out,
+                  long long* counts, int nthreads)
 {
-    ogeo g;
-    if (parse(&g, C, D, I, NULL)) return -1;
-    g.S = S;
+    const ogeo g = *gp;
     if (nthreads > 0) omp_set_num_threads(nthreads);
     long long total = (long long)ndet * nv;
     int err = 0;
@@ -137,6 +139,33 @@ int oracle_pe_shapes(const float* C, const float* D, const float* I, const float
         free(ch);
     }
     return err ? -2 : 0;
+}
+
+int oracle_pe_shapes(const float* C, const float* D, const float* I, const float* S, int prec, const int* dets,
+                     int ndet, long long v0, long long nv, double* out, long long* counts, int nthreads)
+{
+    ogeo g;
+    if (parse(&g, C, D, I, NULL)) return -1;
+    g.S = S;
+    return run_pe(&g, prec, dets, ndet, v0, nv, out, counts, nthreads);
+}
+
+/* PE elements of the sampled form: div[3] crystal sub-elements along x, depth, z and vsub[3]
+ * source points per voxel along x, y, z (the reference: 8 x 16 x 8 and 1 x 1 x 1).  S: optional
+ * hole shapes as for oracle_pe_shapes. */
+int oracle_pe_sampled(const float* C, const float* D, const float* I, const float* S, const int* div,
+                      const int* vsub, int prec, const int* dets, int ndet, long long v0, long long nv, double* out,
+                      int nthreads)
+{
+    ogeo g;
+    if (parse(&g, C, D, I, NULL)) return -1;
+    g.S = S;
+    for (int k = 0; k < 3; ++k) {
+        if (div[k] < 1 || vsub[k] < 1) return -1;
+        g.div[k] = div[k];
+        g.vsub[k] = vsub[k];
+    }
+    return run_pe(&g, prec, dets, ndet, v0, nv, out, NULL, nthreads);
 }
 
 int oracle_pe(const float* C, const float* D, const float* I, int prec, const int* dets, int ndet,

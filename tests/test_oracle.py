@@ -259,3 +259,47 @@ def test_native_collimator_scatter_only_adds_attenuation_on_one_layer():
     assert comb.max() > 0 and nat.max() > 0
     assert np.all(nat <= comb * (1 + 1e-12) + 1e-30)
     assert nat.sum() < 0.99 * comb.sum()
+
+
+# ---- sampled photoelectric form (no reference counterpart) ----------------------------
+
+@pytest.mark.parametrize("prec", [32, 64])
+def test_sampled_form_with_reference_sampling_is_the_restatement(prec):
+    geo = geometry.mini(seed=71, rotated=True, layers=2, n_rot=8, nvox=(6, 5, 3), ncry=(5, 4)).with_rotation(3)
+    a = oracle.pe(geo, prec=prec)
+    b = oracle.pe_sampled(geo, (8, 16, 8), (1, 1, 1), prec=prec)
+    assert np.array_equal(a, b)
+
+
+def test_sampled_source_points_are_shifted_voxel_centres():
+    """In FP64, source point (jx, jz) of a 2 x 1 x 2 grid is the voxel centre of the image
+    shifted by (jx - 1/2, jz - 1/2) quarter voxels; the sampled element is their mean."""
+    geo = geometry.config1()
+    dets = [3, 77, 200]
+    v0, nv = 32 * 9, 96
+    got = oracle.pe_sampled(geo, (4, 4, 4), (2, 1, 2), prec=64, dets=dets, v0=v0, nv=nv)
+    acc = np.zeros_like(got)
+    for fx in (-0.25, 0.25):
+        for fz in (-0.25, 0.25):
+            img = geo.image.copy()
+            img[8] += np.float32(fx * img[3])
+            img[10] += np.float32(fz * img[5])
+            g = geometry.Geometry(geo.name, geo.collimator, geo.detector, img, geo.physics)
+            acc += oracle.pe_sampled(g, (4, 4, 4), (1, 1, 1), prec=64, dets=dets, v0=v0, nv=nv)
+    acc /= 4.0
+    assert got.max() > 0
+    r = rel_err(got, acc)
+    assert np.median(r) < 1e-12 and r.max() < 1e-6, (np.median(r), r.max())
+
+
+def test_sampled_form_converges_with_the_division():
+    """Finer divisions approach one limit: the 16 x 32 x 16 matrix is closer to 32 x 64 x 32 than
+    the reference's 8 x 16 x 8 is (the largest-face solid angle of each sub-element converges
+    to the solid angle of its surface element)."""
+    geo = geometry.config1()
+    dets, v0, nv = [40, 120], 32 * 12, 64
+    m = [oracle.pe_sampled(geo, d, (1, 1, 1), prec=64, dets=dets, v0=v0, nv=nv)
+         for d in ((8, 16, 8), (16, 32, 16), (32, 64, 32))]
+    e8 = np.abs(m[0] - m[2]).sum()
+    e16 = np.abs(m[1] - m[2]).sum()
+    assert e16 < 0.6 * e8, (e8, e16)
