@@ -31,6 +31,7 @@ def _load(name, path):
 
 sysmat = _load("sysmat_binding", os.path.join(HERE, "sysmat.py"))
 geometry = _load("sysmat_geometry", os.path.join(HERE, "geometry.py"))
+sharding = _load("sysmat_sharding", os.path.join(HERE, "sharding.py"))
 
 
 class Projector:
@@ -67,6 +68,46 @@ class Projector:
                                        det_count=self.det_count)
 
 
+class ShardedProjector:
+    """A projector whose detector rows are split across the ranks of a process group
+    (sharding.detector_slab), one GPU per rank.  Each rank recomputes only its own rows of A.
+    Projections stay local (a rank's rows of A x); the products that sum over detector rows
+    are completed with one all-reduce each: the back projection (n_vox values) and the theta
+    gradient with u^T A x (8 values).  Every rank then holds the same totals, so an MLEM loop
+    or a calibration step proceeds identically on all ranks.
+
+    `local` builds the rank's own projector (default: Projector on this rank's rows); any
+    object with project / backproject / vjp over rows det_begin .. det_begin + det_count
+    will do."""
+
+    def __init__(self, geo, group=None, rotation=0.0, device=None, local=None):
+        import torch.distributed as dist
+        self.dist = dist
+        self.group = group
+        self.rank = dist.get_rank(group)
+        self.world = dist.get_world_size(group)
+        self.geo = geo
+        self.det_begin, self.det_count = sharding.detector_slab(geo.n_det, self.rank, self.world)
+        if local is None:
+            dev = torch.cuda.current_device() if device is None else device
+            local = Projector(geo, device=dev, rotation=rotation, det_begin=self.det_begin,
+                              det_count=self.det_count)
+        self.local = local
+
+    def _sum(self, t):
+        self.dist.all_reduce(t, op=self.dist.ReduceOp.SUM, group=self.group)
+        return t
+
+    def project(self, x, theta=None):
+        return self.local.project(x, theta)
+
+    def backproject(self, u, theta=None):
+        return self._sum(self.local.backproject(u, theta))
+
+    def vjp(self, x, u, theta=None):
+        return self._sum(self.local.vjp(x, u, theta))
+
+
 class Projection(torch.autograd.Function):
     """p = A(theta) x.  theta: CPU float64 tensor of 7; x: CUDA float32 tensor of n_vox;
     p: CUDA float64 tensor of the projector's detector rows.  Backward gives d/d theta through
@@ -100,7 +141,8 @@ def project(theta, x, projector):
 
 def mlem(projector, y, n_iter, x0=None, theta=None):
     """MLEM reconstruction x <- x / (A^T 1) * A^T (y / A x) with the on-the-fly projector.
-    y: CUDA tensor of the projector's detector rows; returns a float32 CUDA tensor of n_vox."""
+    y: CUDA tensor of the projector's detector rows; returns a float32 CUDA tensor of n_vox.
+    With a ShardedProjector, y holds this rank's rows and every rank returns the same x."""
     dev = y.device
     sens = projector.backproject(torch.ones(projector.det_count, dtype=torch.float32, device=dev), theta)
     x = torch.ones(projector.geo.n_vox, dtype=torch.float32, device=dev) if x0 is None else x0.clone()
