@@ -224,8 +224,7 @@ extern "C" SYSMAT_API int sysmat_set_hole_shapes(sysmat_ctx* ctx, const float* r
 {
     if (!ctx || !same_device(ctx)) return SYSMAT_ERR_ARG;
     if (!rho_x) {                                   // back to circular holes
-        cudaFree(ctx->d_shapes);
-        ctx->d_shapes = nullptr;
+        // the table stays allocated until sysmat_destroy: batch plans copy its pointer
         ctx->g.hole_shape = nullptr;
         return SYSMAT_OK;
     }

@@ -31,6 +31,7 @@ struct sysmat_batch_plan {
     int device = -1;
     int num_sms = 0;
     std::vector<DevGeom> geoms;            // one per context, as the contexts hold them
+    bool ell = false;                      // some context has elliptical holes
     std::vector<sysmat_batch_item> items;  // non-empty items, in the caller's order
     int bx = 4, by = 4, bz = 2, blocks_per_sm = 0;   // 0: as many as fit
     DevGeom* d_geoms = nullptr;
@@ -103,7 +104,7 @@ int upload_tasks(sysmat_batch_plan* p, const std::vector<sysmat_batch_item>& ite
 int grid_of(const sysmat_batch_plan* p, int mode, int* grid)
 {
     int per_sm = 0;
-    if (configure_pe_batch(mode, &per_sm)) return SYSMAT_ERR_CUDA;
+    if (configure_pe_batch(mode, p->ell, &per_sm)) return SYSMAT_ERR_CUDA;
     if (p->blocks_per_sm > 0 && p->blocks_per_sm < per_sm) per_sm = p->blocks_per_sm;
     *grid = p->num_sms * per_sm;
     return SYSMAT_OK;
@@ -116,7 +117,7 @@ int launch_direct(sysmat_batch_plan* p, int mode, cudaStream_t s)
     int rc = grid_of(p, mode, &grid);
     if (rc) return rc;
     BATCH_TRY(cudaMemsetAsync(p->d_counter, 0, sizeof(unsigned long long), s));
-    return launch_pe_batch(p->launch, mode, grid, s) ? SYSMAT_ERR_CUDA : SYSMAT_OK;
+    return launch_pe_batch(p->launch, mode, p->ell, grid, s) ? SYSMAT_ERR_CUDA : SYSMAT_OK;
 }
 
 }  // namespace
@@ -127,13 +128,16 @@ extern "C" SYSMAT_API int sysmat_batch_create(sysmat_batch_plan** out, sysmat_ct
     if (!out || !ctxs || n_ctx < 1 || n_items < 0 || (n_items > 0 && !items)) return SYSMAT_ERR_ARG;
     *out = nullptr;
     const int device = ctxs[0] ? ctxs[0]->device : -1;
-    for (int c = 0; c < n_ctx; ++c)   // elliptical holes are not supported by the batched kernel
-        if (!ctxs[c] || ctxs[c]->device != device || ctxs[c]->g.hole_shape) return SYSMAT_ERR_ARG;
+    for (int c = 0; c < n_ctx; ++c)
+        if (!ctxs[c] || ctxs[c]->device != device) return SYSMAT_ERR_ARG;
     if (!device_is(device)) return SYSMAT_ERR_ARG;
     auto* p = new sysmat_batch_plan();
     p->device = device;
     p->num_sms = ctxs[0]->num_sms;
-    for (int c = 0; c < n_ctx; ++c) p->geoms.push_back(ctxs[c]->g);
+    for (int c = 0; c < n_ctx; ++c) {
+        p->geoms.push_back(ctxs[c]->g);
+        p->ell = p->ell || ctxs[c]->g.hole_shape != nullptr;
+    }
     for (int i = 0; i < n_items; ++i) {
         const sysmat_batch_item& it = items[i];
         if (it.ctx < 0 || it.ctx >= n_ctx ||
@@ -210,7 +214,7 @@ extern "C" SYSMAT_API int sysmat_batch_run(sysmat_batch_plan* p, int mode, void*
         cudaGraph_t graph = nullptr;
         BATCH_TRY(cudaStreamBeginCapture(p->capture, cudaStreamCaptureModeThreadLocal));
         const bool ok = cudaMemsetAsync(p->d_counter, 0, sizeof(unsigned long long), p->capture) == cudaSuccess &&
-                        launch_pe_batch(p->launch, mode, grid, p->capture) == 0;
+                        launch_pe_batch(p->launch, mode, p->ell, grid, p->capture) == 0;
         const cudaError_t end = cudaStreamEndCapture(p->capture, &graph);
         if (!ok || end != cudaSuccess || !graph) {
             if (graph) cudaGraphDestroy(graph);

@@ -605,7 +605,8 @@ __device__ __forceinline__ KeptList start_kept_list(const DevGeom& g, const Bloc
 // the kept objects that meet the round's slope box, walked in round buffers (an overfull
 // round in pieces: each lane's walk state carries over, so the attenuation order is kept).
 // Returns whether the lane skips the sub-element: `dead`, or blocked with every mu >= 0 (the
-// contribution is then exactly 0).
+// contribution is then exactly 0).  Used by the sampled form; pe_element keeps the same walk
+// inline (through this helper the reference-order kernel measured 1.5 % slower).
 template <bool COUNT, bool ELL>
 __device__ __forceinline__ bool walk_sub_element(const DevGeom& g, const BlockSmem& bs, WarpSmem& ws,
                                                  const Elem& e, int d, const SubElem& q, bool dead,
@@ -658,7 +659,11 @@ __device__ double pe_element(const DevGeom& g, const BlockSmem& bs, WarpSmem& ws
 {
     Elem e;
     if (!init_element(g, ws, d, v, cr, sr, lane, e)) return 0.0;
-    KeptList kl = start_kept_list(g, bs, ws, e, d, lane);
+    const bool from_super = bs.s_count >= 0;
+    const int n_src = from_super ? bs.s_count : g.n_holes + g.n_det;
+    int count = 0;
+    int cursor = build_chunk(g, bs, ws, e, d, 0, n_src, from_super, lane, &count);
+    const bool single = cursor >= n_src;
 
     float chain = 0.0f;
     double dacc = 0.0;
@@ -672,9 +677,49 @@ __device__ double pe_element(const DevGeom& g, const BlockSmem& bs, WarpSmem& ws
                          (lane & 1);
         const SubElem q = sub_element(e, sidx);
         Walk s{0.0f, 0.0f, 0, 0, 0, 0, 0};
-        const bool skip = walk_sub_element<COUNT, ELL>(g, bs, ws, e, d, q, false, r == 0, kl, lane, s,
-                                                       n_sub_entries);
-        const float contrib = skip ? 0.0f : finish_sub_element(e, q, s.att);
+        RayCyl rc;
+        ray_cyl_init(rc, e.xI, e.yI, e.zI, q.xD, q.yD, q.zD);
+        const bool blocked = plate_penalty(g, ws, e, q, s.att);
+        const bool skip = blocked && g.nonneg_mu;
+        // slope box of the rays that still need the walk in this round
+        float4 box = make_float4(skip ? INFINITY : q.sa_a, skip ? -INFINITY : q.sa_a,
+                                 skip ? INFINITY : q.sa_b, skip ? -INFINITY : q.sa_b);
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1) {
+            box.x = fminf(box.x, __shfl_xor_sync(0xffffffffu, box.x, off));
+            box.y = fmaxf(box.y, __shfl_xor_sync(0xffffffffu, box.y, off));
+            box.z = fminf(box.z, __shfl_xor_sync(0xffffffffu, box.z, off));
+            box.w = fmaxf(box.w, __shfl_xor_sync(0xffffffffu, box.w, off));
+        }
+        // walk this round's objects: kept entries meeting the round box, copied with their
+        // geometry into the round buffer; an overfull round is walked in pieces (the walk
+        // state of each lane carries over, so the attenuation order is unchanged)
+        int cur = 0;
+        bool first_chunk = true;
+        while (true) {
+            if (!single && !first_chunk) {
+                cur = build_chunk(g, bs, ws, e, d, cur, n_src, from_super, lane, &count);
+            } else if (!single) {
+                if (r > 0) cur = build_chunk(g, bs, ws, e, d, 0, n_src, from_super, lane, &count);
+                else cur = cursor;
+            }
+            first_chunk = false;
+            int k = 0;
+            while (k < count) {
+                int next = count, nh = 0;
+                const int nr = fill_round<ELL>(g, ws, e, k, count, box, 0, lane, &next, &nh);
+                if constexpr (COUNT) n_sub_entries += nr;
+                if (!skip) walk_round<ELL>(g, ws, nh, nr, q.xD, q.yD, q.zD, q.sa_a, q.sa_b, q.cosang, rc, s);
+                __syncwarp();
+                k = next;
+            }
+            if (single || cur >= n_src) break;
+        }
+        float contrib = 0.0f;
+        if (!skip) {
+            if (s.lay < g.n_layers) close_layers(g, s, g.n_layers, q.cosang);
+            contrib = finish_sub_element(e, q, s.att);
+        }
         if constexpr (COUNT) {
             n_hole_hits += s.hole_hits;
             n_cry_hits += s.cry_hits;
@@ -709,8 +754,8 @@ __device__ double pe_element(const DevGeom& g, const BlockSmem& bs, WarpSmem& ws
             atomicAdd(&counters[2], (unsigned long long)n_cry_hits);
             atomicAdd(&counters[3], 1ull);
             atomicAdd(&counters[4], (unsigned long long)n_blocked);
-            atomicAdd(&counters[5], kl.single ? 0ull : 1ull);              // chunked elements
-            atomicAdd(&counters[6], (unsigned long long)kl.count);         // kept objects (last chunk)
+            atomicAdd(&counters[5], single ? 0ull : 1ull);                 // chunked elements
+            atomicAdd(&counters[6], (unsigned long long)count);            // kept objects (last chunk)
             atomicAdd(&counters[7], (unsigned long long)n_sub_entries);    // round sub-list entries
             atomicAdd(&counters[8], bs.s_count < 0 ? 1ull : 0ull);         // superset overflow
             atomicAdd(&counters[9], (unsigned long long)(bs.s_count < 0 ? 0 : bs.s_count));
@@ -732,7 +777,8 @@ __device__ double pe_element(const DevGeom& g, const BlockSmem& bs, WarpSmem& ws
 // sub-elements (x, depth, z), every contribution summed in FP64.  Each source point has its
 // own cone test and kept list; its sub-elements are taken 32 at a time in (z, depth, x) order,
 // x fastest, so a round is a compact patch of the crystal.  With 8 x 16 x 8 and 1 x 1 x 1 it
-// computes the same contributions as pe_element<1> (sums in another order, in FP64).
+// runs pe_element<1>'s float program, summed in another order (a separately compiled
+// instance: the compiler may contract the position expressions differently, in the last bit).
 template <bool ELL>
 __device__ double pe_element_sampled(const DevGeom& g, const BlockSmem& bs, WarpSmem& ws, int d, long long v,
                                      float cr, float sr, int lane, const Sampling& sm)
@@ -912,7 +958,7 @@ struct BatchSmem {
 // Batched launch: one persistent grid over the items of many (geometry, rotation, block)
 // tasks, taken from one work counter; a block finds its item's task by binary search over
 // the tasks' first item numbers.
-template <int MODE>
+template <int MODE, bool ELL>
 __global__ void __launch_bounds__(kThreads, 2) pe_batch_kernel(BatchLaunch B)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -955,8 +1001,8 @@ __global__ void __launch_bounds__(kThreads, 2) pe_batch_kernel(BatchLaunch B)
         const int rem = (int)(b - (long long)gz * T.nbx * T.nby);
         const int gy = rem / T.nbx, gx = rem - gy * T.nbx;
         const BrickOut O{T.out, T.ld, T.vox_begin, T.vox_begin + T.vox_count - 1, T.det_begin};
-        pe_brick<MODE, false>(g, bs, ws, lane, wid, O, di, gx, gy, gz, T.iz0, T.iz1, B.bx, B.by, B.bz, cr, sr,
-                              nullptr);
+        pe_brick<MODE, false, ELL>(g, bs, ws, lane, wid, O, di, gx, gy, gz, T.iz0, T.iz1, B.bx, B.by, B.bz, cr,
+                                   sr, nullptr);
     }
 }
 
@@ -1014,7 +1060,7 @@ int launch_pe_adjoint(const DevGeom& g, const AdjLaunch& L, int kind, int num_sm
     return launch_adjoint_kind<2>(g, L, num_sms, stream);
 }
 
-template <int MODE>
+template <int MODE, bool ELL>
 static int configure_batch_mode(int* per_sm)
 {
     const int smem = (int)sizeof(BatchSmem);
@@ -1023,30 +1069,37 @@ static int configure_batch_mode(int* per_sm)
     if (cudaGetDevice(&dev) != cudaSuccess) return -1;
     const unsigned long long bit = 1ull << (dev & 63);
     if (!(__atomic_load_n(&configured, __ATOMIC_ACQUIRE) & bit)) {
-        if (cudaFuncSetAttribute(pe_batch_kernel<MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem) !=
+        if (cudaFuncSetAttribute(pe_batch_kernel<MODE, ELL>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem) !=
             cudaSuccess)
             return -1;
         __atomic_fetch_or(&configured, bit, __ATOMIC_RELEASE);
     }
     *per_sm = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(per_sm, pe_batch_kernel<MODE>, kThreads, smem) !=
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(per_sm, pe_batch_kernel<MODE, ELL>, kThreads, smem) !=
         cudaSuccess)
         return -1;
     if (*per_sm < 1) *per_sm = 1;
     return 0;
 }
 
-int configure_pe_batch(int mode, int* blocks_per_sm)
+int configure_pe_batch(int mode, bool ell, int* blocks_per_sm)
 {
-    return mode == 0 ? configure_batch_mode<0>(blocks_per_sm) : configure_batch_mode<1>(blocks_per_sm);
+    if (ell) return mode == 0 ? configure_batch_mode<0, true>(blocks_per_sm)
+                              : configure_batch_mode<1, true>(blocks_per_sm);
+    return mode == 0 ? configure_batch_mode<0, false>(blocks_per_sm) : configure_batch_mode<1, false>(blocks_per_sm);
 }
 
-int launch_pe_batch(const BatchLaunch& B, int mode, int grid, cudaStream_t stream)
+int launch_pe_batch(const BatchLaunch& B, int mode, bool ell, int grid, cudaStream_t stream)
 {
     if (B.n_tasks < 1 || B.total_items < 1) return 0;
     const int smem = (int)sizeof(BatchSmem);
-    if (mode == 0) pe_batch_kernel<0><<<grid, kThreads, smem, stream>>>(B);
-    else pe_batch_kernel<1><<<grid, kThreads, smem, stream>>>(B);
+    if (ell) {
+        if (mode == 0) pe_batch_kernel<0, true><<<grid, kThreads, smem, stream>>>(B);
+        else pe_batch_kernel<1, true><<<grid, kThreads, smem, stream>>>(B);
+    } else {
+        if (mode == 0) pe_batch_kernel<0, false><<<grid, kThreads, smem, stream>>>(B);
+        else pe_batch_kernel<1, false><<<grid, kThreads, smem, stream>>>(B);
+    }
     return cudaGetLastError() == cudaSuccess ? 0 : -1;
 }
 

@@ -82,8 +82,10 @@ int launch_pe_sampled(const DevGeom& g, const PeLaunch& L, int num_sms, cudaStre
 int launch_pe_adjoint(const DevGeom& g, const AdjLaunch& L, int kind, int num_sms, cudaStream_t stream);
 // Sets the batched kernel's shared-memory attribute on the current device (once) and returns
 // how many of its blocks fit on one SM.  Call before capturing a launch into a graph.
-int configure_pe_batch(int mode, int* blocks_per_sm);
-int launch_pe_batch(const BatchLaunch& B, int mode, int grid, cudaStream_t stream);
+// ell: some system of the launch has elliptical holes (the elliptical instance; it also
+// computes circular holes, bit-identically).
+int configure_pe_batch(int mode, bool ell, int* blocks_per_sm);
+int launch_pe_batch(const BatchLaunch& B, int mode, bool ell, int grid, cudaStream_t stream);
 
 __global__ void derive_crystals(const float* __restrict__ det, float fov, int n, float4* pos,
                                 float4* size, float4* mu, float4* trig);

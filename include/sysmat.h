@@ -114,8 +114,8 @@ SYSMAT_API int sysmat_pe(sysmat_ctx* ctx, float rotation, int det_begin, int det
  * voxel_sub[3]: source points along x, y and z on the centres of a grid over the voxel (each
  * 1..SYSMAT_SAMPLED_MAX_SUB, product <= SYSMAT_SAMPLED_MAX_POINTS).  The element is the mean
  * over the source points of the reference's element at that point with that division, every
- * sub-element contribution summed in FP64; {8,16,8} with {1,1,1} is SYSMAT_MODE_PRECISE's
- * sysmat_pe up to the order of the FP64 sum.  Blocks, strides and errors as sysmat_pe. */
+ * sub-element contribution summed in FP64; {8,16,8} with {1,1,1} runs SYSMAT_MODE_PRECISE's
+ * float program (equal to its last bits).  Blocks, strides and errors as sysmat_pe. */
 #define SYSMAT_SAMPLED_MAX_DIV 64
 #define SYSMAT_SAMPLED_MAX_SUBELEMENTS 4096
 #define SYSMAT_SAMPLED_MAX_SUB 8
@@ -164,7 +164,8 @@ SYSMAT_API int sysmat_scatter(sysmat_ctx* ctx, int parts, int hole_model, float 
  * the reference's chord; rho_x[h] <= 0 keeps it circular.  The hole's radius field in
  * Params_Collimator must bound both semi-axes (the reference cone test and the kernel's
  * filters use it).  rho_x = NULL restores circular holes.  Applies to sysmat_pe (and the
- * entry points built on it); the batched and adjoint paths reject such contexts. */
+ * entry points built on it) and to batch plans created afterwards; the adjoint entry points
+ * reject such contexts. */
 SYSMAT_API int sysmat_set_hole_shapes(sysmat_ctx* ctx, const float* rho_x, const float* rho_z, const float* theta);
 
 /* Whole photoelectric matrix of rotation `rotation` written to `path` in compressed form
@@ -194,7 +195,8 @@ typedef struct sysmat_batch_item {
 typedef struct sysmat_batch_plan sysmat_batch_plan;
 
 /* Validate the items (each block as sysmat_pe checks it) and upload the work queue.  The
- * plan keeps pointers to the contexts' device tables: destroy it before them. */
+ * plan keeps pointers to the contexts' device tables: destroy it before them.  It takes each
+ * context's hole shapes (sysmat_set_hole_shapes) as they are when the plan is created. */
 SYSMAT_API int sysmat_batch_create(sysmat_batch_plan** plan, sysmat_ctx* const* ctxs, int n_ctx,
                                    const sysmat_batch_item* items, int n_items);
 /* Voxel brick of one work item (bx*by*bz <= 512) and resident blocks per SM (0 = all that fit). */

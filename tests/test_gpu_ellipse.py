@@ -78,7 +78,7 @@ def test_all_circular_shape_table_is_bit_identical(gpu):
     assert np.array_equal(_pe(gpu, ctx, 1.0), plain)
 
 
-def test_invalid_shapes_and_unsupported_paths_raise(gpu):
+def test_invalid_shapes_and_the_adjoint_raise(gpu):
     geo, shapes = _system_and_shapes(54)
     ctx = sysmat.Context(geo)
     bad = shapes.copy()
@@ -90,9 +90,32 @@ def test_invalid_shapes_and_unsupported_paths_raise(gpu):
     with pytest.raises(sysmat.SysmatError):
         ctx.set_hole_shapes(bad)
     ctx.set_hole_shapes(shapes)
-    out = gpu.empty((ctx.n_det, ctx.n_vox), dtype=gpu.float32, device="cuda")
-    with pytest.raises(sysmat.SysmatError):
-        sysmat.BatchPlan([ctx], [(0, 0.0, 0, ctx.n_det, 0, ctx.n_vox, out)])
     x = gpu.ones(ctx.n_vox, dtype=gpu.float32, device="cuda")
     with pytest.raises(sysmat.SysmatError):
         ctx.project(x)
+
+
+def test_batched_launch_with_elliptical_holes_equals_single_calls(gpu):
+    """A plan over an elliptical and a circular system runs the batched kernel's elliptical
+    instance; every element equals the single-system sysmat_pe element bit for bit."""
+    torch = gpu
+    geo, shapes = _system_and_shapes(55)
+    ell, circ = sysmat.Context(geo), sysmat.Context(geometry.mini(seed=56, layers=1, nvox=(7, 4, 2), ncry=(4, 4)))
+    ell.set_hole_shapes(shapes)
+    tasks = [(0, 2.0, 0, ell.n_det, 0, ell.n_vox), (1, 0.0, 3, 9, 5, 40), (0, 5.0, 7, 4, 13, 50)]
+    ctxs = [ell, circ]
+    for mode in (sysmat.MODE_REFERENCE, sysmat.MODE_PRECISE):
+        exp = []
+        for (c, rot, d0, nd, v0, nv) in tasks:
+            t = torch.empty((nd, nv), dtype=torch.float32, device="cuda")
+            ctxs[c].pe(t, rotation=rot, det_begin=d0, det_count=nd, vox_begin=v0, vox_count=nv, mode=mode)
+            exp.append(t.cpu().numpy())
+        outs = [torch.full((t[3], t[5]), -1.0, dtype=torch.float32, device="cuda") for t in tasks]
+        sysmat.batch(ctxs, [t + (o,) for t, o in zip(tasks, outs)], mode=mode)
+        for o, e in zip(outs, exp):
+            assert np.array_equal(o.cpu().numpy(), e)
+    # the shapes matter: the elliptical system's block differs from its circular one
+    plain = sysmat.Context(geo)
+    t = torch.empty((plain.n_det, plain.n_vox), dtype=torch.float32, device="cuda")
+    plain.pe(t, rotation=2.0)
+    assert not np.array_equal(t.cpu().numpy(), exp[0])
