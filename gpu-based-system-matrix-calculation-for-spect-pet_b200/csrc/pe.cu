@@ -371,7 +371,9 @@ __device__ __forceinline__ int fill_round(const DevGeom& g, WarpSmem& ws, const 
                 const float4 hb = __ldg(&g.hole.b[id]);
                 ws.ra[pos] = make_float4(ha.x, ha.w, hb.x, hb.y);
                 ws.rb[pos] = make_float4(ha.y, ha.z, 0.0f, 0.0f);
-                if constexpr (ELL) ws.rc[pos] = __ldg(&g.hole_shape[id]);   // rho_x, rho_z, cos, sin
+                if constexpr (ELL) {        // rho_x, rho_z, cos, sin; a batch may mix in circular systems
+                    ws.rc[pos] = g.hole_shape ? __ldg(&g.hole_shape[id]) : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+                }
                 ws.rl[pos] = layer_of_hole(g, id);
             } else {
                 const int o = id - g.n_holes;
