@@ -16,7 +16,8 @@ of the PE kernel against measured FP32 / MUFU peaks, `cpu_baseline` = the CPU or
 reference's float arithmetic restated in C, OpenMP) on a bounded sample, and `scatter` =
 the primary-Compton rate on a configuration-3 plane, `batch` = the configuration-4 design
 sweep in one batched launch against one launch per task, `sampled` = configuration 2 with
-the sampling it states (2x2x2 voxel sub-samples, 2x8x2 crystal sub-elements).
+the sampling it states (2x2x2 voxel sub-samples, 2x8x2 crystal sub-elements), `fp64` = the
+FP64 mode (the element program in double) on the headline plane.
 
 `--impl reference` times the reference's own CUDA program (its source compiled for sm_100a
 by oracle/Makefile into oracle/_ref) through its own host entry point PESysMatGen on a
@@ -271,6 +272,10 @@ def run_sysmat(args, rank, world, local):
     if not args.no_sampled and world == 1:
         sampled = run_sampled(args, sysmat, torch)
 
+    fp64 = None
+    if not args.no_fp64 and world == 1:
+        fp64 = run_fp64(args, sysmat, torch)
+
     result = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": region_ms / args.steps, "higher_is_better": True,
@@ -280,7 +285,7 @@ def run_sysmat(args, rank, world, local):
                    "elements_per_step_per_gpu": D * nxy, "summation": "reference order (float chain)",
                    "l2": "flushed between steps (256 MB write)"},
         "clocks": clk.summary(), "gpu_launches": args.steps,
-        "roofline": roof, "e2e": e2e, "scatter": scatter, "batch": batch, "sampled": sampled,
+        "roofline": roof, "e2e": e2e, "scatter": scatter, "batch": batch, "sampled": sampled, "fp64": fp64,
     }
     return result
 
@@ -362,6 +367,30 @@ def run_sampled(args, sysmat, torch, rows=512):
             "summation": "FP64",
             "workload": f"config2 as stated: 2x2x2 voxel sub-samples, 2x8x2 crystal sub-elements; crystals "
                         f"{d0}..{d0 + rows - 1} x z-plane 16 ({rows * nxy} elements)"}
+
+
+def run_fp64(args, sysmat, torch):
+    """FP64 mode (the reference's element program in double: within the float output's
+    rounding of the FP64 restatement) on the headline step: z-plane 16 of configuration 2 for
+    all 4096 crystals, reference sampling (8x16x8, voxel centres); one untimed step, one timed."""
+    g = geometry.config2()
+    ctx = sysmat.Context(g)
+    nxy = int(g.image[0]) * int(g.image[1])
+    out = torch.empty((ctx.n_det, nxy), dtype=torch.float32, device="cuda")
+
+    def step():
+        ctx.pe(out, vox_begin=16 * nxy, vox_count=nxy, mode=sysmat.MODE_FP64)
+
+    step()
+    torch.cuda.synchronize()
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record()
+    step()
+    b.record()
+    torch.cuda.synchronize()
+    ms = a.elapsed_time(b)
+    return {"value": ctx.n_det * nxy / (ms * 1e-3), "unit": UNIT, "ms_per_step": ms, "arithmetic": "f64",
+            "workload": f"config2 PE in FP64: all {ctx.n_det} crystals x z-plane 16 ({ctx.n_det * nxy} elements)"}
 
 
 def run_batch(args, sysmat, torch, n_instances=64, rows=8, sweep=True):
@@ -533,6 +562,7 @@ def main():
     ap.add_argument("--no-scatter", action="store_true")
     ap.add_argument("--no-batch", action="store_true")
     ap.add_argument("--no-sampled", action="store_true")
+    ap.add_argument("--no-fp64", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
     if args.warmup < 3 and args.impl == "sysmat":

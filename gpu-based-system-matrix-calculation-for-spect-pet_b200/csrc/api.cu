@@ -194,6 +194,47 @@ extern "C" SYSMAT_API int sysmat_create(sysmat_ctx** out, int device, const floa
     ctx->g.hole.raw = th + 2 * Hs;
     derive_crystals<<<(D + 127) / 128, 128>>>(ctx->d_det, g.fov, D, t, t + D, t + 2 * D, t + 3 * D);
     if (H > 0) derive_holes<<<(H + 127) / 128, 128>>>(ctx->d_col, g.fov, H, th, th + Hs, th + 2 * Hs);
+
+    // FP64 mode tables: crystals 3 x D4, holes 2 x D4, layers kLayer64 doubles each (from the
+    // raw floats in double, as the FP64 restatement forms them: PESysMatGen.cu:1242-1249)
+    const size_t n64 = 3 * (size_t)D + 2 * (size_t)Hs;
+    const size_t layer_bytes = sizeof(double) * kLayer64 * (size_t)(g.n_layers > 0 ? g.n_layers : 1);
+    if (cudaMalloc(&ctx->d_tables64, sizeof(D4) * n64 + layer_bytes) != cudaSuccess) {
+        ctx->d_tables64 = nullptr;
+        sysmat_destroy(ctx);
+        return SYSMAT_ERR_NOMEM;
+    }
+    D4* t64 = static_cast<D4*>(ctx->d_tables64);
+    ctx->g.t64.cry_pos = t64;
+    ctx->g.t64.cry_size = t64 + D;
+    ctx->g.t64.cry_trig = t64 + 2 * D;
+    ctx->g.t64.hole_a = t64 + 3 * D;
+    ctx->g.t64.hole_b = t64 + 3 * D + Hs;
+    double* lay64 = reinterpret_cast<double*>(t64 + n64);
+    ctx->g.t64.layer = lay64;
+    {
+        std::vector<double> hl(kLayer64 * (size_t)(g.n_layers > 0 ? g.n_layers : 1), 0.0);
+        const double fov = (double)g.fov;
+        for (int m = 0; m < g.n_layers; ++m) {
+            const float* L = pC + (m + 1) * 10;
+            double* o = hl.data() + kLayer64 * m;
+            o[0] = -(double)L[1] / 2.0;
+            o[1] = (double)L[1] / 2.0;
+            o[2] = -(double)L[2] / 2.0 + fov + (double)L[4];
+            o[3] = (double)L[2] / 2.0 + fov + (double)L[4];
+            o[4] = -(double)L[3] / 2.0;
+            o[5] = (double)L[3] / 2.0;
+            o[6] = (double)L[2];
+            o[7] = (double)L[5];
+        }
+        if (cudaMemcpy(lay64, hl.data(), sizeof(double) * hl.size(), cudaMemcpyHostToDevice) != cudaSuccess) {
+            sysmat_destroy(ctx);
+            return SYSMAT_ERR_CUDA;
+        }
+    }
+    if (D + H > 0)
+        derive_tables64<<<(D + H + 127) / 128, 128>>>(ctx->d_det, ctx->d_col, g.fov, D, H, t64, t64 + D, t64 + 2 * D,
+                                                      t64 + 3 * D, t64 + 3 * D + Hs);
     if (cudaGetLastError() != cudaSuccess || cudaDeviceSynchronize() != cudaSuccess) {
         sysmat_destroy(ctx);
         return SYSMAT_ERR_CUDA;
@@ -208,6 +249,7 @@ extern "C" SYSMAT_API int sysmat_destroy(sysmat_ctx* ctx)
     scatter_scratch_free(ctx->scratch);
     cudaFree(ctx->d_kn_tab);
     cudaFree(ctx->d_shapes);
+    cudaFree(ctx->d_tables64);
     cudaFree(ctx->d_det);
     cudaFree(ctx->d_col);
     cudaFree(ctx->d_img);
@@ -293,7 +335,9 @@ extern "C" SYSMAT_API int sysmat_pe(sysmat_ctx* ctx, float rotation, int det_beg
 {
     int rc = check_block(ctx, det_begin, det_count, vox_begin, vox_count, d_out, ld);
     if (rc) return rc;
-    if (mode != SYSMAT_MODE_REFERENCE && mode != SYSMAT_MODE_PRECISE) return SYSMAT_ERR_ARG;
+    if (mode != SYSMAT_MODE_REFERENCE && mode != SYSMAT_MODE_PRECISE && mode != SYSMAT_MODE_FP64)
+        return SYSMAT_ERR_ARG;
+    if (mode == SYSMAT_MODE_FP64 && ctx->g.hole_shape) return SYSMAT_ERR_ARG;   // circular holes only
     if (det_count == 0 || vox_count == 0) return SYSMAT_OK;
     cudaStream_t s = (cudaStream_t)stream;
     CUDA_TRY(cudaMemsetAsync(ctx->d_counter, 0, sizeof(unsigned long long), s));

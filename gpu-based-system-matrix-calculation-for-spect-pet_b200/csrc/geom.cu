@@ -60,6 +60,28 @@ __global__ void ell_chords_kernel(const float* __restrict__ a, float* __restrict
                        sinf(p[12]));
 }
 
+// FP64 tables: one thread per crystal, then one per hole (all layers), with the double
+// operations of the FP64 restatement of PESysMatGen.cu:1058-1068, :1124-1135, :1159-1166.
+__global__ void derive_tables64(const float* __restrict__ det, const float* __restrict__ col, float fov, int n_det,
+                                int n_holes, D4* cry_pos, D4* cry_size, D4* cry_trig, D4* hole_a, D4* hole_b)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const double f = (double)fov;
+    if (i < n_det) {
+        const float* p = det + 12 * i;
+        const double rot = (double)p[11];
+        cry_pos[i] = D4{(double)p[1], (double)p[2] + f, (double)p[3], (double)p[7]};
+        cry_size[i] = D4{(double)p[4], (double)p[5], (double)p[6], (double)p[8]};
+        cry_trig[i] = D4{cos(rot), sin(rot), cos(-rot), sin(-rot)};
+    } else if (i < n_det + n_holes) {
+        const int h = i - n_det;
+        const float* p = col + 100 + 9 * h;
+        const double y1 = (double)p[1] + f, y2 = (double)p[2] + f, r = (double)p[4];
+        hole_a[h] = D4{(double)p[0], y1, y2, (double)p[3]};
+        hole_b[h] = D4{r, (double)p[5], (y1 + y2) / 2.0, sqrt(r * r * 4.0 + (y1 - y2) * (y1 - y2)) / 2.0};
+    }
+}
+
 }  // namespace sysmat
 
 extern "C" SYSMAT_API int sysmat_ell_chords(const float* d_args, float* d_out, int n, void* stream)

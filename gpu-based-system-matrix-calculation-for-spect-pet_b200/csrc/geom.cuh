@@ -40,6 +40,23 @@ struct HoleTables {
     const float4* raw;
 };
 
+// FP64 mode: the derived geometry in double, formed from the raw float parameters with the
+// double operations of the FP64 restatement (y + FOV and the like in double, not rounded to
+// float as in the tables above).
+struct alignas(32) D4 {
+    double x, y, z, w;
+};
+
+struct Tables64 {
+    const D4* hole_a;      // x, y1 + fov, y2 + fov, z
+    const D4* hole_b;      // r, mu, y centre, cone radius sqrt(4 r^2 + (y1 - y2)^2) / 2
+    const D4* cry_pos;     // x, y + fov, z, mu_total
+    const D4* cry_size;    // w, t, h, mu_pe
+    const D4* cry_trig;    // cos rot, sin rot, cos -rot, sin -rot
+    const double* layer;   // kLayer64 values per layer: x1, x2, y1, y2, z1, z2, thickness, mu_total
+};
+constexpr int kLayer64 = 8;
+
 struct LayerInfo {
     float x1, x2, y1, y2, z1, z2;   // plate box (PESysMatGen.cu:1242-1249)
     float thickness;
@@ -66,6 +83,7 @@ struct DevGeom {
     // optional elliptical holes (sysmat_set_hole_shapes): per hole (rho_x, rho_z, cos theta,
     // sin theta), rho_x = 0 for a circular hole; nullptr when every hole is circular
     const float4* hole_shape;
+    Tables64 t64;        // FP64 mode tables (nullptr pointers where a caller built no such tables)
     LayerInfo layer[kMaxLayers];
 };
 

@@ -27,6 +27,7 @@
 //  * the element sum is one float chain in the reference's sub-element order
 //    (SYSMAT_MODE_REFERENCE, the reference's atomicAdd sequence at :1359) or an FP64
 //    accumulation (SYSMAT_MODE_PRECISE); lane 0 writes dst[d][v].
+#include "chord64.cuh"
 #include "geom.cuh"
 #include "pe.cuh"
 
@@ -54,7 +55,10 @@ struct WarpSmem {
     float4 rr[kRound], ra[kRound], rb[kRound], rc[kRound];
     int rl[kRound];                      // layer of a hole entry; n_layers for crystals
     float4 inner[kMaxLayers];            // plate "through both faces" slope rectangle
-    float chain[256];                    // contributions of sub-elements 256p .. 256p+255
+    union {
+        float chain[256];                // contributions of sub-elements 256p .. 256p+255
+        double e64[32];                  // FP64 mode: the element's constants (Elem64)
+    };
 };
 
 struct BlockSmem {
@@ -332,8 +336,9 @@ __device__ __forceinline__ bool capsule_meets_box(float xo, float zo, float y0, 
 // Copy kept entries [k0, k1) whose rectangle and capsule meet the round's slope box into
 // the round buffer from position n, with their geometry (one entry per lane); returns the
 // new count.  Stops before the buffer could overflow; *next receives the first entry not
-// examined.
-template <bool ELL>
+// examined.  IDS: store each entry's object id (as the bits of ra.x) instead of its float
+// geometry, for walks that read their own geometry tables (FP64 mode).
+template <bool ELL, bool IDS = false>
 __device__ __forceinline__ int fill_round(const DevGeom& g, WarpSmem& ws, const Elem& e, int k0, int k1,
                                           float4 box, int n, int lane, int* next, int* nh)
 {
@@ -366,7 +371,10 @@ __device__ __forceinline__ int fill_round(const DevGeom& g, WarpSmem& ws, const 
         if (keep) {
             const int pos = n + __popc(m & ((1u << lane) - 1u));
             ws.rr[pos] = rect;
-            if (id < g.n_holes) {
+            if constexpr (IDS) {
+                ws.ra[pos].x = __int_as_float(id);
+                ws.rl[pos] = id < g.n_holes ? layer_of_hole(g, id) : g.n_layers;
+            } else if (id < g.n_holes) {
                 const float4 ha = __ldg(&g.hole.a[id]);
                 const float4 hb = __ldg(&g.hole.b[id]);
                 ws.ra[pos] = make_float4(ha.x, ha.w, hb.x, hb.y);
@@ -814,6 +822,8 @@ __device__ double pe_element_sampled(const DevGeom& g, const BlockSmem& bs, Warp
     return dacc / (double)n_pts;
 }
 
+#include "pe_fp64.cuh"
+
 // Block superset of the reference cone test over all voxels within radius rho of
 // (cx, cy, cz): keep object o when |u_o - u_d| <= (rho + r_o)/(L_o - rho)
 // + (rho + r_d)/(L_d - rho) + 1e-4 at the centre (each direction moves by at most
@@ -885,7 +895,8 @@ template <int MODE, bool COUNT, bool ELL = false, bool SAMPLED = false>
 __device__ __forceinline__ void pe_brick(const DevGeom& g, BlockSmem& bs, WarpSmem& ws, int lane, int wid,
                                          const BrickOut& O, int di, int gx, int gy, int gz, int iz0, int iz1,
                                          int bx, int by, int bz, float cr, float sr,
-                                         unsigned long long* counters, const Sampling* smp = nullptr)
+                                         unsigned long long* counters, const Sampling* smp = nullptr,
+                                         float rotation = 0.0f)
 {
     const int x0 = gx * bx, y0 = gy * by, z0 = iz0 + gz * bz;
     const int x1 = min(x0 + bx, g.nx) - 1, y1 = min(y0 + by, g.ny) - 1, z1 = min(z0 + bz, iz1 + 1) - 1;
@@ -908,6 +919,7 @@ __device__ __forceinline__ void pe_brick(const DevGeom& g, BlockSmem& bs, WarpSm
         if (v < O.vox_begin || v > O.vlast) continue;
         float val;
         if constexpr (SAMPLED) val = (float)pe_element_sampled<ELL>(g, bs, ws, d, v, cr, sr, lane, *smp);
+        else if constexpr (MODE == 2) val = (float)pe_element64(g, bs, ws, d, v, cr, sr, rotation, lane);
         else val = (float)pe_element<MODE, COUNT, ELL>(g, bs, ws, d, v, cr, sr, lane, counters);
         if (lane == 0) O.out[(long long)di * O.ld + (v - O.vox_begin)] = val;
         __syncwarp();
@@ -945,7 +957,7 @@ __global__ void __launch_bounds__(kThreads, 2) pe_kernel(DevGeom g, PeLaunch L)
         const int rem = (int)(b - (long long)gz * nbx * nby);
         const int gy = rem / nbx, gx = rem - gy * nbx;
         pe_brick<MODE, COUNT, ELL, SAMPLED>(g, bs, ws, lane, wid, O, di, gx, gy, gz, iz0, iz1, bx, by, bz, cr, sr,
-                                            L.counters, &L.smp);
+                                            L.counters, &L.smp, L.rotation);
     }
 }
 
@@ -1108,11 +1120,13 @@ int launch_pe_batch(const BatchLaunch& B, int mode, bool ell, int grid, cudaStre
 int launch_pe(const DevGeom& g, const PeLaunch& L, int mode, int num_sms, cudaStream_t stream)
 {
     if (g.hole_shape) {                   // systems with elliptical holes
+        if (mode == 2) return -1;         // no FP64 elliptical chord
         if (L.counters) return launch_mode<0, true, true>(g, L, num_sms, stream);
         return mode == 0 ? launch_mode<0, false, true>(g, L, num_sms, stream)
                          : launch_mode<1, false, true>(g, L, num_sms, stream);
     }
     if (L.counters) return launch_mode<0, true, false>(g, L, num_sms, stream);
+    if (mode == 2) return g.t64.cry_pos ? launch_mode<2, false, false>(g, L, num_sms, stream) : -1;
     return mode == 0 ? launch_mode<0, false, false>(g, L, num_sms, stream)
                      : launch_mode<1, false, false>(g, L, num_sms, stream);
 }

@@ -21,6 +21,7 @@ ERRORS = {-1: "SYSMAT_ERR_ARG", -2: "SYSMAT_ERR_CUDA", -3: "SYSMAT_ERR_CAPACITY"
           -4: "SYSMAT_ERR_IO", -5: "SYSMAT_ERR_NOMEM", -6: "SYSMAT_ERR_TIMEOUT"}
 MODE_REFERENCE = 0
 MODE_PRECISE = 1
+MODE_FP64 = 2
 THETA_N = 7
 THETA_NAMES = ("mu_w", "mu_crystal", "radius", "dx", "dy", "dz", "tilt")
 SCATTER_CRYSTAL = 1
