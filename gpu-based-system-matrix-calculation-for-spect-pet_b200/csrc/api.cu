@@ -250,6 +250,7 @@ extern "C" SYSMAT_API int sysmat_destroy(sysmat_ctx* ctx)
     cudaFree(ctx->d_kn_tab);
     cudaFree(ctx->d_shapes);
     cudaFree(ctx->d_tables64);
+    cudaFree(ctx->d_shapes64);
     cudaFree(ctx->d_det);
     cudaFree(ctx->d_col);
     cudaFree(ctx->d_img);
@@ -266,8 +267,9 @@ extern "C" SYSMAT_API int sysmat_set_hole_shapes(sysmat_ctx* ctx, const float* r
 {
     if (!ctx || !same_device(ctx)) return SYSMAT_ERR_ARG;
     if (!rho_x) {                                   // back to circular holes
-        // the table stays allocated until sysmat_destroy: batch plans copy its pointer
+        // the tables stay allocated until sysmat_destroy: batch plans copy their pointers
         ctx->g.hole_shape = nullptr;
+        ctx->g.t64.hole_shape = nullptr;
         return SYSMAT_OK;
     }
     if (!rho_z || !theta) return SYSMAT_ERR_ARG;
@@ -292,15 +294,21 @@ extern "C" SYSMAT_API int sysmat_set_hole_shapes(sysmat_ctx* ctx, const float* r
         ctx->d_shapes = nullptr;
         return SYSMAT_ERR_NOMEM;
     }
+    if (!ctx->d_shapes64 && cudaMalloc(&ctx->d_shapes64, sizeof(D4) * (size_t)(n > 0 ? n : 1)) != cudaSuccess) {
+        ctx->d_shapes64 = nullptr;
+        return SYSMAT_ERR_NOMEM;
+    }
     if (cudaMalloc(&d_s, sizeof(float) * h.size()) != cudaSuccess) return SYSMAT_ERR_NOMEM;
     cudaError_t e = cudaMemcpy(d_s, h.data(), sizeof(float) * h.size(), cudaMemcpyHostToDevice);
     if (e == cudaSuccess && n > 0) {
         derive_shapes<<<(n + 255) / 256, 256>>>(d_s, n, ctx->d_shapes);
+        derive_shapes64<<<(n + 255) / 256, 256>>>(d_s, n, ctx->d_shapes64);
         e = cudaDeviceSynchronize();
     }
     cudaFree(d_s);
     if (e != cudaSuccess) return SYSMAT_ERR_CUDA;
     ctx->g.hole_shape = ctx->d_shapes;
+    ctx->g.t64.hole_shape = ctx->d_shapes64;
     return SYSMAT_OK;
 }
 
@@ -337,7 +345,6 @@ extern "C" SYSMAT_API int sysmat_pe(sysmat_ctx* ctx, float rotation, int det_beg
     if (rc) return rc;
     if (mode != SYSMAT_MODE_REFERENCE && mode != SYSMAT_MODE_PRECISE && mode != SYSMAT_MODE_FP64)
         return SYSMAT_ERR_ARG;
-    if (mode == SYSMAT_MODE_FP64 && ctx->g.hole_shape) return SYSMAT_ERR_ARG;   // circular holes only
     if (det_count == 0 || vox_count == 0) return SYSMAT_OK;
     cudaStream_t s = (cudaStream_t)stream;
     CUDA_TRY(cudaMemsetAsync(ctx->d_counter, 0, sizeof(unsigned long long), s));

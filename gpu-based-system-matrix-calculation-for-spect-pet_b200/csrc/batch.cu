@@ -40,7 +40,7 @@ struct sysmat_batch_plan {
     unsigned long long* d_counter = nullptr;
     BatchLaunch launch{};                  // current task table
     cudaStream_t capture = nullptr;
-    cudaGraphExec_t exec[2] = {nullptr, nullptr};
+    cudaGraphExec_t exec[3] = {nullptr, nullptr, nullptr};   // one graph per mode
 };
 
 namespace {
@@ -201,9 +201,14 @@ extern "C" SYSMAT_API int sysmat_batch_get_tiles(const sysmat_batch_plan* p, int
     return SYSMAT_OK;
 }
 
+bool plan_mode_ok(const sysmat_batch_plan*, int mode)
+{
+    return mode == SYSMAT_MODE_REFERENCE || mode == SYSMAT_MODE_PRECISE || mode == SYSMAT_MODE_FP64;
+}
+
 extern "C" SYSMAT_API int sysmat_batch_run(sysmat_batch_plan* p, int mode, void* stream)
 {
-    if (!p || (mode != SYSMAT_MODE_REFERENCE && mode != SYSMAT_MODE_PRECISE)) return SYSMAT_ERR_ARG;
+    if (!p || !plan_mode_ok(p, mode)) return SYSMAT_ERR_ARG;
     if (!device_is(p->device)) return SYSMAT_ERR_ARG;
     if (p->launch.total_items < 1) return SYSMAT_OK;
     cudaGraphExec_t& exec = p->exec[mode];
@@ -238,7 +243,7 @@ extern "C" SYSMAT_API int sysmat_batch_run(sysmat_batch_plan* p, int mode, void*
 // writes rows of the caller's outputs with the values the batch itself computes there.
 extern "C" SYSMAT_API int sysmat_batch_tune(sysmat_batch_plan* p, int mode, void* stream, int* tiles)
 {
-    if (!p || (mode != SYSMAT_MODE_REFERENCE && mode != SYSMAT_MODE_PRECISE)) return SYSMAT_ERR_ARG;
+    if (!p || !plan_mode_ok(p, mode)) return SYSMAT_ERR_ARG;
     if (!device_is(p->device)) return SYSMAT_ERR_ARG;
     if (p->items.empty()) return tiles ? sysmat_batch_get_tiles(p, tiles) : SYSMAT_OK;
     drop_graphs(p);                          // the probe reuses the task array
@@ -295,7 +300,8 @@ extern "C" SYSMAT_API int sysmat_batch_tune(sysmat_batch_plan* p, int mode, void
 extern "C" SYSMAT_API int sysmat_batch(sysmat_ctx* const* ctxs, int n_ctx, const sysmat_batch_item* items,
                                        int n_items, int mode, void* stream)
 {
-    if (mode != SYSMAT_MODE_REFERENCE && mode != SYSMAT_MODE_PRECISE) return SYSMAT_ERR_ARG;
+    if (mode != SYSMAT_MODE_REFERENCE && mode != SYSMAT_MODE_PRECISE && mode != SYSMAT_MODE_FP64)
+        return SYSMAT_ERR_ARG;
     sysmat_batch_plan* p = nullptr;
     int rc = sysmat_batch_create(&p, ctxs, n_ctx, items, n_items);
     if (rc) return rc;

@@ -182,4 +182,45 @@ __device__ __forceinline__ double ray_cyl64_chord(const RayCyl64& c, double xi, 
     return eb - ea;
 }
 
+// Elliptical cylinder ((x' - xc)/rx)^2 + ((z' - zc)/rz)^2 <= 1, y in [y1, y2], with the
+// segment's points rotated by theta about the axis first (PESysMatGen.cu:801-947, defined but
+// not called by the reference kernels); ct, st = cos(theta), sin(theta).  The expressions are
+// the reference's in double; the ending takes the overlap of the side and cap intervals, as
+// ray_cyl64_chord does.
+__device__ __forceinline__ double ell_chord64(double xi, double yi, double zi, double xo, double yo, double zo,
+                                              double xc, double y1, double y2, double zc, double rx, double rz,
+                                              double ct, double st)
+{
+    const double xi_ = xi - xc, zi_ = zi - zc, xo_ = xo - xc, zo_ = zo - zc;
+    xi = xc + xi_ * ct + zi_ * st;
+    zi = zc - xi_ * st + zi_ * ct;
+    xo = xc + xo_ * ct + zo_ * st;
+    zo = zc - xo_ * st + zo_ * ct;
+    if (fabs(y1 - y2) < 0.001) return 0.0;
+    const double tio = sqrt((xo - xi) * (xo - xi) + (yo - yi) * (yo - yi) + (zo - zi) * (zo - zi));
+    const double kx = (xo - xi) / tio, ky = (yo - yi) / tio, kz = (zo - zi) / tio;
+    const double xl = xi + kx / ky * (y1 - yi), xr = xi + kx / ky * (y2 - yi);
+    const double zl = zi + kz / ky * (y1 - yi), zr = zi + kz / ky * (y2 - yi);
+    const double ta = (y1 - yi) / ky, tb = (y2 - yi) / ky;
+    const bool fl = ((xl - xc) * (xl - xc) / rx / rx + (zl - zc) * (zl - zc) / rz / rz) <= 1.0;
+    const bool fr = ((xr - xc) * (xr - xc) / rx / rx + (zr - zc) * (zr - zc) / rz / rz) <= 1.0;
+    if (fr && fl) {
+        if (ta <= 0.0001 || tb <= 0.0001) return 0.0;
+        if (ta >= tio || tb >= tio) return 0.0;
+        return fabs(tb - ta);
+    }
+    const double x_ = xi - xc, z_ = zi - zc;
+    const double a = kx * kx * rz * rz + kz * kz * rx * rx;
+    const double b = kx * x_ * rz * rz + kz * z_ * rx * rx;
+    const double c = rz * rz * x_ * x_ + rx * rx * z_ * z_ - rx * rx * rz * rz;
+    const double delta = b * b - a * c;
+    if (delta <= 0.00001) return 0.0;
+    const double t1 = (-b - sqrt(delta)) / a, t2 = (-b + sqrt(delta)) / a;
+    const double ea = t1 > ta ? t1 : ta, eb = t2 < tb ? t2 : tb;
+    if (!(eb > ea)) return 0.0;
+    if (eb <= 0.0001 || ea <= 0.0001) return 0.0;
+    if (eb >= tio || ea >= tio) return 0.0;
+    return eb - ea;
+}
+
 }  // namespace sysmat

@@ -35,6 +35,7 @@ struct sysmat_ctx {
     double* d_kn_tab = nullptr;     // Klein-Nishina table for kn_e0
     float4* d_shapes = nullptr;     // elliptical holes (sysmat_set_hole_shapes), or nullptr
     void* d_tables64 = nullptr;     // FP64 mode tables (DevGeom::t64)
+    sysmat::D4* d_shapes64 = nullptr;   // FP64 mode elliptical holes, or nullptr
     float kn_e0 = -1.0f;
 };
 

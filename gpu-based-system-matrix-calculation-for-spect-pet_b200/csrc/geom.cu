@@ -49,6 +49,17 @@ __global__ void derive_shapes(const float* __restrict__ s, int n, float4* out)
     out[h] = rx > 0.0f ? make_float4(rx, rz, cosf(th), sinf(th)) : make_float4(0.0f, 0.0f, 1.0f, 0.0f);
 }
 
+// The same shapes for the FP64 mode: cos and sin of the float angle in double, as the FP64
+// restatement evaluates them.
+__global__ void derive_shapes64(const float* __restrict__ s, int n, D4* out)
+{
+    const int h = blockIdx.x * blockDim.x + threadIdx.x;
+    if (h >= n) return;
+    const float rx = s[3 * h], rz = s[3 * h + 1];
+    const double th = (double)s[3 * h + 2];
+    out[h] = rx > 0.0f ? D4{(double)rx, (double)rz, cos(th), sin(th)} : D4{0.0, 0.0, 1.0, 0.0};
+}
+
 // Diagnostic: the elliptical-cylinder chord on arrays of arguments (13 per item, as
 // sysmat_ell_chords documents), one thread per item.
 __global__ void ell_chords_kernel(const float* __restrict__ a, float* __restrict__ out, int n)

@@ -54,6 +54,7 @@ struct Tables64 {
     const D4* cry_size;    // w, t, h, mu_pe
     const D4* cry_trig;    // cos rot, sin rot, cos -rot, sin -rot
     const double* layer;   // kLayer64 values per layer: x1, x2, y1, y2, z1, z2, thickness, mu_total
+    const D4* hole_shape;  // elliptical holes: rho_x, rho_z, cos theta, sin theta (rho_x = 0: circle), or nullptr
 };
 constexpr int kLayer64 = 8;
 

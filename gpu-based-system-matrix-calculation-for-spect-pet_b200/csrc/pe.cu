@@ -1016,7 +1016,7 @@ __global__ void __launch_bounds__(kThreads, 2) pe_batch_kernel(BatchLaunch B)
         const int gy = rem / T.nbx, gx = rem - gy * T.nbx;
         const BrickOut O{T.out, T.ld, T.vox_begin, T.vox_begin + T.vox_count - 1, T.det_begin};
         pe_brick<MODE, false, ELL>(g, bs, ws, lane, wid, O, di, gx, gy, gz, T.iz0, T.iz1, B.bx, B.by, B.bz, cr,
-                                   sr, nullptr);
+                                   sr, nullptr, nullptr, T.rotation);
     }
 }
 
@@ -1098,8 +1098,11 @@ static int configure_batch_mode(int* per_sm)
 
 int configure_pe_batch(int mode, bool ell, int* blocks_per_sm)
 {
-    if (ell) return mode == 0 ? configure_batch_mode<0, true>(blocks_per_sm)
-                              : configure_batch_mode<1, true>(blocks_per_sm);
+    if (mode == 2) return configure_batch_mode<2, false>(blocks_per_sm);   // shapes read at run time
+    if (ell) {
+        return mode == 0 ? configure_batch_mode<0, true>(blocks_per_sm)
+                         : configure_batch_mode<1, true>(blocks_per_sm);
+    }
     return mode == 0 ? configure_batch_mode<0, false>(blocks_per_sm) : configure_batch_mode<1, false>(blocks_per_sm);
 }
 
@@ -1107,7 +1110,9 @@ int launch_pe_batch(const BatchLaunch& B, int mode, bool ell, int grid, cudaStre
 {
     if (B.n_tasks < 1 || B.total_items < 1) return 0;
     const int smem = (int)sizeof(BatchSmem);
-    if (ell) {
+    if (mode == 2) {                              // FP64: shapes read at run time
+        pe_batch_kernel<2, false><<<grid, kThreads, smem, stream>>>(B);
+    } else if (ell) {
         if (mode == 0) pe_batch_kernel<0, true><<<grid, kThreads, smem, stream>>>(B);
         else pe_batch_kernel<1, true><<<grid, kThreads, smem, stream>>>(B);
     } else {
@@ -1119,14 +1124,13 @@ int launch_pe_batch(const BatchLaunch& B, int mode, bool ell, int grid, cudaStre
 
 int launch_pe(const DevGeom& g, const PeLaunch& L, int mode, int num_sms, cudaStream_t stream)
 {
+    if (mode == 2) return g.t64.cry_pos ? launch_mode<2, false, false>(g, L, num_sms, stream) : -1;
     if (g.hole_shape) {                   // systems with elliptical holes
-        if (mode == 2) return -1;         // no FP64 elliptical chord
         if (L.counters) return launch_mode<0, true, true>(g, L, num_sms, stream);
         return mode == 0 ? launch_mode<0, false, true>(g, L, num_sms, stream)
                          : launch_mode<1, false, true>(g, L, num_sms, stream);
     }
     if (L.counters) return launch_mode<0, true, false>(g, L, num_sms, stream);
-    if (mode == 2) return g.t64.cry_pos ? launch_mode<2, false, false>(g, L, num_sms, stream) : -1;
     return mode == 0 ? launch_mode<0, false, false>(g, L, num_sms, stream)
                      : launch_mode<1, false, false>(g, L, num_sms, stream);
 }

@@ -92,6 +92,7 @@ __global__ void derive_crystals(const float* __restrict__ det, float fov, int n,
 __global__ void derive_holes(const float* __restrict__ col, float fov, int n, float4* a, float4* b,
                              float4* raw);
 __global__ void derive_shapes(const float* __restrict__ s, int n, float4* out);
+__global__ void derive_shapes64(const float* __restrict__ s, int n, D4* out);
 __global__ void derive_tables64(const float* __restrict__ det, const float* __restrict__ col, float fov, int n_det,
                                 int n_holes, D4* cry_pos, D4* cry_size, D4* cry_trig, D4* hole_a, D4* hole_b);
 

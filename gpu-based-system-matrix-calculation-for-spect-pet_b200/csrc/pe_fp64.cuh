@@ -189,7 +189,12 @@ __device__ __forceinline__ void walk_round64(const DevGeom& g, const WarpSmem& w
         if (!in_rect(ws.rr[j], sa_a, sa_b)) continue;
         const int id = __float_as_int(ws.ra[j].x);
         const D4 a = g.t64.hole_a[id], b = g.t64.hole_b[id];
-        const double tmp = ray_cyl64_chord(rc, E.xI, E.yI, E.zI, a.x, a.y, a.z, a.w, b.x);
+        double tmp;
+        const D4 S = g.t64.hole_shape ? g.t64.hole_shape[id] : D4{0.0, 0.0, 1.0, 0.0};
+        if (S.x > 0.0)                                          // elliptical hole
+            tmp = ell_chord64(E.xI, E.yI, E.zI, Q.xD, Q.yD, Q.zD, a.x, a.y, a.z, a.w, S.x, S.y, S.z, S.w);
+        else
+            tmp = ray_cyl64_chord(rc, E.xI, E.yI, E.zI, a.x, a.y, a.z, a.w, b.x);
         s.len = s.len + tmp;                                   // :1276-1278
         s.att = s.att + b.y * tmp;
     }

@@ -46,8 +46,8 @@ extern "C" {
 #define SYSMAT_MODE_REFERENCE 0    /* sub-element sum as one float chain in reference order */
 #define SYSMAT_MODE_PRECISE 1      /* sub-element sum accumulated in FP64 */
 /* The reference's element program evaluated in FP64 from the float parameters (geometry,
- * chords, attenuation, exponentials, solid angle); no reference counterpart.  sysmat_pe only,
- * circular holes only. */
+ * chords, attenuation, exponentials, solid angle; elliptical holes included); no reference
+ * counterpart.  Taken by sysmat_pe, sysmat_pe_csr_file and batched launches. */
 #define SYSMAT_MODE_FP64 2
 
 /* Scatter parts (bit mask) and collimator solid-angle models. */

@@ -113,17 +113,52 @@ def test_fp64_blocks_equal_the_full_matrix(gpu):
         assert np.all(blk[:, nv:] == -1.0)
 
 
-def test_fp64_mode_rejects_what_it_does_not_cover(gpu):
-    torch = gpu
-    geo = geometry.mini(seed=16)
-    ctx = sysmat.Context(geo)
+def _elliptical(seed):
+    geo = geometry.mini(seed=seed, rotated=True, layers=2, n_rot=8, nvox=(6, 5, 3), ncry=(5, 4))
     H = geo.n_holes
-    r = geo.collimator[100:100 + 9 * H].reshape(H, 9)[:, 4]
-    ctx.set_hole_shapes(np.stack([r, 0.5 * r, np.zeros(H, np.float32)], 1))
-    out = torch.empty((ctx.n_det, ctx.n_vox), dtype=torch.float32, device="cuda")
-    with pytest.raises(sysmat.SysmatError):                 # no FP64 elliptical chord
-        ctx.pe(out, mode=sysmat.MODE_FP64)
-    ctx.set_hole_shapes(None)
-    ctx.pe(out, mode=sysmat.MODE_FP64)
-    with pytest.raises(sysmat.SysmatError):                 # batched launches take modes 0 and 1
-        sysmat.batch([ctx], [(0, 0.0, 0, ctx.n_det, 0, ctx.n_vox, out)], mode=sysmat.MODE_FP64)
+    rng = np.random.default_rng(seed)
+    r = geo.collimator[100:100 + 9 * H].reshape(H, 9)[:, 4].astype(np.float64)
+    shapes = np.stack([r * rng.uniform(0.5, 1.0, H), r * rng.uniform(0.5, 1.0, H),
+                       rng.uniform(0.0, np.pi, H)], 1).astype(np.float32)
+    shapes[rng.random(H) < 0.2, 0] = 0.0                 # some holes stay circular
+    return geo, shapes
+
+
+def test_fp64_mode_with_elliptical_holes(gpu):
+    """The elliptical chord in double against the FP64 restatement of the reference's
+    length_ellipticalcylinder_ray: the float chord's ill-conditioning is gone."""
+    torch = gpu
+    geo, shapes = _elliptical(18)
+    geo = geo.with_rotation(2)
+    ctx = sysmat.Context(geo)
+    ctx.set_hole_shapes(shapes)
+    a = _fp64(torch, ctx, rotation=2.0)
+    r = rel_err(a, oracle.pe(geo, prec=64, shapes=shapes))
+    assert a.max() > 0
+    assert np.median(r) < 1e-7 and np.mean(r > 1e-7) < 1e-3 and r.max() < TOL, (np.median(r), r.max())
+    ctx.set_hole_shapes(None)                            # back to circles
+    b = _fp64(torch, ctx, rotation=2.0)
+    assert not np.array_equal(a, b)
+    assert rel_err(b, oracle.pe(geo, prec=64)).max() < TOL
+
+
+def test_fp64_batched_launch_equals_single_calls(gpu):
+    """A batch of a circular system, configuration 1 and an elliptical system in FP64."""
+    torch = gpu
+    geo_e, shapes = _elliptical(19)
+    ctxs = [sysmat.Context(geometry.mini(seed=17, rotated=True, layers=2, n_rot=8, nvox=(6, 5, 3), ncry=(5, 4))),
+            sysmat.Context(geometry.config1()), sysmat.Context(geo_e)]
+    ctxs[2].set_hole_shapes(shapes)
+    tasks = [(0, 3.0, 0, ctxs[0].n_det, 0, ctxs[0].n_vox), (1, 0.0, 100, 9, 37, 300), (0, 6.0, 4, 3, 11, 70),
+             (2, 5.0, 0, ctxs[2].n_det, 0, ctxs[2].n_vox)]
+    exp = []
+    for (c, rot, d0, nd, v0, nv) in tasks:
+        exp.append(_fp64(torch, ctxs[c], rotation=rot, det_begin=d0, det_count=nd, vox_begin=v0, vox_count=nv))
+    outs = [torch.full((t[3], t[5]), -1.0, dtype=torch.float32, device="cuda") for t in tasks]
+    plan = sysmat.BatchPlan(ctxs, [t + (o,) for t, o in zip(tasks, outs)])
+    for _ in range(2):                                      # graph capture, then replay
+        plan.run(mode=sysmat.MODE_FP64)
+        torch.cuda.synchronize()
+        for o, e in zip(outs, exp):
+            assert np.array_equal(o.cpu().numpy(), e)
+    plan.close()
