@@ -27,6 +27,10 @@
 //  * the element sum is one float chain in the reference's sub-element order
 //    (SYSMAT_MODE_REFERENCE, the reference's atomicAdd sequence at :1359) or an FP64
 //    accumulation (SYSMAT_MODE_PRECISE); lane 0 writes dst[d][v].
+//
+// Two more instances share the execution plan: the FP64 mode (SYSMAT_MODE_FP64,
+// pe_fp64.cuh: the element program in double, culling in float) and the sampled form
+// (pe_element_sampled: crystal divisions and voxel source points as parameters).
 #include "chord64.cuh"
 #include "geom.cuh"
 #include "pe.cuh"
