@@ -337,18 +337,12 @@ int check_block(const sysmat_ctx* ctx, int det_begin, int det_count, long long v
 }
 }  // namespace sysmat
 
-extern "C" SYSMAT_API int sysmat_pe(sysmat_ctx* ctx, float rotation, int det_begin, int det_count,
-                         long long vox_begin, long long vox_count, float* d_out, long long ld,
-                         int mode, void* stream)
+namespace {
+
+// The launch record of one photoelectric block, with the context's counter and status word.
+PeLaunch pe_block(sysmat_ctx* ctx, float rotation, int det_begin, int det_count, long long vox_begin,
+                  long long vox_count, float* d_out, long long ld)
 {
-    int rc = check_block(ctx, det_begin, det_count, vox_begin, vox_count, d_out, ld);
-    if (rc) return rc;
-    if (mode != SYSMAT_MODE_REFERENCE && mode != SYSMAT_MODE_PRECISE && mode != SYSMAT_MODE_FP64)
-        return SYSMAT_ERR_ARG;
-    if (det_count == 0 || vox_count == 0) return SYSMAT_OK;
-    cudaStream_t s = (cudaStream_t)stream;
-    CUDA_TRY(cudaMemsetAsync(ctx->d_counter, 0, sizeof(unsigned long long), s));
-    CUDA_TRY(cudaMemsetAsync(ctx->d_status, 0, sizeof(int), s));
     PeLaunch L;
     L.det_begin = det_begin;
     L.det_count = det_count;
@@ -360,12 +354,37 @@ extern "C" SYSMAT_API int sysmat_pe(sysmat_ctx* ctx, float rotation, int det_beg
     L.work_counter = ctx->d_counter;
     L.status = ctx->d_status;
     L.counters = nullptr;
-    if (launch_pe(ctx->g, L, mode, ctx->num_sms, s)) return SYSMAT_ERR_CUDA;
+    return L;
+}
+
+// Zero the counter and status word, launch (launch(L) returns non-zero on a launch error),
+// then wait for the status word: SYSMAT_ERR_CAPACITY if an element overflowed a list.
+template <class Launch>
+int run_pe_block(sysmat_ctx* ctx, const PeLaunch& L, cudaStream_t s, Launch&& launch)
+{
+    CUDA_TRY(cudaMemsetAsync(ctx->d_counter, 0, sizeof(unsigned long long), s));
+    CUDA_TRY(cudaMemsetAsync(ctx->d_status, 0, sizeof(int), s));
+    if (launch(L)) return SYSMAT_ERR_CUDA;
     int status = 0;
     CUDA_TRY(cudaMemcpyAsync(&status, ctx->d_status, sizeof(int), cudaMemcpyDeviceToHost, s));
     CUDA_TRY(cudaStreamSynchronize(s));
-    if (status & kStatusCapacity) return SYSMAT_ERR_CAPACITY;
-    return SYSMAT_OK;
+    return (status & kStatusCapacity) ? SYSMAT_ERR_CAPACITY : SYSMAT_OK;
+}
+
+}  // namespace
+
+extern "C" SYSMAT_API int sysmat_pe(sysmat_ctx* ctx, float rotation, int det_begin, int det_count,
+                         long long vox_begin, long long vox_count, float* d_out, long long ld,
+                         int mode, void* stream)
+{
+    int rc = check_block(ctx, det_begin, det_count, vox_begin, vox_count, d_out, ld);
+    if (rc) return rc;
+    if (mode != SYSMAT_MODE_REFERENCE && mode != SYSMAT_MODE_PRECISE && mode != SYSMAT_MODE_FP64)
+        return SYSMAT_ERR_ARG;
+    if (det_count == 0 || vox_count == 0) return SYSMAT_OK;
+    cudaStream_t s = (cudaStream_t)stream;
+    const PeLaunch L = pe_block(ctx, rotation, det_begin, det_count, vox_begin, vox_count, d_out, ld);
+    return run_pe_block(ctx, L, s, [&](const PeLaunch& l) { return launch_pe(ctx->g, l, mode, ctx->num_sms, s); });
 }
 
 extern "C" SYSMAT_API int sysmat_pe_sampled(sysmat_ctx* ctx, float rotation, int det_begin, int det_count,
@@ -387,26 +406,9 @@ extern "C" SYSMAT_API int sysmat_pe_sampled(sysmat_ctx* ctx, float rotation, int
     if (smp.sx * smp.sy * smp.sz > SYSMAT_SAMPLED_MAX_POINTS) return SYSMAT_ERR_ARG;
     if (det_count == 0 || vox_count == 0) return SYSMAT_OK;
     cudaStream_t s = (cudaStream_t)stream;
-    CUDA_TRY(cudaMemsetAsync(ctx->d_counter, 0, sizeof(unsigned long long), s));
-    CUDA_TRY(cudaMemsetAsync(ctx->d_status, 0, sizeof(int), s));
-    PeLaunch L;
-    L.det_begin = det_begin;
-    L.det_count = det_count;
-    L.vox_begin = vox_begin;
-    L.vox_count = vox_count;
-    L.ld = ld;
-    L.rotation = rotation;
-    L.out = d_out;
-    L.work_counter = ctx->d_counter;
-    L.status = ctx->d_status;
-    L.counters = nullptr;
+    PeLaunch L = pe_block(ctx, rotation, det_begin, det_count, vox_begin, vox_count, d_out, ld);
     L.smp = smp;
-    if (launch_pe_sampled(ctx->g, L, ctx->num_sms, s)) return SYSMAT_ERR_CUDA;
-    int status = 0;
-    CUDA_TRY(cudaMemcpyAsync(&status, ctx->d_status, sizeof(int), cudaMemcpyDeviceToHost, s));
-    CUDA_TRY(cudaStreamSynchronize(s));
-    if (status & kStatusCapacity) return SYSMAT_ERR_CAPACITY;
-    return SYSMAT_OK;
+    return run_pe_block(ctx, L, s, [&](const PeLaunch& l) { return launch_pe_sampled(ctx->g, l, ctx->num_sms, s); });
 }
 
 extern "C" SYSMAT_API long long sysmat_bitmap_crystal_words(const sysmat_ctx* ctx)
@@ -536,16 +538,7 @@ extern "C" SYSMAT_API int sysmat_pe_work(sysmat_ctx* ctx, float rotation, int de
     unsigned long long* d_cnt = nullptr;
     if (cudaMalloc(&d_cnt, 16 * sizeof(unsigned long long)) != cudaSuccess) return SYSMAT_ERR_NOMEM;
     cudaStream_t s = (cudaStream_t)stream;
-    PeLaunch L;
-    L.det_begin = det_begin;
-    L.det_count = det_count;
-    L.vox_begin = vox_begin;
-    L.vox_count = vox_count;
-    L.ld = ld;
-    L.rotation = rotation;
-    L.out = d_out;
-    L.work_counter = ctx->d_counter;
-    L.status = ctx->d_status;
+    PeLaunch L = pe_block(ctx, rotation, det_begin, det_count, vox_begin, vox_count, d_out, ld);
     L.counters = d_cnt;
     rc = SYSMAT_OK;
     if (cudaMemsetAsync(d_cnt, 0, 16 * sizeof(unsigned long long), s) != cudaSuccess ||
