@@ -55,13 +55,22 @@ class Projector:
             self._theta = theta.copy()
         return self._ctx
 
-    def project(self, x, theta=None):
-        return self.context(theta).project(x, rotation=self.rotation, det_begin=self.det_begin,
-                                           det_count=self.det_count)
+    def project(self, x, theta=None, rows=None):
+        """A x over the projector's rows, or over rows = (first, count) relative to them."""
+        b, n = self._rows(rows)
+        return self.context(theta).project(x, rotation=self.rotation, det_begin=b, det_count=n)
 
-    def backproject(self, u, theta=None):
-        return self.context(theta).backproject(u, rotation=self.rotation, det_begin=self.det_begin,
-                                               det_count=self.det_count)
+    def backproject(self, u, theta=None, rows=None):
+        b, n = self._rows(rows)
+        return self.context(theta).backproject(u, rotation=self.rotation, det_begin=b, det_count=n)
+
+    def _rows(self, rows):
+        if rows is None:
+            return self.det_begin, self.det_count
+        first, count = rows
+        if first < 0 or count < 0 or first + count > self.det_count:
+            raise ValueError("rows outside the projector's detector rows")
+        return self.det_begin + first, count
 
     def vjp(self, x, u, theta=None):
         return self.context(theta).vjp(x, u, rotation=self.rotation, det_begin=self.det_begin,
@@ -137,6 +146,29 @@ class Projection(torch.autograd.Function):
 
 def project(theta, x, projector):
     return Projection.apply(theta, x, projector)
+
+
+def osem(projector, y, n_iter, n_subsets, x0=None, theta=None):
+    """OSEM: the MLEM update applied subset by subset, the subsets being contiguous blocks
+    of the projector's detector rows (sharding.detector_slab); n_subsets = 1 is mlem.
+    y: CUDA tensor of the projector's detector rows; returns a float32 CUDA tensor of n_vox.
+    One iteration visits every subset once, in order."""
+    dev = y.device
+    n_rows = projector.det_count
+    subsets = [sharding.detector_slab(n_rows, s, n_subsets) for s in range(n_subsets)]
+    subsets = [r for r in subsets if r[1] > 0]
+    sens = [projector.backproject(torch.ones(n, dtype=torch.float32, device=dev), theta, rows=(b, n))
+            for b, n in subsets]
+    x = torch.ones(projector.geo.n_vox, dtype=torch.float32, device=dev) if x0 is None else x0.clone()
+    yd = y.to(torch.float64)
+    for _ in range(n_iter):
+        for (b, n), sn in zip(subsets, sens):
+            p = projector.project(x, theta, rows=(b, n))
+            ys = yd[b:b + n]
+            ratio = torch.where(p > 0, ys / p, torch.zeros_like(p)).to(torch.float32)
+            bp = projector.backproject(ratio, theta, rows=(b, n))
+            x = torch.where(sn > 0, x.to(torch.float64) * bp / sn, torch.zeros_like(sn)).to(torch.float32)
+    return x
 
 
 def mlem(projector, y, n_iter, x0=None, theta=None):
