@@ -77,6 +77,58 @@ class Projector:
                                        det_count=self.det_count)
 
 
+class RotationProjector:
+    """All rotations of one system as one projector: its rows are (rotation, detector) pairs,
+    rotation-major, as the reference's matrix stacks them (A[rotation][detector][voxel]).
+    project / backproject / vjp accept any block of rows (rows = (first, count)); a block that
+    spans rotations is split into one device call per rotation, and back projections and
+    gradients are summed over them.  OSEM with n_subsets = the number of rotations takes one
+    rotation per subset.
+
+    `context(theta)` may be given to supply the per-theta device context (an object with the
+    sysmat.Context project / backproject / vjp methods); by default a Projector's is used."""
+
+    def __init__(self, geo, rotations=None, device=0, context=None):
+        self.geo = geo
+        self.rotations = [float(r) for r in (range(geo.n_rot) if rotations is None else rotations)]
+        self.n_det = geo.n_det
+        self.det_count = len(self.rotations) * self.n_det
+        self._context = context if context is not None else Projector(geo, device=device).context
+
+    def _pieces(self, rows):
+        first, count = (0, self.det_count) if rows is None else rows
+        if first < 0 or count < 0 or first + count > self.det_count:
+            raise ValueError("rows outside the projector's rows")
+        pos, end, out = first, first + count, []
+        while pos < end:
+            r, d0 = divmod(pos, self.n_det)
+            n = min(self.n_det - d0, end - pos)
+            out.append((self.rotations[r], d0, n, pos - first))
+            pos += n
+        return out
+
+    def project(self, x, theta=None, rows=None):
+        ctx = self._context(theta)
+        return torch.cat([ctx.project(x, rotation=rot, det_begin=d0, det_count=n)
+                          for rot, d0, n, _ in self._pieces(rows)])
+
+    def backproject(self, u, theta=None, rows=None):
+        ctx = self._context(theta)
+        q = None
+        for rot, d0, n, off in self._pieces(rows):
+            part = ctx.backproject(u[off:off + n].contiguous(), rotation=rot, det_begin=d0, det_count=n)
+            q = part if q is None else q + part
+        return q
+
+    def vjp(self, x, u, theta=None):
+        ctx = self._context(theta)
+        g = None
+        for rot, d0, n, off in self._pieces(None):
+            part = ctx.vjp(x, u[off:off + n].contiguous(), rotation=rot, det_begin=d0, det_count=n)
+            g = part if g is None else g + part
+        return g
+
+
 class ShardedProjector:
     """A projector whose detector rows are split across the ranks of a process group
     (sharding.detector_slab), one GPU per rank.  Each rank recomputes only its own rows of A.

@@ -1,4 +1,5 @@
-"""CPU tests of OSEM and MLEM (adjoint.osem / adjoint.mlem) on a dense stand-in projector.
+"""CPU tests of OSEM and MLEM (adjoint.osem / adjoint.mlem) and of the all-rotations
+projector (adjoint.RotationProjector) on dense stand-ins.
 
 Both functions only call the projector's project / backproject (over row blocks for OSEM),
 which on a GPU are sysmat_project / sysmat_backproject (tested against the dense matrix in
@@ -90,3 +91,66 @@ def test_osem_raises_the_likelihood_faster_than_mlem():
         return float((p - y * np.log(np.maximum(p, 1e-300))).sum())
 
     assert nll(adjoint.osem(P, yt, 1, 4).numpy()) <= nll(adjoint.mlem(P, yt, 2).numpy())
+
+
+# ---- all rotations as one projector (adjoint.RotationProjector) -------------------------
+
+R = 3
+
+
+class DenseContext:
+    """sysmat.Context's projection methods over dense per-rotation matrices A[r] (and
+    derivative matrices dA[r, i] for the VJP)."""
+
+    def __init__(self, A, dA):
+        import torch
+        self.A, self.dA = torch.from_numpy(A), torch.from_numpy(dA)
+
+    def project(self, x, rotation, det_begin, det_count):
+        return self.A[int(rotation), det_begin:det_begin + det_count] @ x.double()
+
+    def backproject(self, u, rotation, det_begin, det_count):
+        return self.A[int(rotation), det_begin:det_begin + det_count].T @ u.double()
+
+    def vjp(self, x, u, rotation, det_begin, det_count):
+        import torch
+        r, rows = int(rotation), slice(det_begin, det_begin + det_count)
+        u, x = u.double(), x.double()
+        return torch.stack([u @ (self.dA[r, i, rows] @ x) for i in range(7)] + [u @ (self.A[r, rows] @ x)])
+
+
+def _rotations():
+    rng = np.random.default_rng(29)
+    A = rng.uniform(0.0, 1.0, (R, D, V))
+    A[rng.random((R, D, V)) < 0.4] = 0.0
+    dA = rng.normal(size=(R, 7, D, V))
+    geo = types.SimpleNamespace(n_det=D, n_vox=V, n_rot=R)
+    return A, dA, adjoint.RotationProjector(geo, context=lambda theta: DenseContext(A, dA))
+
+
+def test_rotation_projector_stacks_rotations():
+    import torch
+    A, dA, P = _rotations()
+    rng = np.random.default_rng(1)
+    x = torch.from_numpy(rng.uniform(0.5, 2.0, V).astype(np.float32))
+    u = torch.from_numpy(rng.normal(size=R * D).astype(np.float32))
+    stacked = A.reshape(R * D, V)
+    assert P.det_count == R * D
+    assert np.allclose(P.project(x).numpy(), stacked @ x.numpy(), rtol=1e-12)
+    assert np.allclose(P.backproject(u).numpy(), stacked.T @ u.numpy(), rtol=1e-12)
+    b, n = D - 5, D + 9                                   # spans all three rotations
+    assert np.allclose(P.project(x, rows=(b, n)).numpy(), stacked[b:b + n] @ x.numpy(), rtol=1e-12)
+    assert np.allclose(P.backproject(u[:n], rows=(b, n)).numpy(), stacked[b:b + n].T @ u[:n].numpy(), rtol=1e-12)
+    g = P.vjp(x, u).numpy()
+    uu = u.numpy().astype(np.float64).reshape(R, D)
+    ref = [sum(uu[r] @ dA[r, i] @ x.numpy() for r in range(R)) for i in range(7)]
+    assert np.allclose(g[:7], ref, rtol=1e-10) and np.isclose(g[7], u.numpy() @ stacked @ x.numpy(), rtol=1e-10)
+
+
+def test_osem_by_rotation_matches_numpy():
+    import torch
+    A, _, P = _rotations()
+    stacked = A.reshape(R * D, V)
+    y = np.random.default_rng(2).poisson(stacked @ np.full(V, 2.0) * 30.0) / 30.0
+    x = adjoint.osem(P, torch.from_numpy(y), 3, R).numpy()
+    assert np.allclose(x, _numpy_osem(stacked, y, 3, R), rtol=1e-6, atol=0)   # one rotation per subset
