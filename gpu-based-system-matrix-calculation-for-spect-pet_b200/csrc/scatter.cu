@@ -64,67 +64,6 @@ __device__ __forceinline__ float dist3(float x1, float y1, float z1, float x2, f
     return sqrtf((x1 - x2) * (x1 - x2) + (y1 - y2) * (y1 - y2) + (z1 - z2) * (z1 - z2));
 }
 
-// Klein-Nishina shape times sin(theta), and its derivative, in float.
-__device__ __forceinline__ float kn_f(float th, float alpha)
-{
-    float s, c;
-    sincosf(th, &s, &c);
-    const float f1 = alpha * (1.0f - c);
-    const float f2 = 1.0f + c * c;
-    const float p = 1.0f + f1;
-    return f2 / p / p * (1.0f + f1 * f1 / f2 / p) * s;
-}
-
-__device__ __forceinline__ float kn_fprime(float th, float alpha)
-{
-    float s, c;
-    sincosf(th, &s, &c);
-    const float om = 1.0f - c;
-    const float p = 1.0f + alpha * om;
-    const float ip = 1.0f / p;
-    const float ip2 = ip * ip, ip3 = ip2 * ip, ip4 = ip3 * ip;
-    const float g = (1.0f + c * c) * ip2 + alpha * alpha * om * om * ip3;
-    const float gp = 2.0f * c * ip2 + 2.0f * alpha * (1.0f + c * c) * ip3 -
-                     2.0f * alpha * alpha * om * ip3 + 3.0f * alpha * alpha * alpha * om * om * ip4;
-    return c * g - s * s * gp;
-}
-
-// Reference Riemann sum with n + 1 terms starting at a, step 0.01f, via Euler-Maclaurin.
-// The integral uses Gauss-Legendre panels: 4 points up to 0.3 rad, else 8-point panels no
-// wider than 0.8 rad (relative error below 1e-10 in exact arithmetic; the float
-// evaluation error, ~1e-7, dominates).
-__device__ float kn_sum(float a, int n, float alpha)
-{
-    const float h = 0.01f;
-    const float b = a + (float)n * h;
-    const float fa = kn_f(a, alpha), fb = kn_f(b, alpha);
-    float integral = 0.0f;
-    if (n > 0 && (b - a) <= 0.3f) {
-        const float x4[2] = {0.3399810435848563f, 0.8611363115940526f};
-        const float w4[2] = {0.6521451548625461f, 0.3478548451374538f};
-        const float half = 0.5f * (b - a), mid = a + half;
-        integral = half * (w4[0] * (kn_f(mid - half * x4[0], alpha) + kn_f(mid + half * x4[0], alpha)) +
-                           w4[1] * (kn_f(mid - half * x4[1], alpha) + kn_f(mid + half * x4[1], alpha)));
-    } else if (n > 0) {
-        const float xg[4] = {0.1834346424956498f, 0.5255324099163290f, 0.7966664774136267f,
-                             0.9602898564975363f};
-        const float wg[4] = {0.3626837833783620f, 0.3137066458778873f, 0.2223810344533745f,
-                             0.1012285362903763f};
-        const int panels = (int)ceilf((b - a) * 1.25f);
-        const float width = (b - a) / (float)panels;
-        for (int p = 0; p < panels; ++p) {
-            const float lo = a + (float)p * width;
-            const float half = 0.5f * width, mid = lo + half;
-            float acc = 0.0f;
-#pragma unroll
-            for (int k = 0; k < 4; ++k)
-                acc += wg[k] * (kn_f(mid - half * xg[k], alpha) + kn_f(mid + half * xg[k], alpha));
-            integral += half * acc;
-        }
-    }
-    return integral + 0.5f * h * (fa + fb) + (h * h / 12.0f) * (kn_fprime(b, alpha) - kn_fprime(a, alpha));
-}
-
 // Reference Riemann sum with n + 1 terms from a, step 0.01f, in FP64 from the table:
 //   sum = G(b) - G(a) + h/2 (F(a) + F(b)) + h^2/12 (F'(b) - F'(a)),  b = a + n h,
 // G and F by cubic Hermite interpolation on the table (error ~1e-14), F' linearly.
