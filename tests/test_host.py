@@ -126,7 +126,30 @@ def test_reference_entry_points_reject_null_buffers():
     assert lib.scatter_crystal(null, null, null, null, None, null, 0) == -1
 
 
-# ---- multi-rank partitioning (gloo, world_size 2) ----------------------------------------
+def test_native_entry_points_reject_a_null_context():
+    """Every handle entry point answers SYSMAT_ERR_ARG for a null context or plan before any
+    device call (no GPU here)."""
+    import ctypes
+    lib = sysmat.lib()
+    div = (ctypes.c_int * 3)(4, 4, 4)
+    sub = (ctypes.c_int * 3)(1, 1, 1)
+    cnt = (ctypes.c_ulonglong * 12)()
+    calls = {
+        "sysmat_pe": lambda: lib.sysmat_pe(None, 0.0, 0, 1, 0, 1, None, 1, 0, None),
+        "sysmat_pe_sampled": lambda: lib.sysmat_pe_sampled(None, 0.0, 0, 1, 0, 1, div, sub, None, 1, None),
+        "sysmat_pe_work": lambda: lib.sysmat_pe_work(None, 0.0, 0, 1, 0, 1, None, 1, cnt, None),
+        "sysmat_scatter": lambda: lib.sysmat_scatter(None, 3, 0, 0.0, None, 0, 1, 0, 1, None, 1, None),
+        "sysmat_scatter_prepare": lambda: lib.sysmat_scatter_prepare(None, 3, None, None, None),
+        "sysmat_scatter_prepare_native": lambda: lib.sysmat_scatter_prepare_native(None, 3, None, None),
+        "sysmat_set_hole_shapes": lambda: lib.sysmat_set_hole_shapes(None, None, None, None),
+        "sysmat_pe_csr_file": lambda: lib.sysmat_pe_csr_file(None, 0.0, b"x", 0.0, 0, 0, None, None),
+        "sysmat_project": lambda: lib.sysmat_project(None, 0.0, 0, 1, None, None, None),
+        "sysmat_backproject": lambda: lib.sysmat_backproject(None, 0.0, 0, 1, None, None, None),
+        "sysmat_vjp": lambda: lib.sysmat_vjp(None, 0.0, 0, 1, None, None, None, None),
+        "sysmat_batch_run": lambda: lib.sysmat_batch_run(None, 0, None),
+    }
+    for name, call in calls.items():
+        assert call() == -1, name
 
 def test_detector_slabs_cover_rows_once():
     for n, w in ((4096, 2), (4096, 8), (1023, 4), (3, 8)):
