@@ -27,7 +27,6 @@ bounded sample of the same workload; the reference has no CPU implementation.
 from __future__ import annotations
 
 import argparse
-import ctypes
 import importlib.util
 import json
 import os

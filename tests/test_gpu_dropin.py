@@ -9,7 +9,7 @@ import subprocess
 import numpy as np
 import pytest
 
-from conftest import ROOT, TOL, geometry, rel_err, sysmat
+from conftest import ROOT, geometry, sysmat
 
 pytestmark = pytest.mark.gpu
 

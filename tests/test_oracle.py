@@ -6,7 +6,7 @@ import math
 import numpy as np
 import pytest
 
-from conftest import TOL, geometry, golden, oracle, rel_err
+from conftest import geometry, golden, oracle, rel_err
 
 
 # ---- threshold semantics -------------------------------------------------------------

@@ -10,7 +10,6 @@ import socket
 import types
 
 import numpy as np
-import pytest
 
 from conftest import PKG_DIR, _load
 
