@@ -22,6 +22,8 @@
 #include <cstring>
 #include <mutex>
 
+#include <cuda.h>
+
 #include "../../include/sysmat.h"
 #include "geom.cuh"
 #include "pe.cuh"
@@ -52,21 +54,47 @@ constexpr size_t kScratchBytes = kOffStatus + 256;
 
 static __device__ __align__(256) unsigned char g_pe_scratch[kScratchBytes];
 
-// Device address of g_pe_scratch per device (set up once, with that device current).
+// Device address of g_pe_scratch per device, with the CUDA context it was looked up in.
+// A symbol's address belongs to one context: after cudaDeviceReset, or when the caller makes
+// another (non-primary) context current on the same device, the address is looked up again.
 std::mutex g_setup_mu;
-unsigned char* g_scratch_ptr[64] = {};
+struct ScratchSlot {
+    CUcontext ctx;
+    unsigned char* ptr;
+};
+ScratchSlot g_scratch[64] = {};
+using CtxGetCurrentFn = CUresult (*)(CUcontext*);
+CtxGetCurrentFn g_ctx_get_current = nullptr;
+
+int current_context(CUcontext* ctx)
+{
+    if (!g_ctx_get_current) {
+        void* fn = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &fn, cudaEnableDefault, &q) != cudaSuccess ||
+            q != cudaDriverEntryPointSuccess || !fn)
+            return SYSMAT_ERR_CUDA;
+        g_ctx_get_current = reinterpret_cast<CtxGetCurrentFn>(fn);
+    }
+    return g_ctx_get_current(ctx) == CUDA_SUCCESS ? SYSMAT_OK : SYSMAT_ERR_CUDA;
+}
 
 int scratch_for_current_device(unsigned char** out)
 {
     int dev = -1;
     if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return SYSMAT_ERR_CUDA;
     std::lock_guard<std::mutex> lock(g_setup_mu);
-    if (!g_scratch_ptr[dev]) {
+    CUcontext ctx = nullptr;
+    if (current_context(&ctx)) return SYSMAT_ERR_CUDA;
+    if (!ctx || !g_scratch[dev].ptr || g_scratch[dev].ctx != ctx) {
+        // the lookup also binds the runtime's context when this thread has none yet
         void* p = nullptr;
         if (cudaGetSymbolAddress(&p, g_pe_scratch) != cudaSuccess || !p) return SYSMAT_ERR_CUDA;
-        g_scratch_ptr[dev] = static_cast<unsigned char*>(p);
+        if (current_context(&ctx) || !ctx) return SYSMAT_ERR_CUDA;
+        g_scratch[dev].ctx = ctx;
+        g_scratch[dev].ptr = static_cast<unsigned char*>(p);
     }
-    *out = g_scratch_ptr[dev];
+    *out = g_scratch[dev].ptr;
     return SYSMAT_OK;
 }
 

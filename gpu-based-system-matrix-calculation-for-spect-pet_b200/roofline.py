@@ -24,15 +24,15 @@ per-hit terms for the non-zero chords counted by the kernel (sysmat_pe_work).
 """
 from __future__ import annotations
 
-import os
-import re
-
 BOX_FLOPS, BOX_MUFU = 25, 4
 CYL_HIT_FLOPS, CYL_HIT_MUFU = 61, 11
 CRY_HIT_FLOPS, CRY_HIT_MUFU = 45, 4
 SUB_FLOPS, SUB_MUFU = 104, 9
 
-PROFILES = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "profiles")
+# DRAM traffic of one pe_kernel launch, from one ncu capture (dram__bytes_read.sum +
+# dram__bytes_write.sum) of a configuration-2 launch whose output block exceeds L2, so the
+# matrix writes reach DRAM inside the captured launch.  None until such a capture exists.
+PE_DRAM_CAPTURE = None
 
 
 def pe_work(counts: dict, n_layers: int) -> tuple[float, float]:
@@ -46,11 +46,14 @@ def pe_work(counts: dict, n_layers: int) -> tuple[float, float]:
     return float(flops), float(mufu)
 
 
-def measured_traffic(kernel: str, workload: str):
-    """DRAM bytes per launch from the committed ncu summary profiles/<kernel>_<workload>.md
-    (line `dram_bytes_per_launch: N`), or None when no capture was summarised."""
-    path = os.path.join(PROFILES, f"{kernel}_{workload}.md")
-    if not os.path.exists(path):
+def pe_traffic_per_launch(elements: int):
+    """DRAM bytes of a pe_kernel launch over `elements` output elements: the captured launch's
+    bytes scaled by its element count (the kernel's DRAM traffic is its output plus the
+    L2-resident tables, so it grows with the elements), with the capture it came from; None
+    without a capture."""
+    cap = PE_DRAM_CAPTURE
+    if not cap:
         return None
-    m = re.search(r"dram_bytes_per_launch:\s*([0-9.eE+]+)", open(path).read())
-    return float(m.group(1)) if m else None
+    return {"bytes": cap["bytes"] * elements / cap["elements"],
+            "source": f"ncu capture ({cap['command']}): {cap['bytes']:.4g} DRAM bytes over "
+                      f"{cap['elements']} elements, scaled to {elements} elements"}

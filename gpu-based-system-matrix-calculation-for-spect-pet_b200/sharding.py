@@ -9,10 +9,13 @@ from __future__ import annotations
 
 
 def plane_for_step(step: int, rank: int, world: int, n_planes: int, first: int = 0) -> int:
-    """z-plane processed by `rank` at `step`: ranks take interleaved planes so per-rank work
-    is fixed as the world grows (weak scaling) and no two ranks of a step share a plane
-    while step * world + rank < n_planes."""
-    return first + (step * world + rank) % n_planes
+    """z-plane processed by `rank` at `step`: ranks take interleaved planes starting at
+    `first` and wrapping around the image, so every plane lies in [0, n_planes), per-rank work
+    is fixed as the world grows (weak scaling) and the ranks of one step take distinct planes
+    whenever world <= n_planes."""
+    if n_planes < 1:
+        raise ValueError("n_planes must be positive")
+    return (first + step * world + rank) % n_planes
 
 
 def detector_slab(n_det: int, rank: int, world: int) -> tuple[int, int]:

@@ -486,7 +486,8 @@ def pe_noalloc(geo, out, rotation=0.0, det_begin=0, det_count=None, vox_begin=0,
     """Photoelectric block through sysmat_pe_noalloc (no device allocation; host parameter
     arrays, `out` a CUDA float32 tensor).  Returns `out`."""
     (c, pc), (d, pd), (i, pi) = _f32(geo.collimator), _f32(geo.detector), _f32(geo.image)
-    n_det = int(np.floor(float(geo.detector[0]) + 1e-4))
+    # the crystal count as the library decodes it: floor(pD[0] + 1e-6) in float32
+    n_det = int(np.floor(np.float32(geo.detector[0]) + np.float32(0.000001)))
     n_vox = geo.n_vox
     det_count = n_det - det_begin if det_count is None else det_count
     vox_count = n_vox - vox_begin if vox_count is None else vox_count

@@ -4,8 +4,9 @@
  *
  * 1. Reference-compatible entry points.  Same names (where C allows), same argument
  *    meaning, same host-buffer ownership and output layout as the reference programs.
- *    A reference CLI re-linked against libsysmat.so runs unchanged (see
- *    include/sysmat_compat.hpp for the C++ overloads of `scatter`).
+ *    A reference CLI re-linked against libsysmat.so runs unchanged: the C++-mangled
+ *    names it links against (PESysMatGen and the three `scatter` overloads) are exported
+ *    by csrc/cxx_abi.cpp of the package as aliases of the C entry points below.
  *
  * 2. A native, handle-based API on device pointers and a caller-supplied CUDA stream,
  *    used by the reference-compatible layer, the tests and the benchmark.  It never
@@ -263,8 +264,10 @@ SYSMAT_API int sysmat_backproject(sysmat_ctx* ctx, float rotation, int det_begin
  * tables, work counter and status word live in a static device array of about 1.6 MB
  * (each GPU that loads the library holds it until exit), limited to 6666 crystals and 8877
  * holes (larger systems return SYSMAT_ERR_CAPACITY).  The first call on a device looks
- * up that array's device address and should come before any stream capture.  Calls
- * share the array: calls that overlap on the GPU race.  Synchronous on `stream`. */
+ * up that array's device address and should come before any stream capture; the address
+ * is looked up again when the current CUDA context of the device changes (after
+ * cudaDeviceReset, or under another context the caller made current).  Calls share the
+ * array: calls that overlap on the GPU race.  Synchronous on `stream`. */
 SYSMAT_API int sysmat_pe_noalloc(const float* pC, const float* pD, const float* pI, float rotation,
                                  int det_begin, int det_count, long long vox_begin,
                                  long long vox_count, float* d_out, long long ld, int mode,

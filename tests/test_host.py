@@ -167,6 +167,24 @@ def test_plane_assignment_is_disjoint_within_a_step():
             assert len(set(planes)) == world
 
 
+def test_planes_stay_in_the_image_for_long_runs():
+    """A bench run of warm-up + timed steps longer than the image has planes (the 25 steps of
+    a 5 + 20 run on 32 planes starting at plane 16, and longer) wraps around the image
+    instead of running past its last plane."""
+    for n_planes in (1, 16, 32):
+        for first in (0, n_planes // 2, n_planes - 1):
+            for world in (1, 2, 8):
+                for step in range(64):
+                    planes = [sharding.plane_for_step(step, r, world, n_planes, first)
+                              for r in range(world)]
+                    assert all(0 <= p < n_planes for p in planes)
+                    if world <= n_planes:
+                        assert len(set(planes)) == world
+    # consecutive steps of one rank walk the image from `first`
+    assert [sharding.plane_for_step(s, 0, 1, 32, 16) for s in range(18)] == \
+        list(range(16, 32)) + [0, 1]
+
+
 def _gloo_worker(rank, world, port, q):
     import torch
     import torch.distributed as dist
