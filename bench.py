@@ -19,10 +19,12 @@ FP32 twin's rate on the same sample beside it, `accuracy` = max / median relativ
 every matrix below against the FP64 oracle on samples, `scatter` = the primary-Compton
 rate on a configuration-3 plane (kernel, pair-table preparation, and end to end through
 the reference-compatible scatter() with host buffers and bitmap files), `scatter_config2` =
-the same on a configuration-2 voxel row, `batch` = the configuration-4 design sweep in one
+the same on a configuration-2 voxel row, `scatter_grid` = configuration 3 as stated (scatter
+points on a 0.25 mm grid inside the crystals and the tungsten, FP64 sums), `batch` = the configuration-4 design sweep in one
 batched launch against one launch per task, `sampled` = configuration 2 with the sampling it
 states (2x2x2 voxel sub-samples, 2x8x2 crystal sub-elements), `fp64` = the FP64 mode (the
-element program in double) on the headline plane.
+element program in double) on the headline plane, `local` = the local-coordinate FP32 mode
+(within 1e-5 of FP64) on the same plane.
 
 `--impl reference` times the reference's own CUDA program (its source compiled for sm_100a
 by oracle/Makefile into oracle/_ref) through its own host entry points (PESysMatGen,
@@ -331,17 +333,24 @@ def run_sysmat(args, rank, world, local):
         e2e = run_e2e(args, sysmat, g, rank, world, n_planes, first)
 
     legs = {}
+    if world > 1 and not args.no_scatter:
+        legs["scatter_columns"] = run_scatter_columns(args, sysmat, torch, rank, world)
     if world == 1:
         if not args.no_scatter:
             legs["scatter"] = run_scatter(args, sysmat, torch, keep)
         if not args.no_scatter2:
             legs["scatter_config2"] = run_scatter_config2(args, sysmat, torch)
+        if not args.no_grid:
+            legs["scatter_grid"] = run_scatter_grid(args, sysmat, torch, keep)
         if not args.no_batch:
             legs["batch"] = run_batch(args, sysmat, torch)
+            legs["batch_scatter"] = run_batch_scatter(args, sysmat, torch)
         if not args.no_sampled:
             legs["sampled"] = run_sampled(args, sysmat, torch, keep)
         if not args.no_fp64:
             legs["fp64"] = run_fp64(args, sysmat, torch, keep)
+        if not args.no_local:
+            legs["local"] = run_local(args, sysmat, torch, keep)
 
     result = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
@@ -463,6 +472,50 @@ def run_scatter(args, sysmat, torch, keep):
     return res
 
 
+def run_scatter_grid(args, sysmat, torch, keep):
+    """Configuration 3 as stated: primary Compton scatter with scatter points on a 0.25 mm grid
+    inside the crystals (1024 x 8 x 24 x 8 cells) and the tungsten (256 x 40 x 256 cells of the
+    plate, minus the holes), FP64 sums per element (sysmat_scatter_grid).  Voxel row 24 of
+    z-plane 8 (48 voxels) x 1024 crystals per step; one untimed step, one timed."""
+    g = geometry.voxel_slab(geometry.config3(), 8, 24, 1)
+    ctx = sysmat.Context(g)
+    out = torch.empty((ctx.n_det, ctx.n_vox), dtype=torch.float32, device="cuda")
+    ctx.scatter_grid(out, cell=0.25)
+    ms = _events(torch, lambda: ctx.scatter_grid(out, cell=0.25))
+    keep["scatter_grid"] = {"geo": g, "out": out.cpu().numpy()}
+    nel = ctx.n_det * ctx.n_vox
+    ctx.close()
+    return {"value": nel / (ms * 1e-3), "unit": UNIT, "ms_per_step": ms, "summation": "FP64 per element",
+            "workload": "config3 grid scatter: scatter points on a 0.25 mm grid inside the crystals and the "
+                        f"collimator's tungsten; voxel row 24 of z-plane 8 x 1024 crystals ({nel} elements)"}
+
+
+def run_scatter_columns(args, sysmat, torch, rank, world):
+    """Configuration 3, z-plane 8 (1024 crystals x 2304 voxels, crystal + collimator parts),
+    split across ranks by voxel columns (sharding.voxel_block): each rank computes the PE
+    columns its scatter columns read, so the ranks exchange nothing (strong scaling of one
+    plane; device time, max over ranks)."""
+    g = geometry.voxel_slab(geometry.config3(), 8)
+    ctx = sysmat.Context(g)
+    ctx.scatter_prepare(ctx.bitmap_crystal(), ctx.bitmap_collimator())
+    v0, nv = sharding.voxel_block(ctx.n_vox, rank, world)
+    pe = torch.zeros((ctx.n_det, ctx.n_vox), dtype=torch.float32, device="cuda")
+    out = torch.empty((ctx.n_det, nv), dtype=torch.float32, device="cuda")
+
+    def step():
+        ctx.scatter_columns(out, v0, nv, pe=pe)
+
+    step()
+    torch.cuda.synchronize()
+    barrier(world)
+    ms = max_over_ranks(_events(torch, step, n=2), world)
+    ctx.close()
+    nel = ctx.n_det * ctx.n_vox
+    return {"value": nel / (ms * 1e-3), "unit": UNIT, "ms_per_step": ms, "scaling": "strong",
+            "workload": f"config3 z-plane 8 ({nel} elements) PE columns + crystal and collimator scatter, voxel "
+                        f"columns split over {world} ranks, no exchange"}
+
+
 def config2_scatter_slab():
     """Configuration 2 scatter sample: voxel row iy = 48 of z-plane 16 (96 voxels) x 4096
     crystals, 2304 layer-0 holes."""
@@ -554,6 +607,28 @@ def run_fp64(args, sysmat, torch, keep):
             "workload": f"config2 PE in FP64: crystals {d0}..{d0 + D - 1} x z-plane 16 ({D * nxy} elements)"}
 
 
+def run_local(args, sysmat, torch, keep):
+    """Local-coordinate FP32 mode (the reference's element program in float arithmetic that
+    stays within 1e-5 of its FP64 evaluation) on z-plane 16 of configuration 2, all 4096
+    crystals, reference sampling; one untimed step, two timed."""
+    g = geometry.config2()
+    ctx = sysmat.Context(g)
+    nxy = int(g.image[0]) * int(g.image[1])
+    out = torch.empty((ctx.n_det, nxy), dtype=torch.float32, device="cuda")
+
+    def step():
+        ctx.pe(out, vox_begin=16 * nxy, vox_count=nxy, mode=sysmat.MODE_LOCAL)
+
+    step()
+    ms = _events(torch, step, n=2)
+    nx = int(g.image[0])
+    keep["local"] = {"d0": 0, "out": out[:, SAMPLE_ROW * nx:(SAMPLE_ROW + 1) * nx].cpu().numpy()}
+    ctx.close()
+    return {"value": ctx.n_det * nxy / (ms * 1e-3), "unit": UNIT, "ms_per_step": ms, "arithmetic": "f32 (local)",
+            "workload": f"config2 PE, local-coordinate FP32 mode: all crystals x z-plane 16 ({ctx.n_det * nxy} "
+                        "elements)"}
+
+
 def run_batch(args, sysmat, torch, n_instances=64, rows=8, sweep=True):
     """Design sweep of configuration 4: every instance x every one of its rotations, each task
     a block of `rows` crystals (centre of the 32x32 array) x one z-plane (1024 voxels).  The
@@ -600,6 +675,52 @@ def run_batch(args, sysmat, torch, n_instances=64, rows=8, sweep=True):
                         f"(1024 voxels)"}
 
 
+def run_batch_scatter(args, sysmat, torch, n_instances=16, n_rot=4, rows=8):
+    """Batched scatter on a configuration-4 design sweep: n_instances seeded collimators x their
+    first n_rot rotations, each task the crystal + collimator scatter of `rows` crystals (centre
+    of the 32x32 array) x z-plane 8 (1024 voxels), reading that rotation's PE columns.  One
+    persistent launch (replayed as a CUDA graph) against one sysmat_scatter launch per task,
+    same outputs.  Pair tables and PE matrices are built outside the timed region."""
+    geos = geometry.config4(n_instances=n_instances)
+    ctxs = [sysmat.Context(gg) for gg in geos]
+    d0, v0, nv = 16 * 32 + 16 - rows // 2, 1024 * 8, 1024
+    items, pes = [], []
+    for k, ctx in enumerate(ctxs):
+        bc, bh = ctx.bitmap_crystal(), ctx.bitmap_collimator()
+        ctx.scatter_prepare(bc, bh)
+        del bc, bh
+        for r in range(min(n_rot, geos[k].n_rot)):
+            pe = torch.zeros((ctx.n_det, ctx.n_vox), dtype=torch.float32, device="cuda")
+            ctx.pe(pe[:, v0:v0 + nv], rotation=float(r), vox_begin=v0, vox_count=nv)
+            pes.append(pe)
+            out = torch.empty((rows, nv), dtype=torch.float32, device="cuda")
+            items.append((k, 3, sysmat.HOLE_MODEL_COMBINED, float(r), pe, d0, rows, v0, nv, out))
+    stream = torch.cuda.current_stream()
+    plan = sysmat.ScatterBatchPlan(ctxs, items, stream=stream)
+    plan.run(stream=stream)                                   # capture + warm-up
+    batch_ms = _events(torch, lambda: plan.run(stream=stream), n=3, stream=stream)
+    ref = [it[-1].clone() for it in items]
+
+    def plain():
+        for (k, parts, model, rot, pe, dd, nd, vv, nn, out) in items:
+            ctxs[k].scatter(out, pe, parts=parts, hole_model=model, rotation=rot, det_begin=dd, det_count=nd,
+                            vox_begin=vv, vox_count=nn, stream=stream)
+
+    plain()
+    plain_ms = _events(torch, plain, n=3, stream=stream)
+    same = all(bool(torch.equal(it[-1], r)) for it, r in zip(items, ref))
+    plan.close()
+    nel = len(items) * rows * nv
+    for c in ctxs:
+        c.close()
+    return {"value": nel / (batch_ms * 1e-3), "unit": UNIT, "ms_per_step": batch_ms,
+            "plain_value": nel / (plain_ms * 1e-3), "plain_ms_per_step": plain_ms,
+            "speedup_vs_plain": plain_ms / batch_ms, "outputs_identical": same, "tasks": len(items),
+            "gpu_launches_per_step": {"batched": 1, "plain": len(items)},
+            "workload": f"config4 design sweep, scatter: {n_instances} seeded collimators x {n_rot} rotations, each "
+                        f"task crystals {d0}..{d0 + rows - 1} x z-plane 8 (1024 voxels), crystal + collimator parts"}
+
+
 # ---------------------------------------------------------------------------------------
 # CPU baseline and accuracy: the oracle (reference arithmetic in C, FP32 and FP64) on the
 # host cores, as the checker of the matrices the GPU legs produced
@@ -641,6 +762,9 @@ def cpu_baseline(args, g, n_planes, keep):
         idx = np.searchsorted(rows, sel)
         acc["fp64"] = dict(rel_err_stats(f["out"][sel - f["d0"]], o64[idx]), vs="FP64 oracle",
                            sample=f"{sel.size} of the crystals above x the same voxel row")
+    if "local" in keep:
+        f = keep["local"]
+        acc["local"] = dict(rel_err_stats(f["out"][rows], o64), vs="FP64 oracle", sample=base["sample"])
     if "sampled" in keep:
         s = keep["sampled"]
         sel = np.arange(s["d0"] + 8, s["d0"] + s["out"].shape[0], 128)
@@ -661,6 +785,12 @@ def cpu_baseline(args, g, n_planes, keep):
         acc["scatter"] = dict(rel_err_stats(s["out"][sel][:, v3:v3 + nx3], o), vs="FP64 oracle",
                               sample=f"crystals {sel.tolist()} x voxel row 24 of config3 z-plane 8 "
                                      "(the GPU's PE matrix and bitmaps as input)")
+    if "scatter_grid" in keep:
+        s = keep["scatter_grid"]
+        d, v = 528, 22
+        o = oracle.scatter_grid(s["geo"], parts=3, cell=0.25, dets=[d], v0=v, nv=1, threads=threads)
+        acc["scatter_grid"] = dict(rel_err_stats(s["out"][d:d + 1, v:v + 1], o), vs="FP64 definition of the grid model",
+                                   sample=f"crystal {d} x voxel {v} of the grid leg's voxel row")
     return base, acc
 
 
@@ -794,6 +924,8 @@ def main():
     ap.add_argument("--no-batch", action="store_true")
     ap.add_argument("--no-sampled", action="store_true")
     ap.add_argument("--no-fp64", action="store_true")
+    ap.add_argument("--no-local", action="store_true")
+    ap.add_argument("--no-grid", action="store_true")
     ap.add_argument("--fp64-crystals", type=int, default=None,
                     help="crystals (centred) of the FP64 leg; default all (profiling uses a small case)")
     ap.add_argument("--no-cpu-baseline", action="store_true")

@@ -157,6 +157,7 @@ extern "C" SYSMAT_API int sysmat_create(sysmat_ctx** out, int device, const floa
     ctx->g = g;
     ctx->n_holes0_host = nh0;
     ctx->h_img.assign(pI, pI + kNImage);
+    ctx->h_det.assign(pD, pD + kNDetector);
     if (pC) { ctx->h_col15 = pC[15]; ctx->h_col17 = pC[17]; }
     if (pP) ctx->h_phys.assign(pP, pP + kNPhysics);
     cudaDeviceProp prop;
@@ -379,8 +380,10 @@ extern "C" SYSMAT_API int sysmat_pe(sysmat_ctx* ctx, float rotation, int det_beg
 {
     int rc = check_block(ctx, det_begin, det_count, vox_begin, vox_count, d_out, ld);
     if (rc) return rc;
-    if (mode != SYSMAT_MODE_REFERENCE && mode != SYSMAT_MODE_PRECISE && mode != SYSMAT_MODE_FP64)
+    if (mode != SYSMAT_MODE_REFERENCE && mode != SYSMAT_MODE_PRECISE && mode != SYSMAT_MODE_FP64 &&
+        mode != SYSMAT_MODE_LOCAL)
         return SYSMAT_ERR_ARG;
+    if (mode == SYSMAT_MODE_LOCAL && ctx->g.hole_shape) return SYSMAT_ERR_ARG;   // circular holes only
     if (det_count == 0 || vox_count == 0) return SYSMAT_OK;
     cudaStream_t s = (cudaStream_t)stream;
     const PeLaunch L = pe_block(ctx, rotation, det_begin, det_count, vox_begin, vox_count, d_out, ld);
@@ -443,7 +446,7 @@ extern "C" SYSMAT_API int sysmat_scatter_prepare(sysmat_ctx* ctx, int parts, con
         return SYSMAT_ERR_ARG;
     ctx->prepared_parts = 0;
     const int rc = build_scatter_pairs(ctx->g, parts, d_bm_crystal, d_bm_collimator, ctx->scratch,
-                                       &ctx->pairs, &ctx->att, (cudaStream_t)stream);
+                                       &ctx->pairs, &ctx->att, &ctx->att_offsets, (cudaStream_t)stream);
     if (rc == -2) return SYSMAT_ERR_NOMEM;
     if (rc) return SYSMAT_ERR_CUDA;
     ctx->prepared_parts = parts;
@@ -460,7 +463,8 @@ extern "C" SYSMAT_API int sysmat_scatter_prepare_native(sysmat_ctx* ctx, int par
     if ((parts & SYSMAT_SCATTER_COLLIMATOR) && (ctx->g.n_holes < 1 || ctx->g.n_layers < 1)) return SYSMAT_ERR_ARG;
     ctx->prepared_parts = 0;
     const int rc = build_scatter_pairs_native(ctx->g, parts, d_bm_crystal, ctx->scratch, &ctx->pairs,
-                                              &ctx->pairs_native, &ctx->att, (cudaStream_t)stream);
+                                              &ctx->pairs_native, &ctx->att, &ctx->att_offsets,
+                                              (cudaStream_t)stream);
     if (rc == -2) return SYSMAT_ERR_NOMEM;
     if (rc) return SYSMAT_ERR_CUDA;
     ctx->prepared_parts = parts;
@@ -468,10 +472,13 @@ extern "C" SYSMAT_API int sysmat_scatter_prepare_native(sysmat_ctx* ctx, int par
     return SYSMAT_OK;
 }
 
-extern "C" SYSMAT_API int sysmat_scatter(sysmat_ctx* ctx, int parts, int hole_model, float rotation,
-                                         const float* d_pe, int det_begin, int det_count,
-                                         long long vox_begin, long long vox_count, float* d_out,
-                                         long long ld, void* stream)
+namespace sysmat {
+
+// Checks a scatter block against the context (as sysmat_scatter documents), builds the
+// Klein-Nishina table of the context's photopeak if needed, and fills the launch.
+int scatter_setup(sysmat_ctx* ctx, int parts, int hole_model, float rotation, const float* d_pe, int det_begin,
+                  int det_count, long long vox_begin, long long vox_count, float* d_out, long long ld,
+                  cudaStream_t stream, ScatterPhysics* ph_out, ScatterLaunch* L_out)
 {
     int rc = check_block(ctx, det_begin, det_count, vox_begin, vox_count, d_out, ld);
     if (rc) return rc;
@@ -482,6 +489,7 @@ extern "C" SYSMAT_API int sysmat_scatter(sysmat_ctx* ctx, int parts, int hole_mo
     // the pair tables' layout follows the model they were prepared for
     if ((hole_model == SYSMAT_HOLE_MODEL_NATIVE) != (ctx->prepared_native != 0)) return SYSMAT_ERR_ARG;
     if ((parts & SYSMAT_SCATTER_CRYSTAL) && !d_pe) return SYSMAT_ERR_ARG;
+    if (!std::isfinite(rotation)) return SYSMAT_ERR_ARG;
     if (ctx->h_phys.size() != (size_t)kNPhysics) return SYSMAT_ERR_ARG;
     const float* P = ctx->h_phys.data();
     ScatterPhysics ph;
@@ -510,6 +518,7 @@ extern "C" SYSMAT_API int sysmat_scatter(sysmat_ctx* ctx, int parts, int hole_mo
     L.pairs = ctx->pairs;
     L.native = ctx->pairs_native;
     L.att = ctx->att;
+    L.att_offsets = ctx->att_offsets;
     L.out = d_out;
     if (!ctx->d_kn_tab || ctx->kn_e0 != ph.e0) {     // (re)build the FP64 Klein-Nishina table
         std::vector<double> tab(3 * (size_t)(kKnTable + 1));
@@ -520,11 +529,28 @@ extern "C" SYSMAT_API int sysmat_scatter(sysmat_ctx* ctx, int parts, int hole_mo
             return SYSMAT_ERR_NOMEM;
         }
         CUDA_TRY(cudaMemcpyAsync(ctx->d_kn_tab, tab.data(), sizeof(double) * tab.size(),
-                                 cudaMemcpyHostToDevice, (cudaStream_t)stream));
-        CUDA_TRY(cudaStreamSynchronize((cudaStream_t)stream));
+                                 cudaMemcpyHostToDevice, stream));
+        CUDA_TRY(cudaStreamSynchronize(stream));
         ctx->kn_e0 = ph.e0;
     }
     L.kn_tab = ctx->d_kn_tab;
+    *ph_out = ph;
+    *L_out = L;
+    return SYSMAT_OK;
+}
+
+}  // namespace sysmat
+
+extern "C" SYSMAT_API int sysmat_scatter(sysmat_ctx* ctx, int parts, int hole_model, float rotation,
+                                         const float* d_pe, int det_begin, int det_count,
+                                         long long vox_begin, long long vox_count, float* d_out,
+                                         long long ld, void* stream)
+{
+    ScatterPhysics ph;
+    ScatterLaunch L;
+    const int rc = scatter_setup(ctx, parts, hole_model, rotation, d_pe, det_begin, det_count, vox_begin,
+                                 vox_count, d_out, ld, (cudaStream_t)stream, &ph, &L);
+    if (rc) return rc;
     return launch_scatter(ctx->g, ph, L, (cudaStream_t)stream) ? SYSMAT_ERR_CUDA : SYSMAT_OK;
 }
 

@@ -24,7 +24,7 @@ __device__ __forceinline__ void slab64(double p0, double lo, double hi, double i
 // full crossings only (PESysMatGen.cu:28-232); inside = true: the segment ends inside the
 // box (:328-589).  Returns true and sets tmin, tmax, tio when the caller must finish with
 // the interval tests; returns false with the result in *out otherwise.
-__device__ __noinline__ bool box64_parallel(const double p0[3], const double p1[3], const double lo[3],
+static __device__ __noinline__ bool box64_parallel(const double p0[3], const double p1[3], const double lo[3],
                                             const double hi[3], bool inside, double* out, double* tmin,
                                             double* tmax, double* tio)
 {

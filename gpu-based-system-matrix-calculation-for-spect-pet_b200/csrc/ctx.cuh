@@ -19,6 +19,7 @@ struct sysmat_ctx {
     float* d_phys = nullptr;
     std::vector<float> h_phys;
     std::vector<float> h_img;
+    std::vector<float> h_det;       // detector parameters (grid scatter: crystal cell divisions)
     float h_col15 = 0.0f, h_col17 = 0.0f;   // layer-0 mu_total and mu_compton (scatter.cu:1716)
     // derived tables
     float4* d_tables = nullptr;
@@ -32,6 +33,7 @@ struct sysmat_ctx {
     sysmat::PairRec* pairs = nullptr;
     sysmat::PairNative* pairs_native = nullptr;   // native model's extra pair fields
     sysmat::AttEntry* att = nullptr;
+    long long* att_offsets = nullptr;             // 64-bit attenuator-list offset per pair
     double* d_kn_tab = nullptr;     // Klein-Nishina table for kn_e0
     float4* d_shapes = nullptr;     // elliptical holes (sysmat_set_hole_shapes), or nullptr
     void* d_tables64 = nullptr;     // FP64 mode tables (DevGeom::t64)
@@ -44,4 +46,9 @@ namespace sysmat {
 // matrix, ld >= vox_count, d_out is set and the context's device is current.
 int check_block(const sysmat_ctx* ctx, int det_begin, int det_count, long long vox_begin,
                 long long vox_count, const float* d_out, long long ld);
+// Checks a scatter block as sysmat_scatter does and fills its launch (building the context's
+// Klein-Nishina table when needed; synchronises `stream` then).
+int scatter_setup(sysmat_ctx* ctx, int parts, int hole_model, float rotation, const float* d_pe, int det_begin,
+                  int det_count, long long vox_begin, long long vox_count, float* d_out, long long ld,
+                  cudaStream_t stream, ScatterPhysics* ph, ScatterLaunch* L);
 }  // namespace sysmat

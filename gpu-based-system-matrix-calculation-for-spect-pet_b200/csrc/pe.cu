@@ -827,6 +827,7 @@ __device__ double pe_element_sampled(const DevGeom& g, const BlockSmem& bs, Warp
 }
 
 #include "pe_fp64.cuh"
+#include "pe_local.cuh"
 
 // Block superset of the reference cone test over all voxels within radius rho of
 // (cx, cy, cz): keep object o when |u_o - u_d| <= (rho + r_o)/(L_o - rho)
@@ -888,6 +889,8 @@ struct BrickOut {
     float* out;
     long long ld, vox_begin, vlast;
     int det_begin;
+    float* sub_out;           // per-sub-element contributions (local sampled form), or nullptr
+    int det_count;
 };
 
 // One work item: crystal det_begin + di against one voxel brick of bx x by x bz voxels (brick
@@ -922,7 +925,12 @@ __device__ __forceinline__ void pe_brick(const DevGeom& g, BlockSmem& bs, WarpSm
         const long long v = ix + g.nx * ((long long)iy + (long long)g.ny * iz);
         if (v < O.vox_begin || v > O.vlast) continue;
         float val;
-        if constexpr (SAMPLED) val = (float)pe_element_sampled<ELL>(g, bs, ws, d, v, cr, sr, lane, *smp);
+        if constexpr (MODE == 3) {
+            float* so = nullptr;
+            if (SAMPLED && O.sub_out)
+                so = O.sub_out + ((v - O.vox_begin) * O.det_count + di) * (long long)(smp->nx * smp->ny * smp->nz);
+            val = (float)pe_element_local(g, bs, ws, d, v, cr, sr, rotation, lane, SAMPLED ? smp : nullptr, so);
+        } else if constexpr (SAMPLED) val = (float)pe_element_sampled<ELL>(g, bs, ws, d, v, cr, sr, lane, *smp);
         else if constexpr (MODE == 2) val = (float)pe_element64(g, bs, ws, d, v, cr, sr, rotation, lane);
         else val = (float)pe_element<MODE, COUNT, ELL>(g, bs, ws, d, v, cr, sr, lane, counters);
         if (lane == 0) O.out[(long long)di * O.ld + (v - O.vox_begin)] = val;
@@ -948,7 +956,7 @@ __global__ void __launch_bounds__(kThreads, 2) pe_kernel(DevGeom g, PeLaunch L)
     const int nbz = (iz1 - iz0 + 1 + bz - 1) / bz;
     const long long n_bricks = (long long)nbx * nby * nbz;
     const long long total = n_bricks * L.det_count;
-    const BrickOut O{L.out, L.ld, L.vox_begin, vlast, L.det_begin};
+    const BrickOut O{L.out, L.ld, L.vox_begin, vlast, L.det_begin, L.sub_out, L.det_count};
     for (;;) {
         if (threadIdx.x == 0) bs.item = (long long)atomicAdd(L.work_counter, 1ull);
         __syncthreads();
@@ -1018,7 +1026,7 @@ __global__ void __launch_bounds__(kThreads, 2) pe_batch_kernel(BatchLaunch B)
         const int gz = (int)(b / ((long long)T.nbx * T.nby));
         const int rem = (int)(b - (long long)gz * T.nbx * T.nby);
         const int gy = rem / T.nbx, gx = rem - gy * T.nbx;
-        const BrickOut O{T.out, T.ld, T.vox_begin, T.vox_begin + T.vox_count - 1, T.det_begin};
+        const BrickOut O{T.out, T.ld, T.vox_begin, T.vox_begin + T.vox_count - 1, T.det_begin, nullptr, T.det_count};
         pe_brick<MODE, false, ELL>(g, bs, ws, lane, wid, O, di, gx, gy, gz, T.iz0, T.iz1, B.bx, B.by, B.bz, cr,
                                    sr, nullptr, nullptr, T.rotation);
     }
@@ -1129,6 +1137,7 @@ int launch_pe_batch(const BatchLaunch& B, int mode, bool ell, int grid, cudaStre
 int launch_pe(const DevGeom& g, const PeLaunch& L, int mode, int num_sms, cudaStream_t stream)
 {
     if (mode == 2) return g.t64.cry_pos ? launch_mode<2, false, false>(g, L, num_sms, stream) : -1;
+    if (mode == 3) return (g.t64.cry_pos && !g.hole_shape) ? launch_mode<3, false, false>(g, L, num_sms, stream) : -1;
     if (g.hole_shape) {                   // systems with elliptical holes
         if (L.counters) return launch_mode<0, true, true>(g, L, num_sms, stream);
         return mode == 0 ? launch_mode<0, false, true>(g, L, num_sms, stream)
@@ -1137,6 +1146,12 @@ int launch_pe(const DevGeom& g, const PeLaunch& L, int mode, int num_sms, cudaSt
     if (L.counters) return launch_mode<0, true, false>(g, L, num_sms, stream);
     return mode == 0 ? launch_mode<0, false, false>(g, L, num_sms, stream)
                      : launch_mode<1, false, false>(g, L, num_sms, stream);
+}
+
+int launch_pe_local_sampled(const DevGeom& g, const PeLaunch& L, int num_sms, cudaStream_t stream)
+{
+    if (!g.t64.cry_pos || g.hole_shape) return -1;
+    return launch_mode<3, false, false, true>(g, L, num_sms, stream);
 }
 
 int launch_pe_sampled(const DevGeom& g, const PeLaunch& L, int num_sms, cudaStream_t stream)

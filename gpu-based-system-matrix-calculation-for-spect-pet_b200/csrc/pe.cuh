@@ -35,7 +35,10 @@ struct PeLaunch {
     // [1] non-zero hole chords, [2] non-zero crystal chords, [3] elements, [4] plate-blocked
     // sub-elements, [5] cone-test candidates (holes + crystals)
     unsigned long long* counters;
-    Sampling smp;                          // read by the sampled instance only
+    Sampling smp;                          // read by the sampled instances only
+    // local sampled instance only (optional): per-sub-element contributions, written at
+    // ((v - vox_begin) * det_count + (d - det_begin)) * n_sub + (iz * ny + iy) * nx + ix
+    float* sub_out = nullptr;
 };
 
 // One (geometry, rotation, detector x voxel block) task of a batched launch.  The host fills
@@ -78,6 +81,9 @@ struct AdjLaunch {
 int launch_pe(const DevGeom& g, const PeLaunch& L, int mode, int num_sms, cudaStream_t stream);
 // The sampled form (L.smp), accumulated in FP64.
 int launch_pe_sampled(const DevGeom& g, const PeLaunch& L, int num_sms, cudaStream_t stream);
+// The local-coordinate FP32 form with the crystal division of L.smp (voxel centres only),
+// optionally writing every sub-element's contribution to L.sub_out.
+int launch_pe_local_sampled(const DevGeom& g, const PeLaunch& L, int num_sms, cudaStream_t stream);
 // kind 0: projection, kind 1: vector-Jacobian product, kind 2: back projection.
 int launch_pe_adjoint(const DevGeom& g, const AdjLaunch& L, int kind, int num_sms, cudaStream_t stream);
 // Sets the batched kernel's shared-memory attribute on the current device (once) and returns

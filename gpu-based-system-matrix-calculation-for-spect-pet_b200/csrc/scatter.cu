@@ -33,7 +33,7 @@ namespace sysmat {
 
 namespace {
 
-constexpr int kItemThreads = 128;
+constexpr int kItemThreads = kScatterBlockVoxels;
 constexpr int kPairChunk = 512;
 
 // ---- reference helper formulas (scatter.cu:961-1038) ----
@@ -65,30 +65,8 @@ __device__ __forceinline__ float dist3(float x1, float y1, float z1, float x2, f
 }
 
 // Reference Riemann sum with n + 1 terms from a, step 0.01f, in FP64 from the table:
-//   sum = G(b) - G(a) + h/2 (F(a) + F(b)) + h^2/12 (F'(b) - F'(a)),  b = a + n h,
-// G and F by cubic Hermite interpolation on the table (error ~1e-14), F' linearly.
-__device__ __forceinline__ void kn_tab_eval(const double* __restrict__ tab, double th, double& G,
-                                            double& F, double& Fp)
-{
-    const double hc = 3.14159265358979323846 / kKnTable;
-    double x = th / hc;
-    int i = (int)x;
-    i = i < 0 ? 0 : (i > kKnTable - 1 ? kKnTable - 1 : i);
-    const double t = x - (double)i;
-    const double t2 = t * t, t3 = t2 * t;
-    const double h00 = 2.0 * t3 - 3.0 * t2 + 1.0, h10 = t3 - 2.0 * t2 + t;
-    const double h01 = -2.0 * t3 + 3.0 * t2, h11 = t3 - t2;
-    const double* Gt = tab;
-    const double* Ft = tab + (kKnTable + 1);
-    const double* Pt = tab + 2 * (kKnTable + 1);
-    const double g0 = __ldg(&Gt[i]), g1 = __ldg(&Gt[i + 1]);
-    const double f0 = __ldg(&Ft[i]), f1 = __ldg(&Ft[i + 1]);
-    const double p0 = __ldg(&Pt[i]), p1 = __ldg(&Pt[i + 1]);
-    G = h00 * g0 + h10 * hc * f0 + h01 * g1 + h11 * hc * f1;
-    F = h00 * f0 + h10 * hc * p0 + h01 * f1 + h11 * hc * p1;
-    Fp = (1.0 - t) * p0 + t * p1;
-}
-
+//   sum = G(b) - G(a) + h/2 (F(a) + F(b)) + h^2/12 (F'(b) - F'(a)),  b = a + n h
+// (G, F and F' from kn_tab_eval, scatter.cuh).
 __device__ __forceinline__ double kn_sum_tab(float a, int n, const double* __restrict__ tab)
 {
     const double h = (double)0.01f;
@@ -97,15 +75,6 @@ __device__ __forceinline__ double kn_sum_tab(float a, int n, const double* __res
     kn_tab_eval(tab, ad, Ga, Fa, Pa);
     kn_tab_eval(tab, bd, Gb, Fb, Pb);
     return (Gb - Ga) + 0.5 * h * (Fa + Fb) + (h * h / 12.0) * (Pb - Pa);
-}
-
-__device__ __forceinline__ float window_prob(float e, float res, float lo, float hi)
-{
-    const float sigma = res / 2.35482f * e;
-    const float s2 = (float)((double)sigma * 1.4142135623730951);   // sigma * sqrt(2.0)
-    const float z1 = (lo - e) / s2;
-    const float z2 = (hi - e) / s2;
-    return 0.5f * (erff(z2) - erff(z1));
 }
 
 // Crystal d's single sub-element centre (1x1x1 division, :1242-1252) in its own frame and
@@ -346,7 +315,7 @@ __device__ void tungsten_path(const DevGeom& g, int h, float sx, float sy, float
 
 template <bool NATIVE>
 __global__ void pair_count_kernel(DevGeom g, int parts, const uint32_t* bm_cry, const uint32_t* bm_col,
-                                  int* counts)
+                                  long long* counts)
 {
     const int ns = g.n_det + (NATIVE ? g.n_holes : g.n_holes0);
     const long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -364,7 +333,7 @@ __global__ void pair_count_kernel(DevGeom g, int parts, const uint32_t* bm_cry, 
 
 template <bool NATIVE>
 __global__ void pair_fill_kernel(DevGeom g, int parts, const uint32_t* bm_cry, const uint32_t* bm_col,
-                                 const int* offsets, PairRec* pairs, PairNative* nat, AttEntry* att)
+                                 const long long* offsets, PairRec* pairs, PairNative* nat, AttEntry* att)
 {
     const int ns = g.n_det + (NATIVE ? g.n_holes : g.n_holes0);
     const long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -387,11 +356,13 @@ __global__ void pair_fill_kernel(DevGeom g, int parts, const uint32_t* bm_cry, c
         const float yt = q.yDs + 1000.0f * (q.yDs - r.yss) / r.lsd;
         const float zt = q.zDs + 1000.0f * (q.zDs - r.zss) / r.lsd;
         r.labs = box_chord(r.xss, r.yss, r.zss, xt, yt, zt, ux1, uy1, uz1, ux2, uy2, uz2);
-        r.att_begin = offsets[p];
+        // row-relative start: a row holds at most ns * D entries, which fits an int
+        r.att_begin = (int)(offsets[p] - offsets[(long long)d * ns]);
+        AttEntry* dst = att + offsets[p];
         int k = 0;
         for_each_attenuator<NATIVE>(g, bm_cry, bm_col, s, d, xs, ys, zs, q, [&](int a, float len) {
             const float4 mu = __ldg(&g.cry.mu[a]);
-            att[r.att_begin + k] = AttEntry{len, mu.y, mu.z};
+            dst[k] = AttEntry{len, mu.y, mu.z};
             ++k;
         });
         r.att_count = k;
@@ -497,15 +468,14 @@ __device__ float scatter_item(const ElemConst& e, const PairRec& pr, const PairN
     return (float)c;
 }
 
+// One block's share of a scatter launch: detector row di, voxels vblock * kItemThreads + t
+// (t = threadIdx.x).  sp, spn: the block's pair staging buffers in shared memory.
 template <bool NATIVE>
-__global__ void __launch_bounds__(kItemThreads)
-scatter_kernel(DevGeom g, ScatterPhysics ph, ScatterLaunch L)
+__device__ __forceinline__ void scatter_rows(const DevGeom& g, const ScatterPhysics& ph, const ScatterLaunch& L,
+                                             int di, long long vblock, PairRec* sp, PairNative* spn)
 {
-    __shared__ PairRec sp[kPairChunk];
-    __shared__ PairNative spn[NATIVE ? kPairChunk : 1];
-    const int di = blockIdx.y;
     const int d = L.det_begin + di;
-    const long long vi = (long long)blockIdx.x * kItemThreads + threadIdx.x;
+    const long long vi = vblock * kItemThreads + threadIdx.x;
     const bool active = vi < L.vox_count;
     const long long v = L.vox_begin + (active ? vi : 0);
     const int ns = g.n_det + (NATIVE ? g.n_holes : g.n_holes0);
@@ -536,6 +506,7 @@ scatter_kernel(DevGeom g, ScatterPhysics ph, ScatterLaunch L)
     const int s_begin = (L.parts & 1) ? 0 : g.n_det;
     const int s_end = (L.parts & 2) ? ns : g.n_det;
     const PairRec* prow = L.pairs + (long long)d * ns;
+    const AttEntry* att_row = L.att + L.att_offsets[(long long)d * ns];
     for (int s0 = s_begin; s0 < s_end; s0 += kPairChunk) {
         const int cnt = min(kPairChunk, s_end - s0);
         __syncthreads();
@@ -576,7 +547,7 @@ scatter_kernel(DevGeom g, ScatterPhysics ph, ScatterLaunch L)
                 else w_s = sa / ph.col_mu_tot0 * ph.col_mu_c0;            // :1716
             }
             // one call site keeps a single copy of the item code
-            const double c = (double)scatter_item<NATIVE>(e, pr, spn[NATIVE ? k : 0], L.att, xs, ys, zs, w_s,
+            const double c = (double)scatter_item<NATIVE>(e, pr, spn[NATIVE ? k : 0], att_row, xs, ys, zs, w_s,
                                                           ph.e0, ph.integ, L.kn_tab);
             if (crystal) acc_c += c;
             else acc_h += c;
@@ -588,6 +559,66 @@ scatter_kernel(DevGeom g, ScatterPhysics ph, ScatterLaunch L)
     else if (L.parts & 1) outv = (float)acc_c;
     else outv = (float)acc_h;
     L.out[(long long)di * L.ld + vi] = outv;
+}
+
+template <bool NATIVE>
+__global__ void __launch_bounds__(kItemThreads)
+scatter_kernel(DevGeom g, ScatterPhysics ph, ScatterLaunch L)
+{
+    __shared__ PairRec sp[kPairChunk];
+    __shared__ PairNative spn[NATIVE ? kPairChunk : 1];
+    scatter_rows<NATIVE>(g, ph, L, blockIdx.y, blockIdx.x, sp, spn);
+}
+
+// Batched scatter: one persistent grid over the (row, voxel block) items of many tasks, taken
+// from one counter; a block finds its item's task by binary search over the tasks' first item
+// numbers and copies the task (and its geometry, when it changes) into shared memory.  Each
+// item runs scatter_rows, so every element equals the single launch's bit for bit.
+__global__ void __launch_bounds__(kItemThreads) scatter_batch_kernel(ScatterBatchLaunch B)
+{
+    __shared__ PairRec sp[kPairChunk];
+    __shared__ PairNative spn[kPairChunk];
+    __shared__ DevGeom sg;
+    __shared__ ScatterTask st;
+    __shared__ long long s_item;
+    __shared__ int s_task;
+    int cur_task = -1, cur_geom = -1;
+    for (;;) {
+        if (threadIdx.x == 0) {
+            const long long item = (long long)atomicAdd(B.work_counter, 1ull);
+            int lo = 0, hi = B.n_tasks - 1;
+            while (lo < hi) {                       // last task with item_begin <= item
+                const int mid = (lo + hi + 1) >> 1;
+                if (B.tasks[mid].item_begin <= item) lo = mid; else hi = mid - 1;
+            }
+            s_item = item;
+            s_task = lo;
+        }
+        __syncthreads();
+        const long long item = s_item;
+        const int task = s_task;
+        __syncthreads();
+        if (item >= B.total_items) break;
+        if (task != cur_task) {                     // block-uniform
+            const int* src = reinterpret_cast<const int*>(B.tasks + task);
+            int* dst = reinterpret_cast<int*>(&st);
+            for (int i = threadIdx.x; i < (int)(sizeof(ScatterTask) / sizeof(int)); i += kItemThreads) dst[i] = src[i];
+            __syncthreads();
+            if (st.geom != cur_geom) {
+                const int* gs = reinterpret_cast<const int*>(B.geoms + st.geom);
+                int* gd = reinterpret_cast<int*>(&sg);
+                for (int i = threadIdx.x; i < (int)(sizeof(DevGeom) / sizeof(int)); i += kItemThreads) gd[i] = gs[i];
+                cur_geom = st.geom;
+            }
+            cur_task = task;
+            __syncthreads();
+        }
+        const long long local = item - st.item_begin;
+        const int di = (int)(local / st.n_vblocks);
+        const long long vb = local - (long long)di * st.n_vblocks;
+        if (st.L.hole_model == 2) scatter_rows<true>(sg, st.ph, st.L, di, vb, sp, spn);
+        else scatter_rows<false>(sg, st.ph, st.L, di, vb, sp, spn);
+    }
 }
 
 }  // namespace
@@ -624,17 +655,18 @@ int launch_bitmap_collimator(const DevGeom& g, uint32_t* words, cudaStream_t s)
 
 template <bool NATIVE>
 static int build_pairs(const DevGeom& g, int parts, const uint32_t* bm_cry, const uint32_t* bm_col,
-                       ScatterScratch& scratch, PairRec** pairs, PairNative** native, AttEntry** att, cudaStream_t s)
+                       ScatterScratch& scratch, PairRec** pairs, PairNative** native, AttEntry** att,
+                       long long** att_offsets, cudaStream_t s)
 {
     const int ns = g.n_det + (NATIVE ? g.n_holes : g.n_holes0);
     const long long np = (long long)g.n_det * ns;
-    // layout: [counts/offsets (np+1 ints)][cub temp][pairs][att]
+    // layout: [counts (np+1)][64-bit offsets (np+1)][cub temp][pairs][native][att]
     size_t temp_bytes = 0;
-    cub::DeviceScan::ExclusiveSum(nullptr, temp_bytes, (int*)nullptr, (int*)nullptr, (int)(np + 1), s);
+    cub::DeviceScan::ExclusiveSum(nullptr, temp_bytes, (long long*)nullptr, (long long*)nullptr, np + 1, s);
     auto align = [](size_t x) { return (x + 255) & ~size_t(255); };
     const size_t off_counts = 0;
-    const size_t off_offsets = align(off_counts + sizeof(int) * (np + 1));
-    const size_t off_temp = align(off_offsets + sizeof(int) * (np + 1));
+    const size_t off_offsets = align(off_counts + sizeof(long long) * (np + 1));
+    const size_t off_temp = align(off_offsets + sizeof(long long) * (np + 1));
     const size_t off_pairs = align(off_temp + temp_bytes);
     const size_t off_native = align(off_pairs + sizeof(PairRec) * np);
     const size_t fixed = align(off_native + (NATIVE ? sizeof(PairNative) * np : 0));
@@ -644,15 +676,16 @@ static int build_pairs(const DevGeom& g, int parts, const uint32_t* bm_cry, cons
         scratch.bytes = fixed;
     }
     char* base = (char*)scratch.base;
-    int* counts = (int*)(base + off_counts);
-    int* offsets = (int*)(base + off_offsets);
+    long long* counts = (long long*)(base + off_counts);
+    long long* offsets = (long long*)(base + off_offsets);
     const unsigned blocks = (unsigned)((np + 255) / 256);
     pair_count_kernel<NATIVE><<<blocks, 256, 0, s>>>(g, parts, bm_cry, bm_col, counts);
-    if (cudaMemsetAsync(counts + np, 0, sizeof(int), s) != cudaSuccess) return -1;
-    cub::DeviceScan::ExclusiveSum(base + off_temp, temp_bytes, counts, offsets, (int)(np + 1), s);
-    int total = 0;
-    if (cudaMemcpyAsync(&total, offsets + np, sizeof(int), cudaMemcpyDeviceToHost, s) != cudaSuccess) return -1;
+    if (cudaMemsetAsync(counts + np, 0, sizeof(long long), s) != cudaSuccess) return -1;
+    cub::DeviceScan::ExclusiveSum(base + off_temp, temp_bytes, counts, offsets, np + 1, s);
+    long long total = 0;
+    if (cudaMemcpyAsync(&total, offsets + np, sizeof(long long), cudaMemcpyDeviceToHost, s) != cudaSuccess) return -1;
     if (cudaStreamSynchronize(s) != cudaSuccess) return -1;
+    if (total < 0) return -1;
     const size_t need = fixed + sizeof(AttEntry) * (size_t)(total > 0 ? total : 1);
     if (scratch.bytes < need) {
         // grow, keeping nothing but the offsets (re-run the cheap count+scan afterwards)
@@ -660,30 +693,48 @@ static int build_pairs(const DevGeom& g, int parts, const uint32_t* bm_cry, cons
         if (cudaMalloc(&scratch.base, need) != cudaSuccess) { scratch.base = nullptr; return -2; }
         scratch.bytes = need;
         base = (char*)scratch.base;
-        counts = (int*)(base + off_counts);
-        offsets = (int*)(base + off_offsets);
+        counts = (long long*)(base + off_counts);
+        offsets = (long long*)(base + off_offsets);
         pair_count_kernel<NATIVE><<<blocks, 256, 0, s>>>(g, parts, bm_cry, bm_col, counts);
-        if (cudaMemsetAsync(counts + np, 0, sizeof(int), s) != cudaSuccess) return -1;
-        cub::DeviceScan::ExclusiveSum(base + off_temp, temp_bytes, counts, offsets, (int)(np + 1), s);
+        if (cudaMemsetAsync(counts + np, 0, sizeof(long long), s) != cudaSuccess) return -1;
+        cub::DeviceScan::ExclusiveSum(base + off_temp, temp_bytes, counts, offsets, np + 1, s);
     }
     *pairs = (PairRec*)(base + off_pairs);
     PairNative* nat = NATIVE ? (PairNative*)(base + off_native) : nullptr;
     if (native) *native = nat;
     *att = (AttEntry*)(base + fixed);
+    *att_offsets = offsets;
     pair_fill_kernel<NATIVE><<<blocks, 256, 0, s>>>(g, parts, bm_cry, bm_col, offsets, *pairs, nat, *att);
     return cudaGetLastError() == cudaSuccess ? 0 : -1;
 }
 
 int build_scatter_pairs(const DevGeom& g, int parts, const uint32_t* bm_cry, const uint32_t* bm_col,
-                        ScatterScratch& scratch, PairRec** pairs, AttEntry** att, cudaStream_t s)
+                        ScatterScratch& scratch, PairRec** pairs, AttEntry** att, long long** att_offsets,
+                        cudaStream_t s)
 {
-    return build_pairs<false>(g, parts, bm_cry, bm_col, scratch, pairs, nullptr, att, s);
+    return build_pairs<false>(g, parts, bm_cry, bm_col, scratch, pairs, nullptr, att, att_offsets, s);
 }
 
 int build_scatter_pairs_native(const DevGeom& g, int parts, const uint32_t* bm_cry, ScatterScratch& scratch,
-                               PairRec** pairs, PairNative** native, AttEntry** att, cudaStream_t s)
+                               PairRec** pairs, PairNative** native, AttEntry** att, long long** att_offsets,
+                               cudaStream_t s)
 {
-    return build_pairs<true>(g, parts, bm_cry, nullptr, scratch, pairs, native, att, s);
+    return build_pairs<true>(g, parts, bm_cry, nullptr, scratch, pairs, native, att, att_offsets, s);
+}
+
+int scatter_batch_blocks_per_sm()
+{
+    int per_sm = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, scatter_batch_kernel, kItemThreads, 0) != cudaSuccess)
+        return 1;
+    return per_sm < 1 ? 1 : per_sm;
+}
+
+int launch_scatter_batch(const ScatterBatchLaunch& B, int grid, cudaStream_t s)
+{
+    if (B.n_tasks < 1 || B.total_items < 1) return 0;
+    scatter_batch_kernel<<<grid, kItemThreads, 0, s>>>(B);
+    return cudaGetLastError() == cudaSuccess ? 0 : -1;
 }
 
 int launch_scatter(const DevGeom& g, const ScatterPhysics& ph, const ScatterLaunch& L, cudaStream_t s)

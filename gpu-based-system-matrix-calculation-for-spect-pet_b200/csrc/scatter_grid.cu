@@ -1,0 +1,613 @@
+// Grid scatter model (sysmat_scatter_grid): primary Compton scatter at points on a grid of
+// cells inside every crystal and inside the tungsten of every collimator layer.  No reference
+// counterpart: the reference scatters at one point per crystal (its centre) and one per
+// layer-0 hole (ScatterGen_RayTracing_CircularHole/scatter.cu:1218-1223, :1707-1716).  The
+// model's definition, restated in double, is oracle/oracle_grid.h:
+//
+//   S[d, v] = sum_{crystal cells p} w_p T(p, d, v) + sum_{septal cells p} w_p T(p, d, v)
+//
+// w_p: a crystal cell's photoelectric contribution from v (the local-coordinate FP32 element
+// with the crystal divided into cells) times mu_C / mu_pe; a septal cell's Compton
+// interaction probability V / (4 pi r^2) exp(-A(v -> p)) mu_C (in double).  T: the
+// reference's scatter item with scatter point p, all crystals on the way as attenuators and the
+// exact Klein-Nishina fraction.
+//
+// Execution (per call, voxels taken 48 at a time):
+//   1. crystal-cell weights: the local sampled photoelectric kernel writes every sub-element's
+//      contribution (pe_local.cuh) into Wc[voxel][crystal][cell];
+//   2. septal-cell weights: one thread per (voxel, septal cell), in double, into Ws;
+//   3. grid_sum_kernel: a block takes a tile of 64 detectors and a range of points; per chunk
+//      of 256 points it stages the weights of all the chunk's voxels in shared memory, and per
+//      detector it forms each point's detector-only terms in double once (position in the
+//      detector's frame, absorption chord, attenuation sums of the crystals, tungsten and hole
+//      media on the way, Lpe and Lc, so that the attenuation at any scattered energy E' is
+//      Lpe (E0/E')^3 + Lc E0/E'), then evaluates the voxel-dependent part of every item in
+//      float and sums per (detector, voxel) in FP64: warp sums, a shared tile of block sums,
+//      one double atomic per (detector, voxel) and block.
+// Calls are synchronous: the weights live in scratch allocated and freed by the call.
+#include <cmath>
+#include <cstdio>
+#include <vector>
+
+#include <cub/cub.cuh>
+#include <thrust/iterator/counting_iterator.h>
+
+#include "../../include/sysmat.h"
+#include "chord64.cuh"
+#include "ctx.cuh"
+#include "geom.cuh"
+#include "pe.cuh"
+#include "scatter.cuh"
+
+#define CUDA_TRY(expr)                                                                     \
+    do {                                                                                   \
+        cudaError_t _e = (expr);                                                           \
+        if (_e != cudaSuccess) {                                                           \
+            std::fprintf(stderr, "sysmat: %s failed: %s (%s:%d)\n", #expr,                 \
+                         cudaGetErrorString(_e), __FILE__, __LINE__);                      \
+            return SYSMAT_ERR_CUDA;                                                        \
+        }                                                                                  \
+    } while (0)
+
+namespace sysmat {
+
+namespace {
+
+constexpr int kGridThreads = 256;
+constexpr int kGridChunk = 256;          // points per chunk (one per thread)
+constexpr int kGridMaxVox = 48;          // voxels per pass
+constexpr int kGridDetTile = 64;         // detectors per block
+constexpr int kGridChunksPerBlock = 8;
+
+struct GridLayer {
+    double x0, y0, z0;                   // plate box corner
+    double cx, cy, cz;                   // cell size
+    int nx, ny, nz;
+    int hole_begin, hole_count;
+    float mu_t, mu_pe, mu_c;
+};
+
+struct GridGeom {
+    int n_layers;
+    GridLayer layer[kMaxLayers];
+    long long sep_begin[kMaxLayers + 1];   // septal cells of layer m: [sep_begin[m], sep_begin[m+1])
+    const int* sep_cell;                   // linear cell index (ix + nx (iy + ny iz)) within its layer
+    const float* raw_col;                  // collimator parameters (hole media)
+};
+
+__device__ __forceinline__ void voxel_centre64(const DevGeom& g, long long v, float rotation, double& x, double& y,
+                                               double& z)
+{
+    const long long nxy = (long long)g.nx * g.ny;
+    const int iz = (int)(v / nxy);
+    const long long r = v - (long long)iz * nxy;
+    const int iy = (int)(r / g.nx);
+    const int ix = (int)(r - (long long)iy * g.nx);
+    const double ang = (double)rotation * (double)g.angle_step;
+    double sa, ca;
+    sincos(ang, &sa, &ca);
+    double xv = ((double)ix - (double)g.nx / 2.0 + 0.5) * (double)g.wx + (double)g.shx;
+    double yv = ((double)iy - (double)g.ny / 2.0 + 0.5) * (double)g.wy + (double)g.shy;
+    x = xv * ca - yv * sa;
+    y = xv * sa + yv * ca;
+    z = ((double)iz - (double)g.nz / 2.0 + 0.5) * (double)g.wz + (double)g.shz;
+}
+
+__device__ __forceinline__ void septal_point(const GridGeom& G, long long j, int& m, double p[3])
+{
+    m = 0;
+    while (m + 1 < G.n_layers && j >= G.sep_begin[m + 1]) ++m;
+    const GridLayer& L = G.layer[m];
+    const int c = __ldg(&G.sep_cell[j]);
+    const int ix = c % L.nx, iy = (c / L.nx) % L.ny, iz = c / (L.nx * L.ny);
+    p[0] = L.x0 + ((double)ix + 0.5) * L.cx;
+    p[1] = L.y0 + ((double)iy + 0.5) * L.cy;
+    p[2] = L.z0 + ((double)iz + 0.5) * L.cz;
+}
+
+// Hole h's axis (x, z) is farther than r from the xz projection of segment a -> b (with a
+// small margin): the segment cannot meet the hole.
+__device__ __forceinline__ bool hole_far(double ax, double az, double bx, double bz, double hx, double hz, double r)
+{
+    const double ex = bx - ax, ez = bz - az;
+    const double l2 = ex * ex + ez * ez;
+    double t = l2 > 0.0 ? ((hx - ax) * ex + (hz - az) * ez) / l2 : 0.0;
+    t = t < 0.0 ? 0.0 : (t > 1.0 ? 1.0 : t);
+    const double dx = ax + t * ex - hx, dz = az + t * ez - hz;
+    return dx * dx + dz * dz > (r + 1e-6) * (r + 1e-6);
+}
+
+// Attenuation sums (mu_total, mu_pe, mu_C times length) of layer m along the segment A -> B,
+// A before B in depth (the direction the reference's chords assume): the plate chord minus the
+// hole chords, with the layer's coefficients, plus the hole chords with the holes' own
+// coefficients.  inside: 0 none, 1 A lies inside the plate, 2 B lies inside.
+__device__ void layer_path64(const DevGeom& g, const GridGeom& G, int m, const double A[3], const double B[3],
+                             int inside, double& wt, double& wpe, double& wc)
+{
+    const double* Ly = g.t64.layer + kLayer64 * m;
+    double box;
+    if (inside == 2)
+        box = box_chord_inside64(A[0], A[1], A[2], B[0], B[1], B[2], Ly[0], Ly[2], Ly[4], Ly[1], Ly[3], Ly[5]);
+    else if (inside == 1)
+        box = box_chord_inside64(B[0], B[1], B[2], A[0], A[1], A[2], Ly[0], Ly[2], Ly[4], Ly[1], Ly[3], Ly[5]);
+    else
+        box = box_chord64(A[0], A[1], A[2], B[0], B[1], B[2], Ly[0], Ly[2], Ly[4], Ly[1], Ly[3], Ly[5]);
+    if (box == 0.0) return;
+    const GridLayer& L = G.layer[m];
+    RayCyl64 rc;
+    ray_cyl64_init(rc, A[0], A[1], A[2], B[0], B[1], B[2]);
+    double hsum = 0.0;
+    for (int j = L.hole_begin; j < L.hole_begin + L.hole_count; ++j) {
+        const D4 a = g.t64.hole_a[j];
+        const double r = g.t64.hole_b[j].x;
+        if (hole_far(A[0], A[2], B[0], B[2], a.x, a.w, r)) continue;
+        const double l = ray_cyl64_chord(rc, A[0], A[1], A[2], a.x, a.y, a.z, a.w, r);
+        if (l == 0.0) continue;
+        const float* hp = G.raw_col + 100 + 9 * j;
+        hsum += l;
+        wt += (double)__ldg(&hp[5]) * l;
+        wpe += (double)__ldg(&hp[6]) * l;
+        wc += (double)__ldg(&hp[7]) * l;
+    }
+    const double lw = box - hsum;
+    if (lw > 0.0) {
+        wt += (double)L.mu_t * lw;
+        wpe += (double)L.mu_pe * lw;
+        wc += (double)L.mu_c * lw;
+    }
+}
+
+// Septal weight V / (4 pi r^2) exp(-A(v -> p)) mu_C for every (voxel, septal cell).
+__global__ void septal_weight_kernel(DevGeom g, GridGeom G, long long vox_begin, int nv, float rotation,
+                                     long long n_sep, float* __restrict__ ws)
+{
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= (long long)nv * n_sep) return;
+    const int vi = (int)(i / n_sep);
+    const long long j = i - (long long)vi * n_sep;
+    int m;
+    double p[3], I3[3];
+    septal_point(G, j, m, p);
+    voxel_centre64(g, vox_begin + vi, rotation, I3[0], I3[1], I3[2]);
+    double at = 0.0, ape = 0.0, ac = 0.0;
+    for (int mm = 0; mm < G.n_layers; ++mm) layer_path64(g, G, mm, I3, p, mm == m ? 2 : 0, at, ape, ac);
+    const GridLayer& L = G.layer[m];
+    const double r2 = (p[0] - I3[0]) * (p[0] - I3[0]) + (p[1] - I3[1]) * (p[1] - I3[1]) + (p[2] - I3[2]) * (p[2] - I3[2]);
+    const double vcell = L.cx * L.cy * L.cz;
+    ws[i] = (float)(vcell / (4.0 * 3.14159265358979323846 * r2) * exp(-at) * (double)L.mu_c);
+}
+
+// Septal cells of layer m: cell centre outside every hole of the layer.
+__global__ void septal_mark_kernel(DevGeom g, GridLayer L, unsigned char* __restrict__ flag)
+{
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= L.nx * L.ny * L.nz) return;
+    const int ix = c % L.nx, iy = (c / L.nx) % L.ny, iz = c / (L.nx * L.ny);
+    const double x = L.x0 + ((double)ix + 0.5) * L.cx, y = L.y0 + ((double)iy + 0.5) * L.cy;
+    const double z = L.z0 + ((double)iz + 0.5) * L.cz;
+    unsigned char sep = 1;
+    for (int j = L.hole_begin; j < L.hole_begin + L.hole_count && sep; ++j) {
+        const D4 a = g.t64.hole_a[j];
+        const double r = g.t64.hole_b[j].x;
+        const double dx = x - a.x, dz = z - a.w;
+        if (dx * dx + dz * dz <= r * r && y >= a.y && y <= a.z) sep = 0;
+    }
+    flag[c] = sep;
+}
+
+struct GridSum {
+    int det_begin, det_count;            // rows of this launch
+    long long vox_begin;
+    int nv;
+    float rotation;
+    int snx, sny, snz, n_sub;            // crystal cells
+    long long n_cry_pts, n_pts;          // D * n_sub; + septal cells
+    const float* wc;                     // [nv][D][n_sub]
+    const float* ws;                     // [nv][n_sep]
+    long long n_sep;
+    double* acc;                         // [det_count][nv]
+    float e0, lo, hi;
+    int same_window;
+    const double* kn_tab;
+    double kn_total;
+};
+
+// Detector-only terms of point p for detector d (double, rounded once): p in d's frame, the
+// absorption chord of the extended ray p -> d's centre in d, and the attenuation sums Lpe, Lc
+// of everything on the way (crystals other than d and the scattering crystal, and for septal
+// points the tungsten and hole media).  Returns false when the point does not scatter into d.
+__device__ bool point_terms(const DevGeom& g, const GridGeom& G, const GridSum& S, int d, long long pidx, float* out)
+{
+    double p[3];
+    int k = -1, m = -1;
+    double conv = 1.0;
+    if (pidx < S.n_cry_pts) {
+        k = (int)(pidx / S.n_sub);
+        if (k == d) return false;
+        const int sidx = (int)(pidx - (long long)k * S.n_sub);
+        const int nxy = S.snx * S.sny;
+        const int iz = sidx / nxy, rem = sidx - iz * nxy, iy = rem / S.snx, ix = rem - iy * S.snx;
+        const D4 P = g.t64.cry_pos[k], Z = g.t64.cry_size[k], T = g.t64.cry_trig[k];
+        const double xDs = -Z.x / 2.0 + ((double)ix + 0.5) / (double)S.snx * Z.x;
+        const double zDs = -Z.z / 2.0 + ((double)iz + 0.5) / (double)S.snz * Z.z;
+        const double yDs = -Z.y / 2.0 + ((double)iy + 0.5) / (double)S.sny * Z.y;
+        p[0] = P.x + (xDs * T.x - zDs * T.y);
+        p[1] = P.y + yDs;
+        p[2] = P.z + (xDs * T.y + zDs * T.x);
+        const float4 mu = __ldg(&g.cry.mu[k]);
+        conv = (double)mu.z / (double)mu.y;                   // photoelectric -> Compton weight
+    } else {
+        septal_point(G, pidx - S.n_cry_pts, m, p);
+    }
+    const D4 Pd = g.t64.cry_pos[d], Zd = g.t64.cry_size[d], Td = g.t64.cry_trig[d];
+    const double D3[3] = {Pd.x, Pd.y, Pd.z};                  // centre of the 1 x 1 x 1 division
+    const double ex = p[0] - Pd.x, ez = p[2] - Pd.z;
+    const double ps[3] = {ex * Td.z - ez * Td.w, p[1] - Pd.y, ex * Td.w + ez * Td.z};
+    const double lsd = sqrt(ps[0] * ps[0] + ps[1] * ps[1] + ps[2] * ps[2]);
+    // absorption: the ray p -> centre extended 1000 mm through d (scatter.cu:1420-1424)
+    const double labs = box_chord64(ps[0], ps[1], ps[2], -1000.0 * ps[0] / lsd, -1000.0 * ps[1] / lsd,
+                                    -1000.0 * ps[2] / lsd, -0.5 * Zd.x, -0.5 * Zd.y, -0.5 * Zd.z, 0.5 * Zd.x,
+                                    0.5 * Zd.y, 0.5 * Zd.z);
+    double lpe = 0.0, lc = 0.0;
+    // crystals on the way: bounding-sphere reject, then the reference box chord in double
+    const float fx = (float)p[0], fy = (float)p[1], fz = (float)p[2];
+    const float gx = (float)D3[0] - fx, gy = (float)D3[1] - fy, gz = (float)D3[2] - fz;
+    const float gl2 = gx * gx + gy * gy + gz * gz;
+    for (int a = 0; a < g.n_det; ++a) {
+        if (a == d || a == k) continue;
+        const float4 pa = __ldg(&g.cry.pos[a]);
+        const float ra = 0.5f * __ldg(&g.cry.size[a].w) + 1e-3f;
+        const float hx = pa.x - fx, hy = pa.y - fy, hz = pa.z - fz;
+        float t = (hx * gx + hy * gy + hz * gz) / gl2;
+        t = fminf(fmaxf(t, 0.0f), 1.0f);
+        const float qx = hx - t * gx, qy = hy - t * gy, qz = hz - t * gz;
+        if (qx * qx + qy * qy + qz * qz > ra * ra) continue;
+        const D4 Pa = g.t64.cry_pos[a], Za = g.t64.cry_size[a], Ta = g.t64.cry_trig[a];
+        const double ax = p[0] - Pa.x, az = p[2] - Pa.z, bx = D3[0] - Pa.x, bz = D3[2] - Pa.z;
+        const double la = box_chord64(ax * Ta.z - az * Ta.w, p[1] - Pa.y, ax * Ta.w + az * Ta.z,
+                                      bx * Ta.z - bz * Ta.w, D3[1] - Pa.y, bx * Ta.w + bz * Ta.z, -0.5 * Za.x,
+                                      -0.5 * Za.y, -0.5 * Za.z, 0.5 * Za.x, 0.5 * Za.y, 0.5 * Za.z);
+        if (la != 0.0) {
+            const float4 mu = __ldg(&g.cry.mu[a]);
+            lpe += (double)mu.y * la;
+            lc += (double)mu.z * la;
+        }
+    }
+    if (m >= 0) {                                             // tungsten and hole media on the way
+        double wt = 0.0;
+        for (int mm = 0; mm < G.n_layers; ++mm) layer_path64(g, G, mm, p, D3, mm == m ? 1 : 0, wt, lpe, lc);
+    }
+    out[0] = (float)ps[0];
+    out[1] = (float)ps[1];
+    out[2] = (float)ps[2];
+    out[3] = (float)lsd;
+    out[4] = (float)labs;
+    out[5] = (float)lpe;
+    out[6] = (float)lc;
+    out[7] = (float)conv;
+    return true;
+}
+
+__device__ __forceinline__ double kn_integral(const double* __restrict__ tab, double th)
+{
+    double G, F, P;
+    kn_tab_eval(tab, th, G, F, P);
+    return G;
+}
+
+__device__ __forceinline__ float cone_cos(float ax, float ay, float az, float la, float bx, float by, float bz)
+{
+    const float lb = sqrtf(bx * bx + by * by + bz * bz);
+    float c = (ax * bx + ay * by + az * bz) / (la * lb);
+    return fminf(fmaxf(c, -1.0f), 1.0f);
+}
+
+constexpr int kTerms = 8;
+
+struct GridSmem {
+    double acc[kGridDetTile][kGridMaxVox];      // block sums per (detector, voxel)
+    float wt[kGridMaxVox][kGridChunk];          // the chunk's weights
+    float terms[kTerms][kGridChunk];            // the chunk's detector-only terms
+    float4 vox_s[kGridMaxVox];                  // voxels in the current detector's frame
+};
+
+__global__ void __launch_bounds__(kGridThreads) grid_sum_kernel(DevGeom g, GridGeom G, GridSum S)
+{
+    extern __shared__ __align__(16) unsigned char grid_smem_raw[];
+    GridSmem& sm = *reinterpret_cast<GridSmem*>(grid_smem_raw);
+    auto& wt = sm.wt;
+    auto& terms = sm.terms;
+    auto& acc = sm.acc;
+    auto& vox_s = sm.vox_s;
+    const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
+    const int d0 = S.det_begin + blockIdx.y * kGridDetTile;
+    const int nd = min(kGridDetTile, S.det_begin + S.det_count - d0);
+    for (int i = t; i < kGridDetTile * kGridMaxVox; i += kGridThreads) (&acc[0][0])[i] = 0.0;
+    const float e0 = S.e0;
+    const float ang = S.rotation * g.angle_step;
+    const float crot = cosf(ang), srot = sinf(ang);
+    for (int ch = 0; ch < kGridChunksPerBlock; ++ch) {
+        const long long p0 = ((long long)blockIdx.x * kGridChunksPerBlock + ch) * kGridChunk;
+        if (p0 >= S.n_pts) break;
+        const long long pidx = p0 + t;
+        __syncthreads();
+        for (int vi = 0; vi < S.nv; ++vi) {                     // stage the chunk's weights
+            float w = 0.0f;
+            if (pidx < S.n_cry_pts) w = S.wc[(long long)vi * S.n_cry_pts + pidx];
+            else if (pidx < S.n_pts) w = S.ws[(long long)vi * S.n_sep + (pidx - S.n_cry_pts)];
+            wt[vi][t] = w;
+        }
+        for (int dl = 0; dl < nd; ++dl) {
+            const int d = d0 + dl;
+            const float4 P = __ldg(&g.cry.pos[d]), T = __ldg(&g.cry.trig[d]), M = __ldg(&g.cry.mu[d]);
+            const float4 Z = __ldg(&g.cry.size[d]);
+            __syncthreads();                                    // previous detector's terms are consumed
+            float tv[kTerms];
+            const bool ok = pidx < S.n_pts && point_terms(g, G, S, d, pidx, tv);
+            if (!ok) tv[7] = 0.0f;                              // zero weight factor: no contribution
+#pragma unroll
+            for (int q = 0; q < kTerms; ++q) terms[q][t] = ok ? tv[q] : (q == 3 ? 1.0f : 0.0f);
+            if (t < S.nv) {
+                float x, y, z, xs, ys, zs;
+                voxel_centre(g, S.vox_begin + t, crot, srot, x, y, z);
+                to_crystal_frame(P.x, P.y, P.z, T.z, T.w, x, y, z, xs, ys, zs);
+                vox_s[t] = make_float4(xs, ys, zs, 0.0f);
+            }
+            __syncthreads();
+            // window of crystal d (scatter.cu:1154-1163)
+            const float lo = S.same_window ? S.lo : (1 - M.w / 2.0f) * e0;
+            const float hi = S.same_window ? S.hi : (1 + M.w / 2.0f) * e0;
+            const float rdet = 0.5f * Z.w;                      // sqrt(w^2 + h^2 + t^2) / 2
+            const float hw = 0.5f * Z.x, ht = 0.5f * Z.y, hh = 0.5f * Z.z;
+            for (int vi = warp; vi < S.nv; vi += kGridThreads / 32) {
+                const float4 I = vox_s[vi];
+                double sum = 0.0;
+                for (int j = lane; j < kGridChunk; j += 32) {
+                    const float w = wt[vi][j] * terms[7][j];
+                    if (w == 0.0f) continue;
+                    const float px = terms[0][j], py = terms[1][j], pz = terms[2][j], lsd = terms[3][j];
+                    const float ax = px - I.x, ay = py - I.y, az = pz - I.z;      // v -> p
+                    const float la = sqrtf(ax * ax + ay * ay + az * az);
+                    const float cc = cone_cos(ax, ay, az, la, -px, -py, -pz);     // angle v -> p -> d
+                    const float es = e0 / (1.0f + (e0 / 511.0f) * (1.0f - cc));
+                    const float res = M.w * sqrtf(es / e0);
+                    if ((es * (1 + 2 * res / 2.35482f)) <= lo || (es * (1 - 2 * res / 2.35482f)) >= hi) continue;
+                    const float pwin = window_prob(es, res, lo, hi);
+                    const float sc = sqrtf(fmaxf(1.0f - cc * cc, 0.0f));
+                    float phi;
+                    if (lsd * sc * 2.0f <= rdet) phi = (float)(2.0 * 3.14159265358979323846);
+                    else phi = 4.0f * asinf(fminf(rdet / 2.0f / lsd / sc, 1.0f));
+                    // polar range over the corners of d, seen from p along v -> p (:1305-1335)
+                    float cmin = 2.0f, cmax = -2.0f;
+#pragma unroll
+                    for (int c = 0; c < 8; ++c) {
+                        const float ck = cone_cos(ax, ay, az, la, ((c & 1) ? hw : -hw) - px,
+                                                  ((c & 2) ? ht : -ht) - py, ((c & 4) ? hh : -hh) - pz);
+                        cmin = fminf(cmin, ck);
+                        cmax = fmaxf(cmax, ck);
+                    }
+                    float tmin = acosf(cmax), tmax = acosf(cmin);
+                    const float lthr = box_chord(I.x, I.y, I.z, px + 1000.0f * ax / la, py + 1000.0f * ay / la,
+                                                 pz + 1000.0f * az / la, -hw, -ht, -hh, hw, ht, hh);
+                    if (lthr > 0.001f) tmin = 0.0f;
+                    const double ratio = (kn_integral(S.kn_tab, (double)tmax) - kn_integral(S.kn_tab, (double)tmin)) /
+                                         S.kn_total;
+                    const float r1 = e0 / es, r3 = r1 * r1 * r1;
+                    const float att = terms[5][j] * r3 + terms[6][j] * r1;
+                    const float mpe_s = M.y * r3, mt_s = mpe_s + M.z * r1;
+                    const float absf = -expm1f(-terms[4][j] * mt_s) * mpe_s / mt_s;
+                    sum += (double)(w * phi / 2.0f) / 3.14159265358979323846 * ratio * (double)pwin *
+                           (double)expf(-att) * (double)absf;
+                }
+#pragma unroll
+                for (int off = 16; off > 0; off >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, off);
+                if (lane == 0) acc[dl][vi] += sum;
+            }
+        }
+    }
+    __syncthreads();
+    for (int i = t; i < nd * S.nv; i += kGridThreads) {
+        const int dl = i / S.nv, vi = i - dl * S.nv;
+        const double a = acc[dl][vi];
+        if (a != 0.0) atomicAdd(&S.acc[(long long)(d0 - S.det_begin + dl) * S.nv + vi], a);
+    }
+}
+
+__global__ void grid_store_kernel(const double* __restrict__ acc, int rows, int nv, float* __restrict__ out,
+                                  long long ld, long long col0)
+{
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= (long long)rows * nv) return;
+    const int r = (int)(i / nv), c = (int)(i - (long long)r * nv);
+    out[(long long)r * ld + col0 + c] = (float)acc[i];
+}
+
+struct DevMem {
+    void* p = nullptr;
+    ~DevMem() { if (p) cudaFree(p); }
+};
+
+int grid_division(float size, float cell)
+{
+    const int n = (int)std::ceil((double)size / (double)cell - 1e-9);
+    return n < 1 ? 1 : n;
+}
+
+}  // namespace
+
+}  // namespace sysmat
+
+using namespace sysmat;
+
+extern "C" SYSMAT_API int sysmat_scatter_grid(sysmat_ctx* ctx, int parts, float cell, float rotation, int det_begin,
+                                              int det_count, long long vox_begin, long long vox_count, float* d_out,
+                                              long long ld, void* stream)
+{
+    int rc = check_block(ctx, det_begin, det_count, vox_begin, vox_count, d_out, ld);
+    if (rc) return rc;
+    if (parts < 1 || parts > 3 || !(cell > 0.0f)) return SYSMAT_ERR_ARG;
+    if (ctx->h_phys.size() != (size_t)kNPhysics || ctx->h_det.size() != (size_t)kNDetector) return SYSMAT_ERR_ARG;
+    if ((parts & 2) && ctx->g.n_layers < 1) return SYSMAT_ERR_ARG;
+    if (ctx->g.hole_shape) return SYSMAT_ERR_ARG;               // circular holes only
+    if (det_count == 0 || vox_count == 0) return SYSMAT_OK;
+    cudaStream_t s = (cudaStream_t)stream;
+    const DevGeom& g = ctx->g;
+    const int D = g.n_det;
+    const float* pD = ctx->h_det.data();
+    const float* P = ctx->h_phys.data();
+    if ((int)std::floor(P[0] + 0.5f) != 1) {                   // no Compton scatter (scatter.cu:1144)
+        for (int r = 0; r < det_count; ++r)
+            CUDA_TRY(cudaMemsetAsync(d_out + (long long)r * ld, 0, sizeof(float) * vox_count, s));
+        return cudaStreamSynchronize(s) == cudaSuccess ? SYSMAT_OK : SYSMAT_ERR_CUDA;
+    }
+    // crystal cells: one division for every crystal
+    const int snx = grid_division(pD[4], cell), sny = grid_division(pD[5], cell), snz = grid_division(pD[6], cell);
+    for (int k = 1; k < D; ++k)
+        if (grid_division(pD[12 * k + 4], cell) != snx || grid_division(pD[12 * k + 5], cell) != sny ||
+            grid_division(pD[12 * k + 6], cell) != snz)
+            return SYSMAT_ERR_ARG;
+    const long long n_sub = (long long)snx * sny * snz;
+    if (n_sub > (1 << 20)) return SYSMAT_ERR_CAPACITY;
+
+    // septal cells of every layer (cell centres outside the layer's holes)
+    GridGeom G{};
+    G.n_layers = (parts & 2) ? g.n_layers : 0;
+    G.raw_col = ctx->d_col;
+    DevMem sep_mem;
+    long long n_sep = 0;
+    if (parts & 2) {
+        std::vector<double> lay(kLayer64 * (size_t)g.n_layers);
+        CUDA_TRY(cudaMemcpy(lay.data(), g.t64.layer, sizeof(double) * lay.size(), cudaMemcpyDeviceToHost));
+        long long cells_max = 0;
+        for (int m = 0; m < g.n_layers; ++m) {
+            const double* Ly = lay.data() + kLayer64 * m;
+            GridLayer& L = G.layer[m];
+            L.x0 = Ly[0]; L.y0 = Ly[2]; L.z0 = Ly[4];
+            L.nx = grid_division((float)(Ly[1] - Ly[0]), cell);
+            L.ny = grid_division((float)(Ly[3] - Ly[2]), cell);
+            L.nz = grid_division((float)(Ly[5] - Ly[4]), cell);
+            L.cx = (Ly[1] - Ly[0]) / L.nx; L.cy = (Ly[3] - Ly[2]) / L.ny; L.cz = (Ly[5] - Ly[4]) / L.nz;
+            L.hole_begin = g.layer[m].hole_begin;
+            L.hole_count = g.layer[m].hole_count;
+            L.mu_t = g.layer[m].mu_total; L.mu_pe = g.layer[m].mu_pe; L.mu_c = g.layer[m].mu_c;
+            const long long nc = (long long)L.nx * L.ny * L.nz;
+            if (nc > (1ll << 30)) return SYSMAT_ERR_CAPACITY;
+            cells_max = nc > cells_max ? nc : cells_max;
+        }
+        long long total_cells = 0;
+        for (int m = 0; m < g.n_layers; ++m) total_cells += (long long)G.layer[m].nx * G.layer[m].ny * G.layer[m].nz;
+        size_t temp = 0;
+        cub::DeviceSelect::Flagged(nullptr, temp, thrust::counting_iterator<int>(0), (unsigned char*)nullptr,
+                                   (int*)nullptr, (int*)nullptr, (int)cells_max, s);
+        DevMem flags, tmp, cnt;
+        if (cudaMalloc(&sep_mem.p, sizeof(int) * (size_t)total_cells) != cudaSuccess ||
+            cudaMalloc(&flags.p, (size_t)cells_max) != cudaSuccess || cudaMalloc(&tmp.p, temp + 16) != cudaSuccess ||
+            cudaMalloc(&cnt.p, sizeof(int)) != cudaSuccess)
+            return SYSMAT_ERR_NOMEM;
+        int* sep = (int*)sep_mem.p;
+        for (int m = 0; m < g.n_layers; ++m) {
+            const GridLayer& L = G.layer[m];
+            const int nc = L.nx * L.ny * L.nz;
+            septal_mark_kernel<<<(nc + 255) / 256, 256, 0, s>>>(g, L, (unsigned char*)flags.p);
+            size_t t2 = temp;
+            cub::DeviceSelect::Flagged(tmp.p, t2, thrust::counting_iterator<int>(0), (unsigned char*)flags.p,
+                                       sep + n_sep, (int*)cnt.p, nc, s);
+            int nsel = 0;
+            CUDA_TRY(cudaMemcpyAsync(&nsel, cnt.p, sizeof(int), cudaMemcpyDeviceToHost, s));
+            CUDA_TRY(cudaStreamSynchronize(s));
+            G.sep_begin[m] = n_sep;
+            n_sep += nsel;
+        }
+        for (int m = g.n_layers; m <= kMaxLayers; ++m) G.sep_begin[m] = n_sep;
+        G.sep_cell = sep;
+    }
+
+    // Klein-Nishina table at the photopeak (shared with sysmat_scatter)
+    if (!ctx->d_kn_tab || ctx->kn_e0 != P[7]) {
+        std::vector<double> tab(3 * (size_t)(kKnTable + 1));
+        kn_table_build((double)P[7], tab.data());
+        if (!ctx->d_kn_tab && cudaMalloc(&ctx->d_kn_tab, sizeof(double) * tab.size()) != cudaSuccess) {
+            ctx->d_kn_tab = nullptr;
+            return SYSMAT_ERR_NOMEM;
+        }
+        CUDA_TRY(cudaMemcpyAsync(ctx->d_kn_tab, tab.data(), sizeof(double) * tab.size(), cudaMemcpyHostToDevice, s));
+        CUDA_TRY(cudaStreamSynchronize(s));
+        ctx->kn_e0 = P[7];
+    }
+    double kn_total = 0.0;
+    CUDA_TRY(cudaMemcpy(&kn_total, ctx->d_kn_tab + kKnTable, sizeof(double), cudaMemcpyDeviceToHost));
+
+    // scratch: weights of one pass of voxels, the photoelectric block, the FP64 sums
+    const int nv_max = (int)(vox_count < kGridMaxVox ? vox_count : kGridMaxVox);
+    const long long n_cry_pts = (parts & 1) ? (long long)D * n_sub : 0;
+    DevMem wc, ws, pe, acc;
+    if ((n_cry_pts && cudaMalloc(&wc.p, sizeof(float) * (size_t)nv_max * (size_t)n_cry_pts) != cudaSuccess) ||
+        (n_sep && cudaMalloc(&ws.p, sizeof(float) * (size_t)nv_max * (size_t)n_sep) != cudaSuccess) ||
+        ((parts & 1) && cudaMalloc(&pe.p, sizeof(float) * (size_t)nv_max * D) != cudaSuccess) ||
+        cudaMalloc(&acc.p, sizeof(double) * (size_t)nv_max * det_count) != cudaSuccess)
+        return SYSMAT_ERR_NOMEM;
+
+    GridSum S{};
+    S.det_begin = det_begin;
+    S.det_count = det_count;
+    S.rotation = rotation;
+    S.snx = snx; S.sny = sny; S.snz = snz; S.n_sub = (int)n_sub;
+    S.n_cry_pts = n_cry_pts;
+    S.n_sep = n_sep;
+    S.n_pts = n_cry_pts + n_sep;
+    S.wc = (const float*)wc.p;
+    S.ws = (const float*)ws.p;
+    S.acc = (double*)acc.p;
+    S.e0 = P[7];
+    S.lo = P[5];
+    S.hi = P[6];
+    S.same_window = (int)std::floor(P[4] + 0.5f) > 0;
+    S.kn_tab = ctx->d_kn_tab;
+    S.kn_total = kn_total;
+    CUDA_TRY(cudaFuncSetAttribute(grid_sum_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(GridSmem)));
+    for (long long vb = vox_begin; vb < vox_begin + vox_count; vb += kGridMaxVox) {
+        const int nv = (int)((vox_begin + vox_count - vb) < kGridMaxVox ? (vox_begin + vox_count - vb) : kGridMaxVox);
+        if (parts & 1) {                                          // crystal-cell weights
+            PeLaunch L{};
+            L.det_begin = 0;
+            L.det_count = D;
+            L.vox_begin = vb;
+            L.vox_count = nv;
+            L.ld = nv;
+            L.rotation = rotation;
+            L.out = (float*)pe.p;
+            L.work_counter = ctx->d_counter;
+            L.status = ctx->d_status;
+            L.counters = nullptr;
+            L.smp.nx = snx; L.smp.ny = sny; L.smp.nz = snz;
+            L.smp.sx = L.smp.sy = L.smp.sz = 1;
+            L.sub_out = (float*)wc.p;
+            CUDA_TRY(cudaMemsetAsync(ctx->d_counter, 0, sizeof(unsigned long long), s));
+            CUDA_TRY(cudaMemsetAsync(ctx->d_status, 0, sizeof(int), s));
+            if (launch_pe_local_sampled(g, L, ctx->num_sms, s)) return SYSMAT_ERR_CUDA;
+            int st = 0;
+            CUDA_TRY(cudaMemcpyAsync(&st, ctx->d_status, sizeof(int), cudaMemcpyDeviceToHost, s));
+            CUDA_TRY(cudaStreamSynchronize(s));
+            if (st & kStatusCapacity) return SYSMAT_ERR_CAPACITY;
+        }
+        if (n_sep) {                                              // septal-cell weights
+            const long long n = (long long)nv * n_sep;
+            septal_weight_kernel<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(g, G, vb, nv, rotation, n_sep,
+                                                                              (float*)ws.p);
+            if (cudaGetLastError() != cudaSuccess) return SYSMAT_ERR_CUDA;
+        }
+        S.vox_begin = vb;
+        S.nv = nv;
+        CUDA_TRY(cudaMemsetAsync(acc.p, 0, sizeof(double) * (size_t)nv * det_count, s));
+        const long long pblocks = (S.n_pts + (long long)kGridChunk * kGridChunksPerBlock - 1) /
+                                  ((long long)kGridChunk * kGridChunksPerBlock);
+        dim3 grid((unsigned)pblocks, (unsigned)((det_count + kGridDetTile - 1) / kGridDetTile));
+        grid_sum_kernel<<<grid, kGridThreads, sizeof(GridSmem), s>>>(g, G, S);
+        if (cudaGetLastError() != cudaSuccess) return SYSMAT_ERR_CUDA;
+        const long long n = (long long)nv * det_count;
+        grid_store_kernel<<<(unsigned)((n + 255) / 256), 256, 0, s>>>((const double*)acc.p, det_count, nv, d_out, ld,
+                                                                       vb - vox_begin);
+        if (cudaGetLastError() != cudaSuccess) return SYSMAT_ERR_CUDA;
+    }
+    return cudaStreamSynchronize(s) == cudaSuccess ? SYSMAT_OK : SYSMAT_ERR_CUDA;
+}

@@ -1,9 +1,13 @@
 """Work partitioning of a system-matrix job across ranks (one process per GPU).
 
-Matrix elements are independent, so ranks share no data: each rank owns whole voxel
-planes (z) of the image grid for every detector, the unit the benchmark and the
-multi-GPU driver hand out.  No collective touches the data path; only the timing
+Matrix elements are independent, so ranks share no data: for the photoelectric matrix each
+rank owns whole voxel planes (z) of the image grid for every detector, the unit the benchmark
+and the multi-GPU driver hand out.  No collective touches the data path; only the timing
 reduction (max over ranks) crosses ranks.
+
+Crystal scatter reads the photoelectric element PE[k, v] of every crystal k at the element's
+own voxel v, so a rank that owns a block of voxel columns computes the PE columns of that
+block itself and needs nothing from the other ranks: no all-gather of the PE matrix.
 """
 from __future__ import annotations
 
@@ -24,3 +28,9 @@ def detector_slab(n_det: int, rank: int, world: int) -> tuple[int, int]:
     base, extra = divmod(n_det, world)
     begin = rank * base + min(rank, extra)
     return begin, base + (1 if rank < extra else 0)
+
+
+def voxel_block(n_vox: int, rank: int, world: int) -> tuple[int, int]:
+    """Contiguous voxel columns [begin, begin + count) of `rank` for the scatter path (the
+    photoelectric columns it needs are its own); sizes differ by at most one."""
+    return detector_slab(n_vox, rank, world)

@@ -22,6 +22,7 @@ ERRORS = {-1: "SYSMAT_ERR_ARG", -2: "SYSMAT_ERR_CUDA", -3: "SYSMAT_ERR_CAPACITY"
 MODE_REFERENCE = 0
 MODE_PRECISE = 1
 MODE_FP64 = 2
+MODE_LOCAL = 3
 THETA_N = 7
 THETA_NAMES = ("mu_w", "mu_crystal", "radius", "dx", "dy", "dz", "tilt")
 SCATTER_CRYSTAL = 1
@@ -38,7 +39,8 @@ EXPORTS = ("PESysMatGen", "scatter", "scatter_collimator", "scatter_crystal", "s
            "sysmat_csr_fill", "sysmat_pe_work", "sysmat_batch_create", "sysmat_batch_set_tiles",
            "sysmat_batch_get_tiles", "sysmat_batch_tune", "sysmat_batch_run", "sysmat_batch_destroy",
            "sysmat_batch", "sysmat_scatter_prepare_native", "sysmat_set_hole_shapes", "sysmat_pe_csr_file", "sysmat_project", "sysmat_vjp", "sysmat_backproject",
-           "sysmat_measure_peaks", "sysmat_ell_chords", "sysmat_pe_sampled",
+           "sysmat_measure_peaks", "sysmat_ell_chords", "sysmat_pe_sampled", "sysmat_scatter_grid",
+           "sysmat_scatter_batch_create", "sysmat_scatter_batch_run", "sysmat_scatter_batch_destroy",
            "sysmat_error_string", "sysmat_version")
 
 _fp = ctypes.POINTER(ctypes.c_float)
@@ -123,6 +125,13 @@ def lib():
             "sysmat_backproject": ([_vp, ctypes.c_float, ctypes.c_int, ctypes.c_int, _vp, _vp, _vp],
                                    ctypes.c_int),
             "sysmat_ell_chords": ([_vp, _vp, ctypes.c_int, _vp], ctypes.c_int),
+            "sysmat_scatter_batch_create": ([ctypes.POINTER(_vp), _vp, ctypes.c_int, _vp, ctypes.c_int, _vp],
+                                            ctypes.c_int),
+            "sysmat_scatter_batch_run": ([_vp, _vp], ctypes.c_int),
+            "sysmat_scatter_batch_destroy": ([_vp], ctypes.c_int),
+            "sysmat_scatter_grid": ([_vp, ctypes.c_int, ctypes.c_float, ctypes.c_float, ctypes.c_int, ctypes.c_int,
+                                     ctypes.c_longlong, ctypes.c_longlong, _vp, ctypes.c_longlong, _vp],
+                                    ctypes.c_int),
             "sysmat_error_string": ([ctypes.c_int], ctypes.c_char_p),
             "sysmat_version": ([], ctypes.c_char_p),
         }
@@ -399,11 +408,85 @@ def _context_set_hole_shapes(self, shapes=None):
            "sysmat_set_hole_shapes")
 
 
+def _context_scatter_columns(self, out, vox_begin, vox_count, parts=SCATTER_CRYSTAL | SCATTER_COLLIMATOR,
+                             hole_model=HOLE_MODEL_COMBINED, rotation=0.0, pe=None, stream=None):
+    """Scatter for every detector over voxel columns [vox_begin, vox_begin + vox_count) with the
+    photoelectric columns it reads computed here (the unit a rank owns when voxels are split
+    across ranks: no PE exchange).  The pair tables must be prepared.  `out`: CUDA float32,
+    n_det rows x vox_count; `pe`: optional n_det x n_vox scratch (its other columns are left
+    as they are).  Returns `out`."""
+    import torch
+    if pe is None:
+        pe = torch.zeros((self.n_det, self.n_vox), dtype=torch.float32, device=out.device)
+    if parts & SCATTER_CRYSTAL:
+        self.pe(pe[:, vox_begin:vox_begin + vox_count], rotation=rotation, vox_begin=vox_begin, vox_count=vox_count,
+                stream=stream)
+    return self.scatter(out, pe, parts=parts, hole_model=hole_model, rotation=rotation, vox_begin=vox_begin,
+                        vox_count=vox_count, stream=stream)
+
+
+def _context_scatter_grid(self, out, parts=SCATTER_CRYSTAL | SCATTER_COLLIMATOR, cell=0.25, rotation=0.0,
+                          det_begin=0, det_count=None, vox_begin=0, vox_count=None, stream=None):
+    """Grid scatter model (sysmat_scatter_grid): scatter points on a `cell` mm grid inside the
+    crystals (parts bit SCATTER_CRYSTAL) and the collimator's tungsten (SCATTER_COLLIMATOR),
+    FP64 sums per element.  `out`: CUDA float32, det_count rows."""
+    det_count = self.n_det - det_begin if det_count is None else det_count
+    vox_count = self.n_vox - vox_begin if vox_count is None else vox_count
+    ld = out.stride(0) if out.dim() == 2 else vox_count
+    _check(lib().sysmat_scatter_grid(self.handle, int(parts), float(cell), float(rotation), det_begin, det_count,
+                                     vox_begin, vox_count, _ptr(out), ld, _stream(stream)), "sysmat_scatter_grid")
+    return out
+
+
+Context.scatter_grid = _context_scatter_grid
+Context.scatter_columns = _context_scatter_columns
 Context.set_hole_shapes = _context_set_hole_shapes
 Context.pe_csr_file = _context_pe_csr_file
 Context.project = _context_project
 Context.vjp = _context_vjp
 Context.backproject = _context_backproject
+
+
+class ScatterItem(ctypes.Structure):
+    """sysmat_scatter_item: one scatter task (what one sysmat_scatter call takes)."""
+    _fields_ = [("ctx", ctypes.c_int), ("parts", ctypes.c_int), ("hole_model", ctypes.c_int),
+                ("rotation", ctypes.c_float), ("d_pe", ctypes.c_void_p), ("det_begin", ctypes.c_int),
+                ("det_count", ctypes.c_int), ("vox_begin", ctypes.c_longlong), ("vox_count", ctypes.c_longlong),
+                ("d_out", ctypes.c_void_p), ("ld", ctypes.c_longlong)]
+
+
+class ScatterBatchPlan:
+    """Many scatter tasks in one persistent launch (sysmat_scatter_batch_*).  items: tuples
+    (ctx_index, parts, hole_model, rotation, pe, det_begin, det_count, vox_begin, vox_count, out)
+    with `pe` a CUDA float32 PE matrix (or None without the crystal part) and `out` a CUDA
+    float32 tensor of det_count rows.  Keep the contexts, PE matrices and outputs alive."""
+
+    def __init__(self, contexts, items, stream=None):
+        self._keep = (list(contexts), [(it[4], it[9]) for it in items])
+        arr = (ScatterItem * max(len(items), 1))()
+        for k, (c, parts, model, rot, pe, d0, nd, v0, nv, out) in enumerate(items):
+            ld = out.stride(0) if out.dim() == 2 else nv
+            arr[k] = ScatterItem(int(c), int(parts), int(model), float(rot), pe.data_ptr() if pe is not None else 0,
+                                 int(d0), int(nd), int(v0), int(nv), out.data_ptr(), int(ld))
+        ctxs = (_vp * len(contexts))(*[c.handle.value for c in contexts])
+        h = ctypes.c_void_p()
+        _check(lib().sysmat_scatter_batch_create(ctypes.byref(h), ctxs, len(contexts), arr, len(items),
+                                                 _stream(stream)), "sysmat_scatter_batch_create")
+        self.handle = h
+
+    def run(self, stream=None):
+        _check(lib().sysmat_scatter_batch_run(self.handle, _stream(stream)), "sysmat_scatter_batch_run")
+
+    def close(self):
+        if self.handle:
+            lib().sysmat_scatter_batch_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 def _batch_items(contexts, items):

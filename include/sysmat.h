@@ -50,6 +50,15 @@ extern "C" {
  * chords, attenuation, exponentials, solid angle; elliptical holes included); no reference
  * counterpart.  Taken by sysmat_pe, sysmat_pe_csr_file and batched launches. */
 #define SYSMAT_MODE_FP64 2
+/* The reference's element program in FP32 arithmetic that stays within 1e-5 of its FP64
+ * evaluation: large and shared quantities (voxel, crystal and hole positions relative to the
+ * ray) are formed in double once per element, hole chords are y-extents in the hole's own
+ * frame, the septal length is (T - sum of extents) / cos, crystal and self-attenuation chords
+ * are measured from the sub-element, and the sub-element contributions are summed with
+ * compensated (Neumaier) summation.  No reference counterpart.  Taken by sysmat_pe and
+ * sysmat_pe_csr_file, for circular holes (a context with elliptical hole shapes returns
+ * SYSMAT_ERR_ARG). */
+#define SYSMAT_MODE_LOCAL 3
 
 /* Scatter parts (bit mask) and collimator solid-angle models. */
 #define SYSMAT_SCATTER_CRYSTAL 1
@@ -154,6 +163,49 @@ SYSMAT_API int sysmat_scatter_prepare(sysmat_ctx* ctx, int parts, const uint32_t
  * from the reference's relationship predicate evaluated for every hole (no bitmap file).
  * Use with hole_model SYSMAT_HOLE_MODEL_NATIVE; synchronises `stream` once. */
 SYSMAT_API int sysmat_scatter_prepare_native(sysmat_ctx* ctx, int parts, const uint32_t* d_bm_crystal, void* stream);
+
+/* Primary Compton scatter with scatter points on a grid (no reference counterpart; the
+ * reference scatters at one point per crystal centre and one per layer-0 hole centre,
+ * ScatterGen_RayTracing_CircularHole/scatter.cu:1218-1223, :1707-1716).  Scatter points are
+ * the centres of cells of side `cell` mm (0.25 for the configurations here) inside every
+ * crystal (parts bit SYSMAT_SCATTER_CRYSTAL; weight = the cell's photoelectric contribution
+ * from the voxel in the local-coordinate FP32 form times mu_C / mu_pe) and inside the
+ * tungsten of every collimator layer (bit SYSMAT_SCATTER_COLLIMATOR; weight = V / (4 pi r^2)
+ * exp(-attenuation to the cell) mu_C).  Each item is the reference's scatter item with that
+ * scatter point, every crystal on the way (and the tungsten, for septal points) as
+ * attenuator at the scattered energy, and the exact Klein-Nishina fraction; each element
+ * sums its ~10^6 items in FP64.  Every crystal must have the same cell division; circular
+ * holes only.  Needs no PE matrix or bitmaps.  Synchronous on `stream` (it allocates and
+ * frees its scratch). */
+/* Batched scatter (no reference counterpart; the reference computes one geometry per call,
+ * scatter.cu:2169-2194, :2303-2329): many scatter tasks, each what one sysmat_scatter call
+ * takes, in one persistent launch over a work queue, replayed as a CUDA graph.  Every element
+ * equals the per-task sysmat_scatter element bit for bit.  The plan keeps pointers to the
+ * contexts' pair tables, PE matrices and outputs: keep them alive and prepared as they were at
+ * creation while the plan is used.  Creation may synchronise `stream` once (Klein-Nishina
+ * tables); runs are asynchronous on `stream`. */
+typedef struct sysmat_scatter_item {
+    int ctx;                 /* index into the ctxs array */
+    int parts;               /* SYSMAT_SCATTER_* bits */
+    int hole_model;          /* SYSMAT_HOLE_MODEL_* (as prepared) */
+    float rotation;
+    const float* d_pe;       /* the rotation's PE matrix (D x V), for the crystal part */
+    int det_begin, det_count;
+    long long vox_begin, vox_count;
+    float* d_out;
+    long long ld;
+} sysmat_scatter_item;
+
+typedef struct sysmat_scatter_plan sysmat_scatter_plan;
+
+SYSMAT_API int sysmat_scatter_batch_create(sysmat_scatter_plan** plan, sysmat_ctx* const* ctxs, int n_ctx,
+                                           const sysmat_scatter_item* items, int n_items, void* stream);
+SYSMAT_API int sysmat_scatter_batch_run(sysmat_scatter_plan* plan, void* stream);
+SYSMAT_API int sysmat_scatter_batch_destroy(sysmat_scatter_plan* plan);
+
+SYSMAT_API int sysmat_scatter_grid(sysmat_ctx* ctx, int parts, float cell, float rotation, int det_begin,
+                                   int det_count, long long vox_begin, long long vox_count, float* d_out,
+                                   long long ld, void* stream);
 
 /* Primary-Compton scatter block (parts must have been prepared).  d_pe: the D x V
  * photoelectric matrix (row stride V) the crystal part reads.  hole_model:

@@ -52,6 +52,12 @@ def lib():
         L.oracle_pe_sampled.argtypes = [_fp, _fp, _fp, _fp, _ip, _ip, ctypes.c_int, _ip, ctypes.c_int,
                                         ctypes.c_longlong, ctypes.c_longlong, _dp, ctypes.c_int]
         L.oracle_pe_sampled.restype = ctypes.c_int
+        L.oracle_pe_local.argtypes = [_fp, _fp, _fp, _ip, ctypes.c_int, ctypes.c_longlong, ctypes.c_longlong, _dp,
+                                      ctypes.c_int]
+        L.oracle_pe_local.restype = ctypes.c_int
+        L.oracle_scatter_grid.argtypes = [_fp, _fp, _fp, _fp, ctypes.c_int, ctypes.c_double, _ip, ctypes.c_int,
+                                          ctypes.c_longlong, ctypes.c_longlong, _dp, ctypes.c_int]
+        L.oracle_scatter_grid.restype = ctypes.c_int
         for name in ("oracle_box_chord", "oracle_box_chord_inside", "oracle_cyl_chord", "oracle_ell_chord"):
             getattr(L, name).argtypes = [ctypes.c_int, _dp]
             getattr(L, name).restype = ctypes.c_double
@@ -98,6 +104,21 @@ def pe(geo, prec=64, dets=None, v0=0, nv=None, threads=0, counts=False, shapes=N
     if rc:
         raise RuntimeError(f"oracle_pe failed ({rc})")
     return (out, cnt) if counts else out
+
+
+def pe_local(geo, dets=None, v0=0, nv=None, threads=0):
+    """PE elements (len(dets), nv) of the local-coordinate FP32 form (oracle_local.h), as float
+    values widened to float64."""
+    nv = geo.n_vox - v0 if nv is None else nv
+    c, pc = _f32(geo.collimator)
+    d, pd = _f32(geo.detector)
+    i, pi = _f32(geo.image)
+    dd, pdd = _dets(geo, dets)
+    out = np.zeros((dd.size, nv), dtype=np.float64)
+    rc = lib().oracle_pe_local(pc, pd, pi, pdd, dd.size, v0, nv, out.ctypes.data_as(_dp), threads)
+    if rc:
+        raise RuntimeError(f"oracle_pe_local failed ({rc})")
+    return out
 
 
 def pe_sampled(geo, crystal_div, voxel_sub, prec=64, dets=None, v0=0, nv=None, threads=0, shapes=None):
@@ -164,6 +185,23 @@ def scatter(geo, pe_matrix, part, bitmap, prec=64, dets=None, v0=0, nv=None, thr
                               dd.size, v0, nv, out.ctypes.data_as(_dp), threads)
     if rc:
         raise RuntimeError(f"oracle_scatter failed ({rc})")
+    return out
+
+
+def scatter_grid(geo, parts=3, cell=0.25, dets=None, v0=0, nv=None, threads=0):
+    """Elements (len(dets), nv) of the grid scatter model (oracle_grid.h) in double: parts 1 =
+    crystal cells, 2 = septal cells; cell = grid step in mm."""
+    nv = geo.n_vox - v0 if nv is None else nv
+    c, pc = _f32(geo.collimator)
+    d, pd = _f32(geo.detector)
+    i, pi = _f32(geo.image)
+    p, pp = _f32(geo.physics)
+    dd, pdd = _dets(geo, dets)
+    out = np.zeros((dd.size, nv), dtype=np.float64)
+    rc = lib().oracle_scatter_grid(pc, pd, pi, pp, int(parts), float(cell), pdd, dd.size, v0, nv,
+                                   out.ctypes.data_as(_dp), threads)
+    if rc:
+        raise RuntimeError(f"oracle_scatter_grid failed ({rc})")
     return out
 
 

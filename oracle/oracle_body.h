@@ -285,7 +285,7 @@ static inline void FN(to_frame)(const FN(crystal)* c, REAL x, REAL y, REAL z,
  * reference's 8 x 16 x 8).                                                              */
 
 static REAL FN(pe_element_at)(const ogeo* g, int d, REAL xI, REAL yI, REAL zI, int* cand_c, int* cand_h,
-                              int* ncand_h, pe_counts* cnt)
+                              int* ncand_h, pe_counts* cnt, REAL* per_sub)
 {
     const float* C = g->C;
     const REAL fov = (REAL)g->I[11];
@@ -430,6 +430,7 @@ static REAL FN(pe_element_at)(const ogeo* g, int d, REAL xI, REAL yI, REAL zI, i
         REAL labs = FN(box_chord)(xIs, yIs, zIs, xt, yt, zt, ux1, uy1, uz1, ux2, uy2, uz2);
         REAL absf = ((REAL)1.0f - EXP(-labs * cd.mu_t)) * cd.mu_pe / cd.mu_t;
         if (cnt) cnt->subelements++;
+        if (per_sub) per_sub[((long long)iz * NXS + ix) * NYS + iy] = eff * sa * absf;
         sum = sum + eff * sa * absf;
     }
     return sum;
@@ -445,7 +446,7 @@ static REAL FN(pe_element)(const ogeo* g, int d, long long v, int* cand_c, int* 
     REAL xI, yI, zI;
     if (sx == 1 && sy == 1 && sz == 1) {
         FN(voxel_centre)(g, v, &xI, &yI, &zI);
-        return FN(pe_element_at)(g, d, xI, yI, zI, cand_c, cand_h, ncand_h, cnt);
+        return FN(pe_element_at)(g, d, xI, yI, zI, cand_c, cand_h, ncand_h, cnt, NULL);
     }
     double acc = 0.0;
     for (int jz = 0; jz < sz; ++jz)
@@ -453,7 +454,7 @@ static REAL FN(pe_element)(const ogeo* g, int d, long long v, int* cand_c, int* 
     for (int jx = 0; jx < sx; ++jx) {
         FN(voxel_point)(g, v, ((REAL)jx + (REAL)0.5f) / (REAL)sx, ((REAL)jy + (REAL)0.5f) / (REAL)sy,
                         ((REAL)jz + (REAL)0.5f) / (REAL)sz, &xI, &yI, &zI);
-        acc += (double)FN(pe_element_at)(g, d, xI, yI, zI, cand_c, cand_h, ncand_h, cnt);
+        acc += (double)FN(pe_element_at)(g, d, xI, yI, zI, cand_c, cand_h, ncand_h, cnt, NULL);
     }
     return (REAL)(acc / (double)(sx * sy * sz));
 }

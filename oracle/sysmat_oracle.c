@@ -78,6 +78,20 @@ typedef struct {
 #define FABS fabs
 #include "oracle_body.h"
 
+#undef REAL
+#undef SUFFIX
+#undef SQRT
+#undef EXP
+#undef COS
+#undef SIN
+#undef ACOS
+#undef ASIN
+#undef ERF
+#undef FABS
+
+#include "oracle_local.h"
+#include "oracle_grid.h"
+
 /* Decode counts the way the reference kernels do (PESysMatGen.cu:964-1013,
  * scatter.cu:1555, :1108-1110). */
 static int parse(ogeo* g, const float* C, const float* D, const float* I, const float* P)
@@ -166,6 +180,55 @@ int oracle_pe_sampled(const float* C, const float* D, const float* I, const floa
         g.vsub[k] = vsub[k];
     }
     return run_pe(&g, prec, dets, ndet, v0, nv, out, NULL, nthreads);
+}
+
+/* PE elements of the local-coordinate FP32 form (oracle_local.h; the reference's sampling:
+ * 8 x 16 x 8 sub-elements, voxel centres), as float values widened to double. */
+int oracle_pe_local(const float* C, const float* D, const float* I, const int* dets, int ndet, long long v0,
+                    long long nv, double* out, int nthreads)
+{
+    ogeo g;
+    if (parse(&g, C, D, I, NULL)) return -1;
+    if (nthreads > 0) omp_set_num_threads(nthreads);
+    long long total = (long long)ndet * nv;
+    int err = 0;
+#pragma omp parallel
+    {
+        int* cc = (int*)malloc(sizeof(int) * (size_t)(g.ncry + 1));
+        int* ch = (int*)malloc(sizeof(int) * (size_t)(g.nholes + 1));
+        lhole* lh = (lhole*)malloc(sizeof(lhole) * (size_t)(g.nholes + 1));
+        lcry* lc = (lcry*)malloc(sizeof(lcry) * (size_t)(g.ncry + 1));
+        int nch[MAX_LAYERS];
+        if (!cc || !ch || !lh || !lc) err = 1;
+#pragma omp for schedule(dynamic, 16)
+        for (long long e = 0; e < total; ++e) {
+            if (!cc || !ch || !lh || !lc) continue;
+            int d = dets[e / nv];
+            long long v = v0 + e % nv;
+            double xI, yI, zI;
+            voxel_centre_f64(&g, v, &xI, &yI, &zI);
+            out[e] = (double)pe_element_local(&g, d, xI, yI, zI, cc, ch, nch, lh, lc);
+        }
+        free(cc);
+        free(ch);
+        free(lh);
+        free(lc);
+    }
+    return err ? -2 : 0;
+}
+
+/* Elements of the grid scatter model (oracle_grid.h) for detectors dets[0..ndet) and voxels
+ * [v0, v0+nv), in double; parts: 1 crystal cells, 2 septal cells; cell: grid step (mm).  Each
+ * element spreads its cells over the threads. */
+int oracle_scatter_grid(const float* C, const float* D, const float* I, const float* P, int parts, double cell,
+                        const int* dets, int ndet, long long v0, long long nv, double* out, int nthreads)
+{
+    ogeo g;
+    if (parse(&g, C, D, I, P)) return -1;
+    if (!(cell > 0)) return -1;
+    for (long long e = 0; e < (long long)ndet * nv; ++e)
+        out[e] = grid_element(&g, parts, dets[e / nv], v0 + e % nv, cell, nthreads);
+    return 0;
 }
 
 int oracle_pe(const float* C, const float* D, const float* I, int prec, const int* dets, int ndet,

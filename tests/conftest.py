@@ -31,6 +31,11 @@ sysmat = _load("sysmat_binding", os.path.join(PKG_DIR, "sysmat.py"))
 import oracle  # noqa: E402  (test infrastructure)
 
 
+def sharding_module():
+    """The package's work-partitioning module (importable in spawned test ranks)."""
+    return _load("sysmat_sharding", os.path.join(PKG_DIR, "sharding.py"))
+
+
 def pytest_configure(config):
     config.addinivalue_line("markers", "gpu: needs a CUDA GPU (B200) and the built libsysmat.so")
 

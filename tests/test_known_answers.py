@@ -56,9 +56,10 @@ def closed_form(collimator, div=(8, 16, 8)):
 
 
 @pytest.mark.parametrize("collimator", ["none", "plate", "hole"])
-@pytest.mark.parametrize("prec, tol", [(64, 1e-10), (32, 2e-6)])
+@pytest.mark.parametrize("prec, tol", [(64, 1e-10), (32, 2e-6), ("local", 2e-7)])
 def test_oracle_known_answer(collimator, prec, tol):
-    a = float(oracle.pe(_geometry(collimator), prec=prec)[0, 0])
+    g = _geometry(collimator)
+    a = float((oracle.pe_local(g) if prec == "local" else oracle.pe(g, prec=prec))[0, 0])
     b = closed_form("none" if collimator == "hole" else collimator)
     assert abs(a - b) <= tol * b, (a, b, abs(a - b) / b)
 
@@ -75,7 +76,8 @@ def test_device_known_answer(gpu, collimator):
     ctx = sysmat.Context(_geometry(collimator))
     b = closed_form("none" if collimator == "hole" else collimator)
     out = torch.empty((1, 1), dtype=torch.float32, device="cuda")
-    for mode, tol in ((sysmat.MODE_REFERENCE, 2e-6), (sysmat.MODE_PRECISE, 2e-6), (sysmat.MODE_FP64, 1e-7)):
+    for mode, tol in ((sysmat.MODE_REFERENCE, 2e-6), (sysmat.MODE_PRECISE, 2e-6), (sysmat.MODE_FP64, 1e-7),
+                      (sysmat.MODE_LOCAL, 2e-7)):
         ctx.pe(out, mode=mode)
         a = float(out.cpu()[0, 0])
         assert abs(a - b) <= tol * b, (mode, a, b, abs(a - b) / b)

@@ -303,3 +303,35 @@ def test_sampled_form_converges_with_the_division():
     e8 = np.abs(m[0] - m[2]).sum()
     e16 = np.abs(m[1] - m[2]).sum()
     assert e16 < 0.6 * e8, (e8, e16)
+
+
+@pytest.mark.parametrize("name", ["mini0", "mini1r2", "mini2w"])
+def test_local_form_within_1e5_of_fp64(name):
+    """The local-coordinate FP32 scheme (oracle_local.h, the CPU twin of SYSMAT_MODE_LOCAL)
+    stays within 1e-5 of the FP64 restatement where the reference's float program does not."""
+    geo, z = golden(name)
+    o64 = oracle.pe(geo, prec=64)
+    r = rel_err(oracle.pe_local(geo), o64)
+    assert r.max() <= 1e-5 and np.median(r) < 1e-6, (r.max(), np.median(r))
+    assert r.max() < rel_err(oracle.pe(geo, prec=32), o64).max()
+
+
+def test_local_form_config2_sample_within_1e5_of_fp64():
+    g = geometry.voxel_slab(geometry.config2(), 16)
+    dets, v0, nv = np.arange(8, 4096, 512), 96 * 48, 96
+    o64 = oracle.pe(g, prec=64, dets=dets, v0=v0, nv=nv)
+    r = rel_err(oracle.pe_local(g, dets=dets, v0=v0, nv=nv), o64)
+    assert r.max() <= 1e-5, r.max()
+
+
+def test_grid_model_converges_as_the_cells_shrink():
+    """The grid scatter model (oracle_grid.h) is a discretisation: halving the 0.25 mm cell
+    changes each element by a few percent (the crystal cells' solid angle is the reference's
+    largest-face approximation, and septal cell centres fall in or out of holes), and the crystal
+    and septal parts are both present in a system whose crystals lie behind a tungsten plate."""
+    geo = geometry.mini(seed=3, nvox=(2, 1, 1), ncry=(2, 2), nholes=3)
+    for parts in (1, 2):
+        s1 = oracle.scatter_grid(geo, parts=parts, cell=0.125)
+        s2 = oracle.scatter_grid(geo, parts=parts, cell=0.0625)
+        assert s1.max() > 0
+        assert np.all(np.abs(s2 - s1) <= 0.1 * np.abs(s2)), parts
