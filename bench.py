@@ -202,12 +202,13 @@ def plane_geometry(g, n_planes, plane):
     return geometry.voxel_slab(g, plane) if n_planes > 1 else g
 
 
-def rel_err_stats(a, b, threshold=1e-5):
-    """max / median of |a - b| / max(|b|, tau), tau = 1e-6 * max|b| over the sample, and the
-    count of elements above `threshold`."""
+def rel_err_stats(a, b, scale=None, threshold=1e-5):
+    """max / median of |a - b| / max(|b|, tau), tau = 1e-6 * the matrix's largest element
+    (`scale`; the sample's own largest when not given), and the count of elements above
+    `threshold`."""
     a = np.asarray(a, dtype=np.float64).ravel()
     b = np.asarray(b, dtype=np.float64).ravel()
-    m = np.abs(b).max() if b.size else 0.0
+    m = float(scale) if scale is not None else (np.abs(b).max() if b.size else 0.0)
     tau = 1e-6 * m if m > 0 else 1e-300
     r = np.abs(a - b) / np.maximum(np.abs(b), tau)
     return {"max_rel_err": float(r.max()), "median_rel_err": float(np.median(r)),
@@ -324,7 +325,8 @@ def run_sysmat(args, rank, world, local):
     ctx.pe(out, rotation=0.0, det_count=D, vox_begin=acc_plane * nxy, vox_count=nxy, stream=stream)
     torch.cuda.synchronize()
     keep = {"pe": out[:, SAMPLE_ROW * int(g.image[0]):(SAMPLE_ROW + 1) * int(g.image[0])].cpu().numpy()
-            if n_planes > 1 else out.cpu().numpy(), "plane": acc_plane, "D": D}
+            if n_planes > 1 else out.cpu().numpy(), "plane": acc_plane, "D": D,
+            "pe_max": float(out.max().item())}
     del out, flush
     ctx.close()
 
@@ -449,7 +451,7 @@ def run_scatter(args, sysmat, torch, keep):
            "workload": "config3 primary Compton (crystal + collimator) on z-plane 8: 1024 crystals x "
                        "2304 voxels, 1024 layer-0 holes; value = scatter kernel on resident buffers, "
                        "value_with_prepare adds the pair-table preparation"}
-    keep["scatter"] = {"geo": g, "pe": pe.cpu().numpy(), "out": out.cpu().numpy(),
+    keep["scatter"] = {"geo": g, "pe": pe.cpu().numpy(), "out": out.cpu().numpy(), "max": float(out.max().item()),
                        "bc": bitmaps["c"].cpu().numpy().view(np.uint32),
                        "bh": bitmaps["h"].cpu().numpy().view(np.uint32)}
     del bitmaps
@@ -482,7 +484,7 @@ def run_scatter_grid(args, sysmat, torch, keep):
     out = torch.empty((ctx.n_det, ctx.n_vox), dtype=torch.float32, device="cuda")
     ctx.scatter_grid(out, cell=0.25)
     ms = _events(torch, lambda: ctx.scatter_grid(out, cell=0.25))
-    keep["scatter_grid"] = {"geo": g, "out": out.cpu().numpy()}
+    keep["scatter_grid"] = {"geo": g, "out": out.cpu().numpy(), "max": float(out.max().item())}
     nel = ctx.n_det * ctx.n_vox
     ctx.close()
     return {"value": nel / (ms * 1e-3), "unit": UNIT, "ms_per_step": ms, "summation": "FP64 per element",
@@ -576,7 +578,8 @@ def run_sampled(args, sysmat, torch, keep, rows=512):
     step()
     ms = _events(torch, step, n=2)
     nx = int(g.image[0])
-    keep["sampled"] = {"d0": d0, "out": out[:, SAMPLE_ROW * nx:(SAMPLE_ROW + 1) * nx].cpu().numpy()}
+    keep["sampled"] = {"d0": d0, "out": out[:, SAMPLE_ROW * nx:(SAMPLE_ROW + 1) * nx].cpu().numpy(),
+                       "max": float(out.max().item())}
     ctx.close()
     return {"value": rows * nxy / (ms * 1e-3), "unit": UNIT, "ms_per_step": ms, "rays_per_element": 8 * 32,
             "summation": "FP64",
@@ -752,7 +755,8 @@ def cpu_baseline(args, g, n_planes, keep):
                       f"{SAMPLE_ROW} of z-plane {plane}); FP64 oracle, OpenMP, {dt:.1f} s (FP32 twin on the "
                       f"same elements: {dt32:.1f} s)"}
     pe_gpu = keep["pe"][rows]
-    acc = {"pe": dict(rel_err_stats(pe_gpu, o64), vs="FP64 oracle",
+    scale = keep["pe_max"]                      # the plane's largest element: tau = 1e-6 of it
+    acc = {"pe": dict(rel_err_stats(pe_gpu, o64, scale), vs="FP64 oracle",
                       mode="reference (the reference's float program)",
                       bit_identical_to_fp32_twin=float(np.mean(pe_gpu == o32.astype(np.float32))),
                       sample=base["sample"])}
@@ -760,18 +764,18 @@ def cpu_baseline(args, g, n_planes, keep):
         f = keep["fp64"]
         sel = rows[(rows >= f["d0"]) & (rows < f["d0"] + f["out"].shape[0])]
         idx = np.searchsorted(rows, sel)
-        acc["fp64"] = dict(rel_err_stats(f["out"][sel - f["d0"]], o64[idx]), vs="FP64 oracle",
+        acc["fp64"] = dict(rel_err_stats(f["out"][sel - f["d0"]], o64[idx], scale), vs="FP64 oracle",
                            sample=f"{sel.size} of the crystals above x the same voxel row")
     if "local" in keep:
         f = keep["local"]
-        acc["local"] = dict(rel_err_stats(f["out"][rows], o64), vs="FP64 oracle", sample=base["sample"])
+        acc["local"] = dict(rel_err_stats(f["out"][rows], o64, scale), vs="FP64 oracle", sample=base["sample"])
     if "sampled" in keep:
         s = keep["sampled"]
         sel = np.arange(s["d0"] + 8, s["d0"] + s["out"].shape[0], 128)
         gs = geometry.voxel_slab(g, 16)
         os64 = oracle.pe_sampled(gs, (2, 8, 2), (2, 2, 2), prec=64, dets=sel, v0=nx * SAMPLE_ROW, nv=nx,
                                  threads=threads)
-        acc["sampled"] = dict(rel_err_stats(s["out"][sel - s["d0"]], os64), vs="FP64 oracle (sampled form)",
+        acc["sampled"] = dict(rel_err_stats(s["out"][sel - s["d0"]], os64, s["max"]), vs="FP64 oracle (sampled form)",
                               sample=f"crystals {sel.tolist()} x voxel row {SAMPLE_ROW} of z-plane 16")
     if "scatter" in keep:
         s = keep["scatter"]
@@ -782,14 +786,15 @@ def cpu_baseline(args, g, n_planes, keep):
         o = oracle.scatter(gs, s["pe"], "crystal", s["bc"], prec=64, dets=sel, v0=v3, nv=nx3, threads=threads)
         o += oracle.scatter(gs, s["pe"], "collimator", s["bh"], prec=64, dets=sel, v0=v3, nv=nx3,
                             threads=threads)
-        acc["scatter"] = dict(rel_err_stats(s["out"][sel][:, v3:v3 + nx3], o), vs="FP64 oracle",
+        acc["scatter"] = dict(rel_err_stats(s["out"][sel][:, v3:v3 + nx3], o, s["max"]), vs="FP64 oracle",
                               sample=f"crystals {sel.tolist()} x voxel row 24 of config3 z-plane 8 "
                                      "(the GPU's PE matrix and bitmaps as input)")
     if "scatter_grid" in keep:
         s = keep["scatter_grid"]
         d, v = 528, 22
         o = oracle.scatter_grid(s["geo"], parts=3, cell=0.25, dets=[d], v0=v, nv=1, threads=threads)
-        acc["scatter_grid"] = dict(rel_err_stats(s["out"][d:d + 1, v:v + 1], o), vs="FP64 definition of the grid model",
+        acc["scatter_grid"] = dict(rel_err_stats(s["out"][d:d + 1, v:v + 1], o, s["max"]),
+                                   vs="FP64 definition of the grid model",
                                    sample=f"crystal {d} x voxel {v} of the grid leg's voxel row")
     return base, acc
 
@@ -872,7 +877,8 @@ def run_reference(args, rank, world, local):
         if got is not None:
             gp = geometry.voxel_slab(g, acc_plane)
             o64 = oracle.pe(gp, prec=64, dets=rows, v0=nx * SAMPLE_ROW, nv=nx, threads=os.cpu_count() or 1)
-            res["accuracy"] = {"pe": dict(rel_err_stats(got, o64), vs="FP64 oracle",
+            scale = max(float(o.max()) for (p, _, _), o in outs.items() if p == acc_plane)
+            res["accuracy"] = {"pe": dict(rel_err_stats(got, o64, scale), vs="FP64 oracle",
                                           sample=f"{rows.size} crystals (every {SAMPLE_DET_STRIDE}th) x "
                                                  f"voxel row {SAMPLE_ROW} of z-plane {acc_plane}")}
     del outs

@@ -137,44 +137,43 @@ __device__ __forceinline__ float box_chord_near(const float P[3], const float q[
 }
 
 // Hole chord as a y-extent (see the file comment): the ray's offset from the hole axis at the
-// hole's entry plane is (u0, w0), its slopes are (rx, rz) per unit y, the hole spans
-// [0, th] in y from that plane, dy below the voxel.  Cap/side cases and thresholds follow
-// the reference (PESysMatGen.cu:688-799); the t parameters (length from the voxel: ta = dy *
-// sec, ...) enter only its threshold tests.
-__device__ __forceinline__ float hole_extent(float u0, float w0, float rx, float rz, float r, float th, float dy,
-                                             float sec, float tio, float ky)
+// hole's entry plane is (u0, w0), its slopes are (rx, rz) per unit y (a = rx^2 + rz^2, ia =
+// 1/a), the hole spans [0, th] in y from that plane, dy below the voxel.  Cap/side cases and
+// thresholds follow the reference (PESysMatGen.cu:688-799); the t parameters (length from the
+// voxel: ta = dy * sec, ...) enter only its threshold tests.  Offsets, slopes and the roots are
+// in double: near a tangent, and for a hole met far from where the ray enters the plate, the
+// chord is ill-conditioned in them, and float offsets or slopes would move it by ~1e-5 mm.
+__device__ __forceinline__ float hole_extent(double u0d, double w0d, double rxd, double rzd, double ad, double iad,
+                                             float r, float th, float dy, float sec, float tio, float ky)
 {
     if (fabsf(th) < kEps) return 0.0f;
-    const float u1 = u0 + rx * th, w1 = w0 + rz * th;
-    const bool fl = u0 * u0 + w0 * w0 <= r * r;
-    const bool fr = u1 * u1 + w1 * w1 <= r * r;
+    const double u1d = u0d + rxd * (double)th, w1d = w0d + rzd * (double)th;
+    const double r2 = (double)r * (double)r;
+    const bool fl = u0d * u0d + w0d * w0d <= r2;
+    const bool fr = u1d * u1d + w1d * w1d <= r2;
     if (fl && fr) {
         const float ta = dy * sec, tb = (dy + th) * sec;
         if (ta <= 0.0001f || tb <= 0.0001f) return 0.0f;
         if (ta >= tio || tb >= tio) return 0.0f;
         return th;
     }
-    const float a = rx * rx + rz * rz;
-    const float cross = u0 * rz - w0 * rx;
-    const float q = a * r * r - cross * cross;                 // b^2 - a c (Lagrange identity)
-    if (ky * ky * q <= 0.00001f) return 0.0f;                  // the reference's discriminant
-    const float b = u0 * rx + w0 * rz;
-    const float sq = sqrtf(q);
-    const float c = (u0 - r) * (u0 + r) + w0 * w0;
-    float s1, s2;                                              // roots without cancellation
-    if (b > 0.0f) { s1 = __fdividef(-b - sq, a); s2 = __fdividef(c, -b - sq); }
-    else          { s2 = __fdividef(-b + sq, a); s1 = __fdividef(c, -b + sq); }
-    float ea, eb;
+    const double cross = u0d * rzd - w0d * rxd;
+    const double qd = ad * r2 - cross * cross;                 // b^2 - a c (Lagrange identity)
+    if ((double)(ky * ky) * qd <= (double)0.00001f) return 0.0f;   // the reference's discriminant
+    const double bd = u0d * rxd + w0d * rzd;
+    const double sq = (double)sqrtf((float)qd);
+    const double s1 = (-bd - sq) * iad, s2 = (-bd + sq) * iad;
+    double ea, eb;
     if (!fl && !fr) {
-        if (!(s1 >= 0.0f && s2 <= th)) return 0.0f;
+        if (!(s1 >= 0.0 && s2 <= (double)th)) return 0.0f;
         ea = s1; eb = s2;
-    } else if (fl) { ea = 0.0f; eb = s2; }
-    else           { ea = s1; eb = th; }
-    const float t1 = (dy + ea) * sec, t2 = (dy + eb) * sec;
+    } else if (fl) { ea = 0.0; eb = s2; }
+    else           { ea = s1; eb = (double)th; }
+    const float t1 = (dy + (float)ea) * sec, t2 = (dy + (float)eb) * sec;
     if (t2 <= 0.0001f || t1 <= 0.0001f) return 0.0f;
     if (t2 >= tio || t1 >= tio) return 0.0f;
-    if (!fl && !fr) return __fdividef(2.0f * sq, a);
-    return eb - ea;
+    if (!fl && !fr) return (float)(2.0 * sq * iad);
+    return (float)(eb - ea);
 }
 
 // Copy kept entries [k0, k1) whose rectangle and capsule meet the round's slope box into the
@@ -221,9 +220,13 @@ __device__ __forceinline__ int fill_round_local(const DevGeom& g, WarpSmem& ws, 
                 const D4 a = g.t64.hole_a[id];
                 const float4 hb = __ldg(&g.hole.b[id]);
                 const double dy = a.y - E.yI;
-                ws.ra[pos] = make_float4((float)((E.xI - a.x) + L.rxc * dy), (float)((E.zI - a.w) + L.rzc * dy),
-                                         hb.x, hb.y);
-                ws.rb[pos] = make_float4((float)dy, (float)(a.z - a.y), 0.0f, 0.0f);
+                const double hx = (E.xI - a.x) + L.rxc * dy, hz = (E.zI - a.w) + L.rzc * dy;
+                ws.ra[pos] = make_float4((float)hx, (float)hz, hb.x, hb.y);
+                // the offsets in double, as the bit patterns of two floats each
+                ws.rb[pos] = make_float4((float)dy, (float)(a.z - a.y), __int_as_float(__double2hiint(hx)),
+                                         __int_as_float(__double2loint(hx)));
+                ws.rc[pos] = make_float4(__int_as_float(__double2hiint(hz)), __int_as_float(__double2loint(hz)),
+                                         0.0f, 0.0f);
                 ws.rl[pos] = layer_of_hole(g, id);
             } else {
                 const int o = id - g.n_holes;
@@ -252,6 +255,9 @@ struct RayL {
     float qx, qy, qz;            // sub-element centre minus the voxel
     float sq, sec, ky;           // ray length, 1 / cos, cos
     float drx, drz, rx, rz;      // slope difference to the central ray, slopes
+    double dsec;                 // 1 / cos in double (septal lengths: heavily attenuated rays)
+    double ddrx, ddrz;           // slope difference to the central ray, in double
+    double drx_, drz_, da, dia;  // slopes in double, a = rx^2 + rz^2 and 1/a
 };
 
 __device__ __forceinline__ RayL ray_local(const ElemL& L, float xDs, float yDs, float zDs)
@@ -271,23 +277,35 @@ __device__ __forceinline__ RayL ray_local(const ElemL& L, float xDs, float yDs, 
     r.drz = (r.oz * L.fdy - L.fdz * r.oy) * den;
     r.rx = L.frxc + r.drx;
     r.rz = L.frzc + r.drz;
+    const Elem64& E = L.e64;
+    const double dx = (E.xd - E.xI) + (double)r.ox, dy = (E.yd - E.yI) + (double)r.oy;
+    const double dz = (E.zd - E.zI) + (double)r.oz;
+    r.dsec = sqrt(dx * dx + dy * dy + dz * dz) / dy;
+    r.ddrx = ((double)r.ox * (E.yd - E.yI) - (E.xd - E.xI) * (double)r.oy) / (dy * (E.yd - E.yI));
+    r.ddrz = ((double)r.oz * (E.yd - E.yI) - (E.zd - E.zI) * (double)r.oy) / (dy * (E.yd - E.yI));
+    r.drx_ = L.rxc + r.ddrx;
+    r.drz_ = L.rzc + r.ddrz;
+    r.da = r.drx_ * r.drx_ + r.drz_ * r.drz_;
+    r.dia = 1.0 / r.da;
     return r;
 }
 
+// The attenuation sum is kept in double: its float rounding (an ulp of ~50 for the rays that
+// cross the most tungsten) would alone move exp(-att) by ~1e-5.
 struct WalkL {
-    float att;      // accumulated mu * L
+    double att;     // accumulated mu * L
     float ext;      // hole y-extents of the current layer
     float hatt;     // mu-weighted hole y-extents of the current layer
     int lay;
 };
 
-__device__ __forceinline__ void close_layers_local(const DevGeom& g, WalkL& s, int upto, float sec)
+__device__ __forceinline__ void close_layers_local(const DevGeom& g, WalkL& s, int upto, double sec)
 {
     while (s.lay < upto) {                                           // :1276-1284
         const LayerInfo& Ly = g.layer[s.lay];
-        s.att = s.att + s.hatt * sec;
-        const float sept = (Ly.thickness - s.ext) * sec;
-        if (sept >= 0.00001f) s.att = s.att + Ly.mu_total * sept;
+        s.att = s.att + (double)s.hatt * sec;
+        const double sept = (double)(Ly.thickness - s.ext) * sec;
+        if (sept >= (double)0.00001f) s.att = s.att + (double)Ly.mu_total * sept;
         s.ext = 0.0f;
         s.hatt = 0.0f;
         ++s.lay;
@@ -299,17 +317,20 @@ __device__ __forceinline__ void walk_round_local(const DevGeom& g, const WarpSme
 {
     for (int j = 0; j < nh; ++j) {
         const int m = ws.rl[j];
-        if (m != s.lay) close_layers_local(g, s, m, r.sec);
+        if (m != s.lay) close_layers_local(g, s, m, r.dsec);
         if (!in_rect(ws.rr[j], sa_a, sa_b)) continue;
         const float4 A = ws.ra[j];
         const float4 B = ws.rb[j];
-        const float u0 = A.x + r.drx * B.x, w0 = A.y + r.drz * B.x;
-        const float ext = hole_extent(u0, w0, r.rx, r.rz, A.z, B.y, B.x, r.sec, r.sq, r.ky);
+        const float4 Cc = ws.rc[j];
+        const double hx = __hiloint2double(__float_as_int(B.z), __float_as_int(B.w));
+        const double hz = __hiloint2double(__float_as_int(Cc.x), __float_as_int(Cc.y));
+        const double u0 = hx + r.ddrx * (double)B.x, w0 = hz + r.ddrz * (double)B.x;
+        const float ext = hole_extent(u0, w0, r.drx_, r.drz_, r.da, r.dia, A.z, B.y, B.x, r.sec, r.sq, r.ky);
         s.ext = s.ext + ext;
         s.hatt = s.hatt + A.w * ext;
     }
     if (nr <= nh) return;
-    if (s.lay < g.n_layers) close_layers_local(g, s, g.n_layers, r.sec);
+    if (s.lay < g.n_layers) close_layers_local(g, s, g.n_layers, r.dsec);
     for (int j = nh; j < nr; ++j) {                                  // :1290-1325
         if (!in_rect(ws.rr[j], sa_a, sa_b)) continue;
         const float4 A = ws.ra[j];
@@ -319,7 +340,7 @@ __device__ __forceinline__ void walk_round_local(const DevGeom& g, const WarpSme
         const float q[3] = {r.qx * B.x - r.qz * B.y, r.qy, r.qx * B.y + r.qz * B.x};
         const float lo[3] = {-0.5f * B.z, -0.5f * B.w, -0.5f * hh};
         const float hi[3] = {0.5f * B.z, 0.5f * B.w, 0.5f * hh};
-        s.att = s.att + box_chord_near(P, q, lo, hi) * A.w;
+        s.att = s.att + (double)(box_chord_near(P, q, lo, hi) * A.w);
     }
 }
 
@@ -327,7 +348,7 @@ __device__ __forceinline__ void walk_round_local(const DevGeom& g, const WarpSme
 // x L.nz division, from its centre (xDs, yDs, zDs) in crystal d's frame (:1223-1231,
 // :1329-1357).
 __device__ __forceinline__ float finish_local(const ElemL& L, const RayL& r, int ix, int iy, int iz, float xDs,
-                                              float yDs, float zDs, float att)
+                                              float yDs, float zDs, double att)
 {
     const float w = L.w, t = L.t, h = L.h;
     const float gx = L.rfx, gy = L.rfy, gz = L.rfz;
@@ -381,8 +402,10 @@ __device__ __forceinline__ float finish_local(const ElemL& L, const RayL& r, int
     float labs = 0.0f;
     if (ok_abs && npar_abs < 3) labs = (npar_abs == 2) ? fabsf(uhi[m_abs] - ulo[m_abs]) : fa + ba;
     if (labs < kEps) labs = 0.0f;
-    att = att + (l1 - l2) * L.mu_t;
-    const float eff = expf(-att);
+    att = att + (double)((l1 - l2) * L.mu_t);
+    // exp(-att) = exp(-hi) exp(-lo), hi = att rounded to float: keeps expf's relative accuracy
+    const float a_hi = (float)att, a_lo = (float)(att - (double)a_hi);
+    const float eff = expf(-a_hi) * (1.0f - a_lo);
     const float absf = -expm1f(-labs * L.mu_t) * L.mu_pe / L.mu_t;
     // solid angle in double, as the reference's 4*M_PI promotion makes it
     const double dsq = (double)(r.qy * r.qy + r.qx * r.qx + r.qz * r.qz);
@@ -444,13 +467,13 @@ __device__ double pe_element_local(const DevGeom& g, const BlockSmem& bs, WarpSm
         const float yDs = -L.t / 2.0f + ((float)iy + 0.5f) * gy * L.t;
         const RayL r = ray_local(L, xDs, yDs, zDs);
         const float sa_a = e.filt ? r.rx : 0.0f, sa_b = e.filt ? r.rz : 0.0f;
-        WalkL s{0.0f, 0.0f, 0.0f, 0};
+        WalkL s{0.0, 0.0f, 0.0f, 0};
         bool blocked = false;
         for (int m = 0; m < g.n_layers; ++m) {                             // plate penalty :1240-1254
             if (in_rect(ws.inner[m], sa_a, sa_b)) continue;
             const float* pb = L.plate[m];
             const float tl = box_chord(0.0f, 0.0f, 0.0f, r.qx, r.qy, r.qz, pb[0], pb[1], pb[2], pb[3], pb[4], pb[5]);
-            if (tl < 0.1f) { s.att = s.att + 100000.0f; blocked = true; }
+            if (tl < 0.1f) { s.att = s.att + 100000.0; blocked = true; }
         }
         const bool skip = dead || (blocked && g.nonneg_mu);
         float4 box = make_float4(skip ? INFINITY : sa_a, skip ? -INFINITY : sa_a, skip ? INFINITY : sa_b,
@@ -484,7 +507,7 @@ __device__ double pe_element_local(const DevGeom& g, const BlockSmem& bs, WarpSm
         }
         float term = 0.0f;
         if (!skip) {
-            if (s.lay < g.n_layers) close_layers_local(g, s, g.n_layers, r.sec);
+            if (s.lay < g.n_layers) close_layers_local(g, s, g.n_layers, r.dsec);
             term = finish_local(L, r, ix, iy, iz, xDs, yDs, zDs, s.att);
             neumaier_add(sum, comp, term);
         }

@@ -117,31 +117,74 @@ __device__ __forceinline__ bool hole_far(double ax, double az, double bx, double
     return dx * dx + dz * dz > (r + 1e-6) * (r + 1e-6);
 }
 
-// Attenuation sums (mu_total, mu_pe, mu_C times length) of layer m along the segment A -> B,
-// A before B in depth (the direction the reference's chords assume): the plate chord minus the
-// hole chords, with the layer's coefficients, plus the hole chords with the holes' own
-// coefficients.  inside: 0 none, 1 A lies inside the plate, 2 B lies inside.
+// Length of segment A -> B inside the box [lo, hi]: the exact overlap of the segment's
+// parameter range with the three slabs.  The grid model's paths start or end inside the plate
+// or a crystal, where the reference's chords (full crossings between the two ends) do not apply.
+__device__ double seg_box64(const double A[3], const double B[3], const double lo[3], const double hi[3])
+{
+    double t0 = 0.0, t1 = 1.0;
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        const double d = B[a] - A[a];
+        if (d == 0.0) {
+            if (A[a] < lo[a] || A[a] > hi[a]) return 0.0;
+            continue;
+        }
+        double u = (lo[a] - A[a]) / d, v = (hi[a] - A[a]) / d;
+        if (u > v) { const double w = u; u = v; v = w; }
+        t0 = fmax(t0, u);
+        t1 = fmin(t1, v);
+    }
+    if (t1 <= t0) return 0.0;
+    return (t1 - t0) * sqrt((B[0] - A[0]) * (B[0] - A[0]) + (B[1] - A[1]) * (B[1] - A[1]) + (B[2] - A[2]) * (B[2] - A[2]));
+}
+
+// Length of segment A -> B inside the y-parallel cylinder (x - xc)^2 + (z - zc)^2 <= r^2,
+// y in [y1, y2] (exact overlap).
+__device__ double seg_cyl64(const double A[3], const double B[3], double xc, double zc, double y1, double y2, double r)
+{
+    double t0 = 0.0, t1 = 1.0;
+    const double dy = B[1] - A[1];
+    if (dy == 0.0) {
+        if (A[1] < y1 || A[1] > y2) return 0.0;
+    } else {
+        double u = (y1 - A[1]) / dy, v = (y2 - A[1]) / dy;
+        if (u > v) { const double w = u; u = v; v = w; }
+        t0 = fmax(t0, u);
+        t1 = fmin(t1, v);
+    }
+    const double dx = B[0] - A[0], dz = B[2] - A[2], ox = A[0] - xc, oz = A[2] - zc;
+    const double a = dx * dx + dz * dz, b = ox * dx + oz * dz, c = ox * ox + oz * oz - r * r;
+    if (a == 0.0) {
+        if (c > 0.0) return 0.0;
+    } else {
+        const double disc = b * b - a * c;
+        if (disc <= 0.0) return 0.0;
+        const double sq = sqrt(disc);
+        t0 = fmax(t0, (-b - sq) / a);
+        t1 = fmin(t1, (-b + sq) / a);
+    }
+    if (t1 <= t0) return 0.0;
+    return (t1 - t0) * sqrt(a + dy * dy);
+}
+
+// Attenuation sums (mu_total, mu_pe, mu_C times length) of layer m along segment A -> B: its
+// length in the plate box minus its lengths in the layer's holes, with the layer's
+// coefficients, plus its lengths in the holes with the holes' own coefficients.
 __device__ void layer_path64(const DevGeom& g, const GridGeom& G, int m, const double A[3], const double B[3],
-                             int inside, double& wt, double& wpe, double& wc)
+                             double& wt, double& wpe, double& wc)
 {
     const double* Ly = g.t64.layer + kLayer64 * m;
-    double box;
-    if (inside == 2)
-        box = box_chord_inside64(A[0], A[1], A[2], B[0], B[1], B[2], Ly[0], Ly[2], Ly[4], Ly[1], Ly[3], Ly[5]);
-    else if (inside == 1)
-        box = box_chord_inside64(B[0], B[1], B[2], A[0], A[1], A[2], Ly[0], Ly[2], Ly[4], Ly[1], Ly[3], Ly[5]);
-    else
-        box = box_chord64(A[0], A[1], A[2], B[0], B[1], B[2], Ly[0], Ly[2], Ly[4], Ly[1], Ly[3], Ly[5]);
+    const double lo[3] = {Ly[0], Ly[2], Ly[4]}, hi[3] = {Ly[1], Ly[3], Ly[5]};
+    const double box = seg_box64(A, B, lo, hi);
     if (box == 0.0) return;
     const GridLayer& L = G.layer[m];
-    RayCyl64 rc;
-    ray_cyl64_init(rc, A[0], A[1], A[2], B[0], B[1], B[2]);
     double hsum = 0.0;
     for (int j = L.hole_begin; j < L.hole_begin + L.hole_count; ++j) {
         const D4 a = g.t64.hole_a[j];
         const double r = g.t64.hole_b[j].x;
         if (hole_far(A[0], A[2], B[0], B[2], a.x, a.w, r)) continue;
-        const double l = ray_cyl64_chord(rc, A[0], A[1], A[2], a.x, a.y, a.z, a.w, r);
+        const double l = seg_cyl64(A, B, a.x, a.w, a.y, a.z, r);
         if (l == 0.0) continue;
         const float* hp = G.raw_col + 100 + 9 * j;
         hsum += l;
@@ -170,7 +213,7 @@ __global__ void septal_weight_kernel(DevGeom g, GridGeom G, long long vox_begin,
     septal_point(G, j, m, p);
     voxel_centre64(g, vox_begin + vi, rotation, I3[0], I3[1], I3[2]);
     double at = 0.0, ape = 0.0, ac = 0.0;
-    for (int mm = 0; mm < G.n_layers; ++mm) layer_path64(g, G, mm, I3, p, mm == m ? 2 : 0, at, ape, ac);
+    for (int mm = 0; mm < G.n_layers; ++mm) layer_path64(g, G, mm, I3, p, at, ape, ac);
     const GridLayer& L = G.layer[m];
     const double r2 = (p[0] - I3[0]) * (p[0] - I3[0]) + (p[1] - I3[1]) * (p[1] - I3[1]) + (p[2] - I3[2]) * (p[2] - I3[2]);
     const double vcell = L.cx * L.cy * L.cz;
@@ -273,9 +316,20 @@ __device__ bool point_terms(const DevGeom& g, const GridGeom& G, const GridSum& 
             lc += (double)mu.z * la;
         }
     }
+    if (k >= 0) {                                             // the rest of crystal k, from p to its exit
+        const D4 Pk = g.t64.cry_pos[k], Zk = g.t64.cry_size[k], Tk = g.t64.cry_trig[k];
+        const double ax = p[0] - Pk.x, az = p[2] - Pk.z, bx = D3[0] - Pk.x, bz = D3[2] - Pk.z;
+        const double pa[3] = {ax * Tk.z - az * Tk.w, p[1] - Pk.y, ax * Tk.w + az * Tk.z};
+        const double pb[3] = {bx * Tk.z - bz * Tk.w, D3[1] - Pk.y, bx * Tk.w + bz * Tk.z};
+        const double lo[3] = {-0.5 * Zk.x, -0.5 * Zk.y, -0.5 * Zk.z}, hi[3] = {0.5 * Zk.x, 0.5 * Zk.y, 0.5 * Zk.z};
+        const double lk = seg_box64(pa, pb, lo, hi);
+        const float4 mu = __ldg(&g.cry.mu[k]);
+        lpe += (double)mu.y * lk;
+        lc += (double)mu.z * lk;
+    }
     if (m >= 0) {                                             // tungsten and hole media on the way
         double wt = 0.0;
-        for (int mm = 0; mm < G.n_layers; ++mm) layer_path64(g, G, mm, p, D3, mm == m ? 1 : 0, wt, lpe, lc);
+        for (int mm = 0; mm < G.n_layers; ++mm) layer_path64(g, G, mm, p, D3, wt, lpe, lc);
     }
     out[0] = (float)ps[0];
     out[1] = (float)ps[1];

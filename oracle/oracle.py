@@ -55,6 +55,8 @@ def lib():
         L.oracle_pe_local.argtypes = [_fp, _fp, _fp, _ip, ctypes.c_int, ctypes.c_longlong, ctypes.c_longlong, _dp,
                                       ctypes.c_int]
         L.oracle_pe_local.restype = ctypes.c_int
+        L.oracle_pe_subelements.argtypes = [_fp, _fp, _fp, ctypes.c_int, ctypes.c_int, ctypes.c_longlong, _dp]
+        L.oracle_pe_subelements.restype = ctypes.c_int
         L.oracle_scatter_grid.argtypes = [_fp, _fp, _fp, _fp, ctypes.c_int, ctypes.c_double, _ip, ctypes.c_int,
                                           ctypes.c_longlong, ctypes.c_longlong, _dp, ctypes.c_int]
         L.oracle_scatter_grid.restype = ctypes.c_int
@@ -185,6 +187,20 @@ def scatter(geo, pe_matrix, part, bitmap, prec=64, dets=None, v0=0, nv=None, thr
                               dd.size, v0, nv, out.ctypes.data_as(_dp), threads)
     if rc:
         raise RuntimeError(f"oracle_scatter failed ({rc})")
+    return out
+
+
+def pe_subelements(geo, d, v, which=64):
+    """The 1024 sub-element contributions of element (d, v) (index (iz * 8 + ix) * 16 + iy):
+    which = 64 FP64 restatement, 32 FP32 twin, 'local' the local-coordinate FP32 form."""
+    c, pc = _f32(geo.collimator)
+    dd, pd = _f32(geo.detector)
+    i, pi = _f32(geo.image)
+    out = np.zeros(1024, dtype=np.float64)
+    w = 0 if which == "local" else int(which)
+    rc = lib().oracle_pe_subelements(pc, pd, pi, w, int(d), int(v), out.ctypes.data_as(_dp))
+    if rc:
+        raise RuntimeError(f"oracle_pe_subelements failed ({rc})")
     return out
 
 

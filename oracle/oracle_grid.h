@@ -21,8 +21,11 @@
  *   T(p, d, v) = the reference's item (scatter.cu:1232-1427) with scatter point p: cone angle,
  *     Compton energy, 2-sigma window reject and window probability, azimuth range, polar range
  *     over crystal d's corners, absorption in d, attenuation at the scattered energy by every
- *     crystal other than d (and k) that the segment p -> d's centre crosses (all crystals, no
- *     relationship bitmap) and, for septal points, by the tungsten and hole media on the way;
+ *     crystal other than d that the segment p -> d's centre crosses (all crystals, no
+ *     relationship bitmap; for a crystal cell, its own crystal from p to the exit) and, for
+ *     septal points, by the tungsten and hole media on the way (exact segment lengths: the
+ *     paths start or end inside the plate, where the reference's full-crossing chords do not
+ *     apply);
  *     the Klein-Nishina fraction is the exact integral of the reference's Klein-Nishina shape
  *     over [theta_min, theta_max] divided by its integral over [0, pi] (closed form), in place
  *     of the reference's 0.01 rad Riemann sum.
@@ -44,6 +47,59 @@ static double kn_frac(double tmin, double tmax, double a)
     return (kn_prim(cos(tmin), a) - kn_prim(cos(tmax), a)) / (kn_prim(1.0, a) - kn_prim(-1.0, a));
 }
 
+/* Length of segment A -> B inside the box [lo, hi] (exact overlap of the segment's parameter
+ * range with the three slabs).  The grid model's paths start or end inside the plate, where
+ * the reference's box and cylinder chords (full crossings between the two ends) do not
+ * apply. */
+static double seg_box(const double A[3], const double B[3], const double lo[3], const double hi[3])
+{
+    double t0 = 0, t1 = 1;
+    for (int a = 0; a < 3; ++a) {
+        const double d = B[a] - A[a];
+        if (d == 0) {
+            if (A[a] < lo[a] || A[a] > hi[a]) return 0;
+            continue;
+        }
+        double u = (lo[a] - A[a]) / d, v = (hi[a] - A[a]) / d;
+        if (u > v) { const double w = u; u = v; v = w; }
+        if (u > t0) t0 = u;
+        if (v < t1) t1 = v;
+    }
+    if (t1 <= t0) return 0;
+    const double len = sqrt((B[0] - A[0]) * (B[0] - A[0]) + (B[1] - A[1]) * (B[1] - A[1]) + (B[2] - A[2]) * (B[2] - A[2]));
+    return (t1 - t0) * len;
+}
+
+/* Length of segment A -> B inside the y-parallel cylinder (x - xc)^2 + (z - zc)^2 <= r^2,
+ * y in [y1, y2] (exact overlap). */
+static double seg_cyl(const double A[3], const double B[3], double xc, double zc, double y1, double y2, double r)
+{
+    double t0 = 0, t1 = 1;
+    const double dy = B[1] - A[1];
+    if (dy == 0) {
+        if (A[1] < y1 || A[1] > y2) return 0;
+    } else {
+        double u = (y1 - A[1]) / dy, v = (y2 - A[1]) / dy;
+        if (u > v) { const double w = u; u = v; v = w; }
+        if (u > t0) t0 = u;
+        if (v < t1) t1 = v;
+    }
+    const double dx = B[0] - A[0], dz = B[2] - A[2], ox = A[0] - xc, oz = A[2] - zc;
+    const double a = dx * dx + dz * dz, b = ox * dx + oz * dz, c = ox * ox + oz * oz - r * r;
+    if (a == 0) {
+        if (c > 0) return 0;
+    } else {
+        const double disc = b * b - a * c;
+        if (disc <= 0) return 0;
+        const double sq = sqrt(disc);
+        const double u = (-b - sq) / a, v = (-b + sq) / a;
+        if (u > t0) t0 = u;
+        if (v < t1) t1 = v;
+    }
+    if (t1 <= t0) return 0;
+    return (t1 - t0) * sqrt(a + dy * dy);
+}
+
 static void grid_plate_box(const ogeo* g, int m, double b[6])
 {
     const float* Lh = g->C + (m + 1) * 10;
@@ -53,35 +109,32 @@ static void grid_plate_box(const ogeo* g, int m, double b[6])
     b[2] = -(double)Lh[3] / 2.0; b[5] = (double)Lh[3] / 2.0;
 }
 
-/* Attenuation sums (mu_total, mu_pe, mu_C times length) of layer m along the segment A -> B
- * (A before B in depth, y_A < y_B, the direction the reference's chords assume): the plate
- * chord minus the hole chords, times the layer's coefficients, plus the hole chords times the
- * holes' coefficients.  inside: 0 none, 1 A lies inside the plate (the chord runs from A to the
- * plate's exit), 2 B lies inside (from the plate's entry to B). */
-static void grid_layer_path(const ogeo* g, int m, int hole_begin, const double A[3], const double B[3], int inside,
+/* Attenuation sums (mu_total, mu_pe, mu_C times length) of layer m along the segment A -> B:
+ * the segment's length in the plate box minus its lengths in the layer's holes, times the
+ * layer's coefficients, plus its lengths in the holes times the holes' coefficients (exact
+ * overlaps: A or B may lie inside the plate). */
+static void grid_layer_path(const ogeo* g, int m, int hole_begin, const double A[3], const double B[3],
                             double* wt, double* wpe, double* wc)
 {
     const float* C = g->C;
     const double fov = (double)g->I[11];
     double b[6];
     grid_plate_box(g, m, b);
-    double box;
-    if (inside == 2) box = box_chord_inside_f64(A[0], A[1], A[2], B[0], B[1], B[2], b[0], b[1], b[2], b[3], b[4], b[5]);
-    else if (inside == 1) box = box_chord_inside_f64(B[0], B[1], B[2], A[0], A[1], A[2], b[0], b[1], b[2], b[3], b[4], b[5]);
-    else box = box_chord_f64(A[0], A[1], A[2], B[0], B[1], B[2], b[0], b[1], b[2], b[3], b[4], b[5]);
+    const double lo[3] = {b[0], b[1], b[2]}, hi[3] = {b[3], b[4], b[5]};
+    const double box = seg_box(A, B, lo, hi);
     if (box == 0) return;
     double hsum = 0;
     const double ex = B[0] - A[0], ez = B[2] - A[2], l2 = ex * ex + ez * ez;
     for (int j = hole_begin; j < hole_begin + g->nh[m]; ++j) {
         const float* h = C + 100 + 9 * j;
         /* a hole whose axis stays farther than its radius from the segment's xz projection has
-         * a zero chord: skipped without evaluating it */
+         * a zero length: skipped without evaluating it */
         double t = l2 > 0 ? (((double)h[0] - A[0]) * ex + ((double)h[3] - A[2]) * ez) / l2 : 0;
         t = t < 0 ? 0 : (t > 1 ? 1 : t);
         const double dx = A[0] + t * ex - (double)h[0], dz = A[2] + t * ez - (double)h[3];
         if (dx * dx + dz * dz > ((double)h[4] + 1e-6) * ((double)h[4] + 1e-6)) continue;
-        const double l = cyl_chord_f64(A[0], A[1], A[2], B[0], B[1], B[2], (double)h[0], (double)h[1] + fov,
-                                       (double)h[2] + fov, (double)h[3], (double)h[4]);
+        const double l = seg_cyl(A, B, (double)h[0], (double)h[3], (double)h[1] + fov, (double)h[2] + fov,
+                                 (double)h[4]);
         if (l == 0) continue;
         hsum += l;
         *wt += (double)h[5] * l;
@@ -98,7 +151,8 @@ static void grid_layer_path(const ogeo* g, int m, int hole_begin, const double A
 }
 
 /* T(p, d, v) times the weight w (see the file comment).  skip_k: the scatterer crystal (crystal
- * cells) or -1; layer_p: the layer holding a septal point, or -1. */
+ * cells; the scattered photon's path through the rest of it is attenuated too) or -1; layer_p:
+ * the layer holding a septal point, or -1. */
 static double grid_item(const ogeo* g, int d, const crystal_f64* cd, const double I3[3], const double Is[3],
                         const double p[3], double w, int skip_k, int layer_p, double e0, double lo_w, double hi_w)
 {
@@ -153,11 +207,20 @@ static double grid_item(const ogeo* g, int d, const crystal_f64* cd, const doubl
                                         0.5 * ca.t, 0.5 * ca.h);
         if (la != 0) att += la * (ca.mu_pe * sc_pe + ca.mu_c * sc_c);
     }
+    if (skip_k >= 0) {                    /* the rest of the scattering crystal, from p to its exit */
+        crystal_f64 ck;
+        load_crystal_f64(g, skip_k, &ck);
+        double pa[3], pb[3];
+        to_frame_f64(&ck, p[0], p[1], p[2], &pa[0], &pa[1], &pa[2]);
+        to_frame_f64(&ck, D3[0], D3[1], D3[2], &pb[0], &pb[1], &pb[2]);
+        const double lo[3] = {-0.5 * ck.w, -0.5 * ck.t, -0.5 * ck.h}, hi[3] = {0.5 * ck.w, 0.5 * ck.t, 0.5 * ck.h};
+        att += seg_box(pa, pb, lo, hi) * (ck.mu_pe * sc_pe + ck.mu_c * sc_c);
+    }
     if (layer_p >= 0) {                                             /* tungsten and holes on the way */
         int hb = 0;
         for (int m = 0; m < g->L; ++m) {
             double wt = 0, wpe = 0, wc = 0;
-            grid_layer_path(g, m, hb, p, D3, m == layer_p ? 1 : 0, &wt, &wpe, &wc);
+            grid_layer_path(g, m, hb, p, D3, &wt, &wpe, &wc);
             att += wpe * sc_pe + wc * sc_c;
             hb += g->nh[m];
         }
@@ -177,7 +240,7 @@ static double grid_septal_weight(const ogeo* g, int m, int hole_begin, const dou
     double at = 0, ape = 0, ac = 0;
     int hb = 0;
     for (int mm = 0; mm < g->L; ++mm) {
-        grid_layer_path(g, mm, hb, I3, p, mm == m ? 2 : 0, &at, &ape, &ac);
+        grid_layer_path(g, mm, hb, I3, p, &at, &ape, &ac);
         hb += g->nh[mm];
     }
     const double r2 = (p[0] - I3[0]) * (p[0] - I3[0]) + (p[1] - I3[1]) * (p[1] - I3[1]) + (p[2] - I3[2]) * (p[2] - I3[2]);

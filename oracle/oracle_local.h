@@ -23,7 +23,7 @@
  */
 
 typedef struct {
-    float hx, hz;     /* ray through crystal d's centre minus hole centre, at the hole's y1 */
+    double hx, hz;    /* ray through crystal d's centre minus hole centre, at the hole's y1 */
     float dy;         /* y1 - yI */
     float th;         /* y2 - y1 */
     float r, mu;
@@ -98,50 +98,48 @@ static float box_chord_near_f(const float P[3], const float q[3], const float lo
     return smax - smin;
 }
 
-/* Hole chord as a y-extent: the ray's xz offset from the hole axis at the hole's entry
- * plane is (u0, w0), its slopes are (rx, rz) per unit y, the hole spans y in [0, th]
- * relative to that plane.  Follows the reference's cap/side cases and thresholds
+/* Hole chord as a y-extent: the ray's offset from the hole axis at the hole's entry plane is
+ * (u0, w0), its slopes are (rx, rz) per unit y (a = rx^2 + rz^2, ia = 1/a), the hole spans
+ * y in [0, th] relative to that plane.  Follows the reference's cap/side cases and thresholds
  * (PESysMatGen.cu:688-799); t-parameters (length from the voxel) enter only the threshold
- * tests: ta = dy * sec, tb = (dy + th) * sec, tio = ray length. */
-static float hole_extent_f(float u0, float w0, float rx, float rz, float r, float th, float dy, float sec,
-                           float tio, float ky)
+ * tests: ta = dy * sec, tb = (dy + th) * sec, tio = ray length.  Offsets, slopes and roots are
+ * in double: near a tangent, and for a hole met far from where the ray enters the plate, the
+ * chord is ill-conditioned in them. */
+static float hole_extent_f(double u0d, double w0d, double rxd, double rzd, double ad, double iad, float r, float th,
+                           float dy, float sec, float tio, float ky)
 {
     if (fabsf(th) < 0.001f) return 0;
-    const float u1 = u0 + rx * th, w1 = w0 + rz * th;
-    const int fl = u0 * u0 + w0 * w0 <= r * r;
-    const int fr = u1 * u1 + w1 * w1 <= r * r;
-    const float ta = dy * sec, tb = (dy + th) * sec;
+    const double u1d = u0d + rxd * (double)th, w1d = w0d + rzd * (double)th;
+    const double r2 = (double)r * (double)r;
+    const int fl = u0d * u0d + w0d * w0d <= r2;
+    const int fr = u1d * u1d + w1d * w1d <= r2;
     if (fl && fr) {
+        const float ta = dy * sec, tb = (dy + th) * sec;
         if ((double)ta <= 0.0001 || (double)tb <= 0.0001) return 0;
         if (ta >= tio || tb >= tio) return 0;
         return th;
     }
-    const float a = rx * rx + rz * rz;
-    const float cross = u0 * rz - w0 * rx;
-    const float q = a * r * r - cross * cross;          /* b^2 - a c (Lagrange identity) */
-    if ((double)(ky * ky * q) <= 0.00001) return 0;      /* the reference's discriminant */
-    const float b = u0 * rx + w0 * rz;
-    const float sq = sqrtf(q);
-    /* roots of a s^2 + 2 b s + c = 0, c = u0^2 + w0^2 - r^2, without cancellation */
-    const float c = (u0 - r) * (u0 + r) + w0 * w0;
-    float s1, s2;
-    if (b > 0) { s1 = (-b - sq) / a; s2 = c / (-b - sq); }
-    else       { s2 = (-b + sq) / a; s1 = c / (-b + sq); }
-    float ea, eb;
+    const double cross = u0d * rzd - w0d * rxd;
+    const double qd = ad * r2 - cross * cross;          /* b^2 - a c (Lagrange identity) */
+    if ((double)(ky * ky) * qd <= (double)0.00001f) return 0;   /* the reference's discriminant */
+    const double bd = u0d * rxd + w0d * rzd;
+    const double sq = (double)sqrtf((float)qd);
+    const double s1 = (-bd - sq) * iad, s2 = (-bd + sq) * iad;
+    double ea, eb;
     if (!fl && !fr) {
-        if (!(s1 >= 0 && s2 <= th)) return 0;
+        if (!(s1 >= 0 && s2 <= (double)th)) return 0;
         ea = s1; eb = s2;
     } else if (fl) { ea = 0; eb = s2; }
-    else           { ea = s1; eb = th; }
-    const float t1 = (dy + ea) * sec, t2 = (dy + eb) * sec;
+    else           { ea = s1; eb = (double)th; }
+    const float t1 = (dy + (float)ea) * sec, t2 = (dy + (float)eb) * sec;
     if ((double)t2 <= 0.0001 || (double)t1 <= 0.0001) return 0;
     if (t2 >= tio || t1 >= tio) return 0;
-    if (!fl && !fr) return 2.0f * sq / a;
-    return eb - ea;
+    if (!fl && !fr) return (float)(2.0 * sq * iad);
+    return (float)(eb - ea);
 }
 
 static float pe_element_local(const ogeo* g, int d, double xI, double yI, double zI, int* cand_c, int* cand_h,
-                              int* ncand_h, lhole* lh, lcry* lc)
+                              int* ncand_h, lhole* lh, lcry* lc, float* per_sub)
 {
     const float* C = g->C;
     const double fov = (double)g->I[11];
@@ -194,8 +192,8 @@ static float pe_element_local(const ogeo* g, int d, double xI, double yI, double
             if (sqrt((vz - uz) * (vz - uz) + (vy - uy) * (vy - uy) + (vx - ux) * (vx - ux)) <= crit + crit_self) {
                 lhole* e = &lh[hoff + n];
                 const double dy = hy1 - yI;
-                e->hx = (float)((xI - hx) + rxc * dy);
-                e->hz = (float)((zI - hz) + rzc * dy);
+                e->hx = (xI - hx) + rxc * dy;
+                e->hz = (zI - hz) + rzc * dy;
                 e->dy = (float)dy;
                 e->th = (float)(hy2 - hy1);
                 e->r = (float)hr;
@@ -225,7 +223,6 @@ static float pe_element_local(const ogeo* g, int d, double xI, double yI, double
     const float cr = (float)cos(cd.rot), sr = (float)sin(cd.rot);       /* d's frame -> world */
     const float cmr = (float)cos(-cd.rot), smr = (float)sin(-cd.rot);   /* world -> d's frame */
     const float fdx = (float)dcx, fdy = (float)dcy, fdz = (float)dcz;
-    const float frxc = (float)rxc, frzc = (float)rzc;
     const float mu_t = (float)cd.mu_t, mu_pe = (float)cd.mu_pe;
     float sum = 0, comp = 0;
     for (unsigned iz = 0; iz < NZS; ++iz)
@@ -239,8 +236,12 @@ static float pe_element_local(const ogeo* g, int d, double xI, double yI, double
         const float dsq = qy * qy + qx * qx + qz * qz;
         const float sq = sqrtf(dsq);
         const float ky = qy / sq, sec = sq / qy;
-        const float drx = (ox * fdy - fdx * oy) / (qy * fdy), drz = (oz * fdy - fdz * oy) / (qy * fdy);
-        const float rx = frxc + drx, rz = frzc + drz;
+        /* 1 / cos in double (septal lengths of heavily attenuated rays) */
+        const double ddx = dcx + (double)ox, ddy = dcy + (double)oy, ddz = dcz + (double)oz;
+        const double dsec = sqrt(ddx * ddx + ddy * ddy + ddz * ddz) / ddy;
+        const double ddrx = ((double)ox * dcy - dcx * (double)oy) / (ddy * dcy);
+        const double ddrz = ((double)oz * dcy - dcz * (double)oy) / (ddy * dcy);
+        const double rxd = rxc + ddrx, rzd = rzc + ddrz, ad = rxd * rxd + rzd * rzd, iad = 1.0 / ad;
 
         /* solid angle in double, as the reference (:1223-1231) */
         const double fourpi_d2 = 4 * M_PI * (double)dsq;
@@ -252,26 +253,26 @@ static float pe_element_local(const ogeo* g, int d, double xI, double yI, double
                                   (double)sq);
         const float sa = rmax_f32(rmax_f32(sax, say), saz);
 
-        float att = 0;
+        double att = 0;   /* in double: its float rounding alone would move exp(-att) by ~1e-5 */
         for (int m = 0; m < g->L; ++m) {                       /* plate bypass penalty :1240-1254 */
             const float tl = box_chord_f32(0, 0, 0, qx, qy, qz, pl[m].x1, pl[m].y1, pl[m].z1, pl[m].x2, pl[m].y2,
                                            pl[m].z2);
-            if (tl < 0.1f) att = att + 100000.0f;
+            if (tl < 0.1f) att = att + 100000.0;
         }
         hoff = 0;
         for (int m = 0; m < g->L; ++m) {                       /* holes and septa :1257-1286 */
             float ext = 0, hatt = 0;
             for (int j = 0; j < ncand_h[m]; ++j) {
                 const lhole* e = &lh[hoff + j];
-                const float u0 = e->hx + drx * e->dy, w0 = e->hz + drz * e->dy;
-                const float s = hole_extent_f(u0, w0, rx, rz, e->r, e->th, e->dy, sec, sq, ky);
+                const double u0 = e->hx + ddrx * (double)e->dy, w0 = e->hz + ddrz * (double)e->dy;
+                const float s = hole_extent_f(u0, w0, rxd, rzd, ad, iad, e->r, e->th, e->dy, sec, sq, ky);
                 ext = ext + s;
                 hatt = hatt + e->mu * s;
             }
             hoff += ncand_h[m];
-            att = att + hatt * sec;
-            const float sept = (pl[m].T - ext) * sec;
-            if (sept >= 0.00001f) att = att + pl[m].mu * sept;
+            att = att + (double)hatt * dsec;
+            const double sept = (double)(pl[m].T - ext) * dsec;
+            if (sept >= (double)0.00001f) att = att + (double)pl[m].mu * sept;
         }
         for (int j = 0; j < nc; ++j) {                         /* other crystals :1290-1325 */
             const lcry* k = &lc[j];
@@ -279,7 +280,7 @@ static float pe_element_local(const ogeo* g, int d, double xI, double yI, double
             const float q[3] = {qx * k->c - qz * k->s, qy, qx * k->s + qz * k->c};
             const float lo[3] = {-0.5f * k->w, -0.5f * k->t, -0.5f * k->h};
             const float hi[3] = {0.5f * k->w, 0.5f * k->t, 0.5f * k->h};
-            att = att + box_chord_near_f(P, q, lo, hi) * k->mu;
+            att = att + (double)(box_chord_near_f(P, q, lo, hi) * k->mu);
         }
         /* self attenuation and absorption in crystal d's frame, from the sub-element centre */
         const float vq[3] = {qx * cmr - qz * smr, qy, qx * smr + qz * cmr};    /* ray vector in d's frame */
@@ -338,10 +339,12 @@ static float pe_element_local(const ogeo* g, int d, double xI, double yI, double
             else if (ok) labs = fwd + bwd;
             if (labs < 0.001f) labs = 0;
         }
-        att = att + (l1 - l2) * mu_t;
-        const float eff = expf(-att);
+        att = att + (double)((l1 - l2) * mu_t);
+        const float a_hi = (float)att, a_lo = (float)(att - (double)a_hi);
+        const float eff = expf(-a_hi) * (1.0f - a_lo);
         const float absf = -expm1f(-labs * mu_t) * mu_pe / mu_t;
         const float term = eff * sa * absf;
+        if (per_sub) per_sub[(iz * NXS + ix) * NYS + iy] = term;
         /* Neumaier compensated sum */
         const float tsum = sum + term;
         if (fabsf(sum) >= fabsf(term)) comp += (sum - tsum) + term;

@@ -207,7 +207,7 @@ int oracle_pe_local(const float* C, const float* D, const float* I, const int* d
             long long v = v0 + e % nv;
             double xI, yI, zI;
             voxel_centre_f64(&g, v, &xI, &yI, &zI);
-            out[e] = (double)pe_element_local(&g, d, xI, yI, zI, cc, ch, nch, lh, lc);
+            out[e] = (double)pe_element_local(&g, d, xI, yI, zI, cc, ch, nch, lh, lc, NULL);
         }
         free(cc);
         free(ch);
@@ -229,6 +229,40 @@ int oracle_scatter_grid(const float* C, const float* D, const float* I, const fl
     for (long long e = 0; e < (long long)ndet * nv; ++e)
         out[e] = grid_element(&g, parts, dets[e / nv], v0 + e % nv, cell, nthreads);
     return 0;
+}
+
+/* Per-sub-element contributions of element (d, v) (8 x 16 x 8, index (iz * 8 + ix) * 16 + iy):
+ * which = 32 the FP32 twin, 64 the FP64 restatement, 0 the local-coordinate FP32 form.  For
+ * locating where two evaluations of one element part. */
+int oracle_pe_subelements(const float* C, const float* D, const float* I, int which, int d, long long v, double* out)
+{
+    ogeo g;
+    if (parse(&g, C, D, I, NULL)) return -1;
+    int* cc = (int*)malloc(sizeof(int) * (size_t)(g.ncry + 1));
+    int* ch = (int*)malloc(sizeof(int) * (size_t)(g.nholes + 1));
+    lhole* lh = (lhole*)malloc(sizeof(lhole) * (size_t)(g.nholes + 1));
+    lcry* lc = (lcry*)malloc(sizeof(lcry) * (size_t)(g.ncry + 1));
+    int nch[MAX_LAYERS];
+    int rc = 0;
+    if (!cc || !ch || !lh || !lc) rc = -2;
+    else if (which == 64) {
+        double xI, yI, zI;
+        voxel_centre_f64(&g, v, &xI, &yI, &zI);
+        pe_element_at_f64(&g, d, xI, yI, zI, cc, ch, nch, NULL, out);
+    } else if (which == 32) {
+        float xI, yI, zI, tmp[1024];
+        voxel_centre_f32(&g, v, &xI, &yI, &zI);
+        pe_element_at_f32(&g, d, xI, yI, zI, cc, ch, nch, NULL, tmp);
+        for (int i = 0; i < 1024; ++i) out[i] = tmp[i];
+    } else {
+        double xI, yI, zI;
+        float tmp[1024];
+        voxel_centre_f64(&g, v, &xI, &yI, &zI);
+        pe_element_local(&g, d, xI, yI, zI, cc, ch, nch, lh, lc, tmp);
+        for (int i = 0; i < 1024; ++i) out[i] = tmp[i];
+    }
+    free(cc); free(ch); free(lh); free(lc);
+    return rc;
 }
 
 int oracle_pe(const float* C, const float* D, const float* I, int prec, const int* dets, int ndet,

@@ -38,7 +38,7 @@ def test_scatter_batch_equals_per_task_calls(gpu):
         (1, 2, sysmat.HOLE_MODEL_VARIANT, 1.0, 0, c1.n_det, 0, c1.n_vox),
         (1, 3, H, 3.0, c1.n_det - 1, 1, c1.n_vox - 1, 1),
         (2, 3, sysmat.HOLE_MODEL_NATIVE, 1.0, 2, 9, 0, c2.n_vox),
-        (0, 2, H, 0.0, 5, 3, 130, 200),
+        (0, 2, H, 0.0, 5, 3, 40, 70),
     ]
     expected, outs, items = [], [], []
     for (c, parts, model, rot, d0, nd, v0, nv) in tasks:

@@ -316,22 +316,39 @@ def test_local_form_within_1e5_of_fp64(name):
     assert r.max() < rel_err(oracle.pe(geo, prec=32), o64).max()
 
 
+def test_local_form_shifted_config1_within_1e5_of_fp64():
+    geo, _ = golden("config1")
+    img = geo.image.copy()
+    img[8] = np.float32(img[8] + 1.234e-4)
+    img[10] = np.float32(img[10] - 0.567e-4)
+    g = geometry.Geometry("config1_shifted", geo.collimator, geo.detector, img, geo.physics)
+    dets = np.arange(0, g.n_det, 4)
+    o64 = oracle.pe(g, prec=64, dets=dets)
+    r = rel_err(oracle.pe_local(g, dets=dets), o64)
+    assert r.max() <= 1e-5, r.max()
+
+
 def test_local_form_config2_sample_within_1e5_of_fp64():
     g = geometry.voxel_slab(geometry.config2(), 16)
-    dets, v0, nv = np.arange(8, 4096, 512), 96 * 48, 96
+    dets, v0, nv = np.concatenate([np.arange(8, 256, 32), np.arange(8, 4096, 512)]), 96 * 48, 96
     o64 = oracle.pe(g, prec=64, dets=dets, v0=v0, nv=nv)
     r = rel_err(oracle.pe_local(g, dets=dets, v0=v0, nv=nv), o64)
     assert r.max() <= 1e-5, r.max()
 
 
 def test_grid_model_converges_as_the_cells_shrink():
-    """The grid scatter model (oracle_grid.h) is a discretisation: halving the 0.25 mm cell
-    changes each element by a few percent (the crystal cells' solid angle is the reference's
-    largest-face approximation, and septal cell centres fall in or out of holes), and the crystal
-    and septal parts are both present in a system whose crystals lie behind a tungsten plate."""
+    """The grid scatter model (oracle_grid.h) is a discretisation.  Its crystal cells converge as
+    the 0.25 mm cell is refined (within a few percent: each cell's solid angle is the
+    reference's largest-face approximation), and so do its septal cells in a plate without
+    holes.  With holes, cells this size alias the hole walls (mu_W times the cell is ~0.85, and
+    most septal scatter comes from the first tenths of a millimetre of wall), so the septal sum
+    there is a property of the stated grid rather than a converged integral."""
     geo = geometry.mini(seed=3, nvox=(2, 1, 1), ncry=(2, 2), nholes=3)
-    for parts in (1, 2):
-        s1 = oracle.scatter_grid(geo, parts=parts, cell=0.125)
-        s2 = oracle.scatter_grid(geo, parts=parts, cell=0.0625)
-        assert s1.max() > 0
-        assert np.all(np.abs(s2 - s1) <= 0.1 * np.abs(s2)), parts
+    c1 = oracle.scatter_grid(geo, parts=1, cell=0.125)
+    c2 = oracle.scatter_grid(geo, parts=1, cell=0.0625)
+    assert c1.max() > 0 and np.all(np.abs(c2 - c1) <= 0.05 * np.abs(c2))
+    plain = geometry.mini(seed=3, nvox=(2, 1, 1), ncry=(2, 2), nholes=0)
+    s1 = oracle.scatter_grid(plain, parts=2, cell=0.25)
+    s2 = oracle.scatter_grid(plain, parts=2, cell=0.0625)
+    assert s1.max() > 0 and np.all(np.abs(s2 - s1) <= 0.005 * np.abs(s2))
+    assert oracle.scatter_grid(geo, parts=2, cell=0.25).max() > 0
