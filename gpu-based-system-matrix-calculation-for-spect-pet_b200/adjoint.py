@@ -35,14 +35,17 @@ sharding = _load("sysmat_sharding", os.path.join(HERE, "sharding.py"))
 
 
 class Projector:
-    """A system whose parameters theta may change; keeps the context of the last theta."""
+    """A system whose parameters theta may change; keeps the context of the last theta.
+    shapes: optional (n_holes, 3) rows (rho_x, rho_z, theta_h) of elliptical holes
+    (sysmat_set_hole_shapes); the tilt turns their frames with the pattern."""
 
-    def __init__(self, geo, device=0, rotation=0.0, det_begin=0, det_count=None):
+    def __init__(self, geo, device=0, rotation=0.0, det_begin=0, det_count=None, shapes=None):
         self.geo = geo
         self.device = device
         self.rotation = float(rotation)
         self.det_begin = det_begin
         self.det_count = geo.n_det - det_begin if det_count is None else det_count
+        self.shapes = None if shapes is None else np.asarray(shapes, dtype=np.float32).reshape(-1, 3)
         self._theta = None
         self._ctx = None
 
@@ -52,6 +55,8 @@ class Projector:
             if self._ctx is not None:
                 self._ctx.close()
             self._ctx = sysmat.Context(geometry.apply_theta(self.geo, theta), device=self.device)
+            if self.shapes is not None:
+                self._ctx.set_hole_shapes(geometry.apply_theta_shapes(self.shapes, theta))
             self._theta = theta.copy()
         return self._ctx
 
@@ -88,12 +93,12 @@ class RotationProjector:
     `context(theta)` may be given to supply the per-theta device context (an object with the
     sysmat.Context project / backproject / vjp methods); by default a Projector's is used."""
 
-    def __init__(self, geo, rotations=None, device=0, context=None):
+    def __init__(self, geo, rotations=None, device=0, context=None, shapes=None):
         self.geo = geo
         self.rotations = [float(r) for r in (range(geo.n_rot) if rotations is None else rotations)]
         self.n_det = geo.n_det
         self.det_count = len(self.rotations) * self.n_det
-        self._context = context if context is not None else Projector(geo, device=device).context
+        self._context = context if context is not None else Projector(geo, device=device, shapes=shapes).context
 
     def _pieces(self, rows):
         first, count = (0, self.det_count) if rows is None else rows

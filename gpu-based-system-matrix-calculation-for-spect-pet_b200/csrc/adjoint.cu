@@ -18,7 +18,6 @@ int adjoint_call(sysmat_ctx* ctx, float rotation, int det_begin, int det_count, 
                  const float* d_u, double* d_out, int kind, void* stream)
 {
     if (!ctx || det_begin < 0 || det_count < 0 || det_begin + det_count > ctx->g.n_det) return SYSMAT_ERR_ARG;
-    if (ctx->g.hole_shape) return SYSMAT_ERR_ARG;   // circular holes only (the derivative uses their chord)
     const size_t n_out = kind == 0 ? (size_t)det_count
                        : kind == 1 ? (size_t)(SYSMAT_THETA_N + 1) : (size_t)ctx->g.nvox;
     if ((n_out && !d_out) || (det_count && ((kind != 2 && !d_x) || (kind >= 1 && !d_u)))) return SYSMAT_ERR_ARG;

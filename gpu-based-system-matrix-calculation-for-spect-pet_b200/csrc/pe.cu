@@ -318,23 +318,53 @@ __device__ __forceinline__ float ray_cyl_chord(const RayCyl& c, float xc, float 
 // Slope-space shadow of a y-aligned object (hole cylinder, or crystal in the disk around its
 // xz footprint) seen from the voxel: every line from the voxel that meets the object at a
 // depth y in [y0, y1] has slopes within rho(y) = R/(y - yI) of the point c(y) on the
-// segment c(y0) -> c(y1), so within rho(y0) of that segment.  capsule_meets_box is false
-// only when that capsule (radius inflated by the slope margin) is separated from the box
-// along x, along z, or along the segment's normal; decided without divisions.
+// segment c(y0) -> c(y1), so within rho(y0) of that segment (the capsule; its radius is
+// inflated by the slope margin).
+struct Capsule {
+    float ax, az, dx, dz, rho;    // c(y0), c(y1) - c(y0), radius
+};
+
+__device__ __forceinline__ Capsule capsule_of(float xo, float zo, float y0, float y1, float R, const Elem& e)
+{
+    const float r0 = __frcp_rn(y0 - e.yI), r1 = __frcp_rn(y1 - e.yI);
+    Capsule c;
+    c.ax = (xo - e.xI) * r0;
+    c.az = (zo - e.zI) * r0;
+    c.dx = (xo - e.xI) * r1 - c.ax;
+    c.dz = (zo - e.zI) * r1 - c.az;
+    c.rho = R * r0 * 1.0001f + kSlopeMargin;
+    return c;
+}
+
+// False only when the capsule is separated from the box along x, along z, or along the
+// segment's normal; decided without divisions.
+__device__ __forceinline__ bool capsule_meets_box(const Capsule& c, float4 box)
+{
+    const float bx = c.ax + c.dx, bz = c.az + c.dz, rho = c.rho;
+    if (fminf(c.ax, bx) - rho > box.y || fmaxf(c.ax, bx) + rho < box.x) return false;
+    if (fminf(c.az, bz) - rho > box.w || fmaxf(c.az, bz) + rho < box.z) return false;
+    const float mx = 0.5f * (box.x + box.y) - c.ax, mz = 0.5f * (box.z + box.w) - c.az;
+    const float sep = fabsf(c.dx * mz - c.dz * mx) - (fabsf(c.dz) * 0.5f * (box.y - box.x) +
+                                                      fabsf(c.dx) * 0.5f * (box.w - box.z));
+    return !(sep > 0.0f && sep * sep > rho * rho * (c.dx * c.dx + c.dz * c.dz));
+}
+
 __device__ __forceinline__ bool capsule_meets_box(float xo, float zo, float y0, float y1, float R,
                                                   const Elem& e, float4 box)
 {
-    const float r0 = __frcp_rn(y0 - e.yI), r1 = __frcp_rn(y1 - e.yI);
-    const float ax = (xo - e.xI) * r0, az = (zo - e.zI) * r0;
-    const float bx = (xo - e.xI) * r1, bz = (zo - e.zI) * r1;
-    const float rho = R * r0 * 1.0001f + kSlopeMargin;
-    if (fminf(ax, bx) - rho > box.y || fmaxf(ax, bx) + rho < box.x) return false;
-    if (fminf(az, bz) - rho > box.w || fmaxf(az, bz) + rho < box.z) return false;
-    const float dx = bx - ax, dz = bz - az;
-    const float mx = 0.5f * (box.x + box.y) - ax, mz = 0.5f * (box.z + box.w) - az;
-    const float sep = fabsf(dx * mz - dz * mx) - (fabsf(dz) * 0.5f * (box.y - box.x) +
-                                                  fabsf(dx) * 0.5f * (box.w - box.z));
-    return !(sep > 0.0f && sep * sep > rho * rho * (dx * dx + dz * dz));
+    return capsule_meets_box(capsule_of(xo, zo, y0, y1, R, e), box);
+}
+
+// Lane test of a hole entry of the round buffer: is the ray's slope (sa, sb) within the
+// hole's capsule?  c = (c(y0), c(y1) - c(y0)), rho2 = radius^2 (infinite for an entry without
+// a capsule: the hole is closer than kMinDepth to the voxel), inv_len2 = 1/|c(y1) - c(y0)|^2
+// (0 for a degenerate segment).
+__device__ __forceinline__ bool in_capsule(const float4& c, float rho2, float inv_len2, float sa, float sb)
+{
+    const float px = sa - c.x, pz = sb - c.y;
+    const float t = fminf(fmaxf((px * c.z + pz * c.w) * inv_len2, 0.0f), 1.0f);
+    const float ex = px - t * c.z, ez = pz - t * c.w;
+    return ex * ex + ez * ez <= rho2;
 }
 
 // Copy kept entries [k0, k1) whose rectangle and capsule meet the round's slope box into
@@ -352,6 +382,9 @@ __device__ __forceinline__ int fill_round(const DevGeom& g, WarpSmem& ws, const 
         bool keep = false;
         int id = 0;
         float4 rect;
+        // hole entries carry their capsule for the lanes' test (none: every slope passes)
+        float4 cap = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        float rho2 = INFINITY, inv_len2 = 0.0f;
         if (kk < k1) {
             rect = ws.rect[kk];
             keep = rects_overlap(rect, box);
@@ -359,7 +392,12 @@ __device__ __forceinline__ int fill_round(const DevGeom& g, WarpSmem& ws, const 
                 id = ws.id[kk];
                 if (id < g.n_holes) {
                     const float4 ha = __ldg(&g.hole.a[id]);
-                    keep = capsule_meets_box(ha.x, ha.w, ha.y, ha.z, __ldg(&g.hole.b[id].x), e, box);
+                    const Capsule c = capsule_of(ha.x, ha.w, ha.y, ha.z, __ldg(&g.hole.b[id].x), e);
+                    keep = capsule_meets_box(c, box);
+                    cap = make_float4(c.ax, c.az, c.dx, c.dz);
+                    rho2 = c.rho * c.rho;
+                    const float l2 = c.dx * c.dx + c.dz * c.dz;
+                    inv_len2 = l2 > 1e-30f ? __frcp_rn(l2) : 0.0f;
                 } else {
                     const int o = id - g.n_holes;
                     const float4 po = __ldg(&g.cry.pos[o]);
@@ -374,15 +412,17 @@ __device__ __forceinline__ int fill_round(const DevGeom& g, WarpSmem& ws, const 
         *nh += __popc(__ballot_sync(0xffffffffu, keep && id < g.n_holes));
         if (keep) {
             const int pos = n + __popc(m & ((1u << lane) - 1u));
-            ws.rr[pos] = rect;
             if constexpr (IDS) {
+                ws.rr[pos] = id < g.n_holes ? cap : rect;
+                ws.rb[pos] = make_float4(0.0f, 0.0f, rho2, inv_len2);
                 ws.ra[pos].x = __int_as_float(id);
                 ws.rl[pos] = id < g.n_holes ? layer_of_hole(g, id) : g.n_layers;
             } else if (id < g.n_holes) {
                 const float4 ha = __ldg(&g.hole.a[id]);
                 const float4 hb = __ldg(&g.hole.b[id]);
+                ws.rr[pos] = cap;
                 ws.ra[pos] = make_float4(ha.x, ha.w, hb.x, hb.y);
-                ws.rb[pos] = make_float4(ha.y, ha.z, 0.0f, 0.0f);
+                ws.rb[pos] = make_float4(ha.y, ha.z, rho2, inv_len2);
                 if constexpr (ELL) {        // rho_x, rho_z, cos, sin; a batch may mix in circular systems
                     ws.rc[pos] = g.hole_shape ? __ldg(&g.hole_shape[id]) : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
                 }
@@ -394,6 +434,7 @@ __device__ __forceinline__ int fill_round(const DevGeom& g, WarpSmem& ws, const 
                 const float4 to = __ldg(&g.cry.trig[o]);
                 float xa, ya, za;                                   // :1305-1307
                 to_crystal_frame(po.x, po.y, po.z, to.z, to.w, e.xI, e.yI, e.zI, xa, ya, za);
+                ws.rr[pos] = rect;
                 ws.ra[pos] = make_float4(po.x, po.y, po.z, __ldg(&g.cry.mu[o].x));
                 ws.rb[pos] = make_float4(to.z, to.w, so.x, so.y);
                 ws.rc[pos] = make_float4(so.z, xa, ya, za);
@@ -408,6 +449,13 @@ __device__ __forceinline__ int fill_round(const DevGeom& g, WarpSmem& ws, const 
     return n;
 }
 
+// Lane test of round-buffer hole entry j (see in_capsule).
+__device__ __forceinline__ bool hole_in_reach(const WarpSmem& ws, int j, float sa, float sb)
+{
+    const float4 b = ws.rb[j];
+    return in_capsule(ws.rr[j], b.z, b.w, sa, sb);
+}
+
 // Walk round-buffer entries [0, nr) for one sub-element ray (voxel -> (xD, yD, zD)); holes
 // occupy [0, nh) and crystals [nh, nr), both in the reference's object order; the layer
 // terms are added when the walk leaves a layer.
@@ -419,7 +467,7 @@ __device__ __forceinline__ void walk_round(const DevGeom& g, const WarpSmem& ws,
     for (int j = 0; j < nh; ++j) {
         const int m = ws.rl[j];
         if (m != s.lay) close_layers(g, s, m, cosang);
-        if (!in_rect(ws.rr[j], sa_a, sa_b)) continue;
+        if (!hole_in_reach(ws, j, sa_a, sa_b)) continue;
         const float4 A = ws.ra[j];
         const float4 B = ws.rb[j];
         float tmp;
@@ -1058,7 +1106,7 @@ static int launch_mode(const DevGeom& g, const PeLaunch& L, int num_sms, cudaStr
     return cudaGetLastError() == cudaSuccess ? 0 : -1;
 }
 
-template <int KIND>
+template <int KIND, bool ELL>
 static int launch_adjoint_kind(const DevGeom& g, const AdjLaunch& L, int num_sms, cudaStream_t stream)
 {
     const int smem = (int)sizeof(AdjSmem);
@@ -1067,23 +1115,29 @@ static int launch_adjoint_kind(const DevGeom& g, const AdjLaunch& L, int num_sms
     if (cudaGetDevice(&dev) != cudaSuccess) return -1;
     const unsigned long long bit = 1ull << (dev & 63);
     if (!(__atomic_load_n(&configured, __ATOMIC_ACQUIRE) & bit)) {
-        if (cudaFuncSetAttribute(pe_adjoint_kernel<KIND>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem) !=
+        if (cudaFuncSetAttribute(pe_adjoint_kernel<KIND, ELL>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem) !=
             cudaSuccess)
             return -1;
         __atomic_fetch_or(&configured, bit, __ATOMIC_RELEASE);
     }
     int per_sm = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, pe_adjoint_kernel<KIND>, kThreads, smem);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, pe_adjoint_kernel<KIND, ELL>, kThreads, smem);
     if (per_sm < 1) per_sm = 1;
-    pe_adjoint_kernel<KIND><<<num_sms * per_sm, kThreads, smem, stream>>>(g, L);
+    pe_adjoint_kernel<KIND, ELL><<<num_sms * per_sm, kThreads, smem, stream>>>(g, L);
     return cudaGetLastError() == cudaSuccess ? 0 : -1;
 }
 
+// Systems with elliptical holes (sysmat_set_hole_shapes) run the elliptical instances.
 int launch_pe_adjoint(const DevGeom& g, const AdjLaunch& L, int kind, int num_sms, cudaStream_t stream)
 {
-    if (kind == 0) return launch_adjoint_kind<0>(g, L, num_sms, stream);
-    if (kind == 1) return launch_adjoint_kind<1>(g, L, num_sms, stream);
-    return launch_adjoint_kind<2>(g, L, num_sms, stream);
+    if (g.hole_shape) {
+        if (kind == 0) return launch_adjoint_kind<0, true>(g, L, num_sms, stream);
+        if (kind == 1) return launch_adjoint_kind<1, true>(g, L, num_sms, stream);
+        return launch_adjoint_kind<2, true>(g, L, num_sms, stream);
+    }
+    if (kind == 0) return launch_adjoint_kind<0, false>(g, L, num_sms, stream);
+    if (kind == 1) return launch_adjoint_kind<1, false>(g, L, num_sms, stream);
+    return launch_adjoint_kind<2, false>(g, L, num_sms, stream);
 }
 
 template <int MODE, bool ELL>

@@ -9,7 +9,12 @@
 //   dx, dz      shift of every hole centre; dy shift of the hole caps and layer planes;
 //   tilt        rotation of the hole pattern about the y axis (x' = x cos - z sin,
 //               z' = x sin + z cos), the one collimator rotation that keeps holes
-//               parallel to y as the reference's cylinder chord requires.
+//               parallel to y as the reference's cylinder chord requires; it turns an
+//               elliptical hole's frame with it (theta_h + tilt).
+// Elliptical holes (PESysMatGen.cu:801-947, sysmat_set_hole_shapes) contribute the partials
+// of their chord with respect to the centre, the caps and the frame angle; their chord does
+// not read the radius field (it only bounds the ellipse for the cone test), so the radius
+// partial has no elliptical term.
 // The derivative of A[d,v] = sum_s Omega_s exp(-att_s) absf_s follows the reference's float
 // program branch by branch (PESysMatGen.cu:1240-1357): each non-zero hole chord contributes
 // its analytic partials, the layer term mu_L (T/cos - sum L) its own, crystal chords and the
@@ -50,6 +55,61 @@ __device__ __forceinline__ float ray_cyl_chord_grad(const RayCyl& c, float xc, f
     return L;
 }
 
+// Partials of the elliptical-cylinder chord (ell_chord, same case analysis) with respect to the
+// centre (xc, zc), a common shift dy of both cap planes and the frame angle theta (carried in
+// CylGrad.dr).  In the hole's frame the ray is p(t) = (u0 + kx t, y_in + ky t, w0 + kz t) and
+// the side crossings solve a t^2 + 2 b t + c = 0 with a = kx^2 rz^2 + kz^2 rx^2,
+// b = kx u0 rz^2 + kz w0 rx^2, c = rz^2 u0^2 + rx^2 w0^2 - rx^2 rz^2; the centre moves
+// (u0, w0) and the angle turns (u0, w0) and (kx, kz) together.
+__device__ __forceinline__ float ell_chord_grad(float xi, float yi, float zi, float xo, float yo, float zo,
+                                                float xc, float y1, float y2, float zc, float rx, float rz,
+                                                float ct, float st, CylGrad& gr)
+{
+    gr = CylGrad{0.0f, 0.0f, 0.0f, 0.0f};
+    const float L = ell_chord(xi, yi, zi, xo, yo, zo, xc, y1, y2, zc, rx, rz, ct, st);
+    if (L == 0.0f) return L;
+    // the frame quantities of ell_chord, with its expressions (same case flags)
+    const float xi_ = xi - xc, zi_ = zi - zc, xo_ = xo - xc, zo_ = zo - zc;
+    const float xin = xc + xi_ * ct + zi_ * st, zin = zc - xi_ * st + zi_ * ct;
+    const float xout = xc + xo_ * ct + zo_ * st, zout = zc - xo_ * st + zo_ * ct;
+    const float tio = sqrtf((xout - xin) * (xout - xin) + (yo - yi) * (yo - yi) + (zout - zin) * (zout - zin));
+    const float kx = (xout - xin) / tio, ky = (yo - yi) / tio, kz = (zout - zin) / tio;
+    const float xl = xin + kx / ky * (y1 - yi), xr = xin + kx / ky * (y2 - yi);
+    const float zl = zin + kz / ky * (y1 - yi), zr = zin + kz / ky * (y2 - yi);
+    const bool fl = ((xl - xc) * (xl - xc) / rx / rx + (zl - zc) * (zl - zc) / rz / rz) <= 1.0f;
+    const bool fr = ((xr - xc) * (xr - xc) / rx / rx + (zr - zc) * (zr - zc) / rz / rz) <= 1.0f;
+    if (fl && fr) return L;                     // |tb - ta|: cap to cap, shift and turn invariant
+    const float u0 = xin - xc, w0 = zin - zc;
+    const float rx2 = rx * rx, rz2 = rz * rz;
+    const float a = kx * kx * rz2 + kz * kz * rx2;
+    const float b = kx * u0 * rz2 + kz * w0 * rx2;
+    const float c = rz2 * u0 * u0 + rx2 * w0 * w0 - rx2 * rz2;
+    const float sq = sqrtf(b * b - a * c);
+    const float ia = 1.0f / a, isq = 0.5f / sq;
+    const float t1 = (-b - sq) * ia, t2 = (-b + sq) * ia;
+    // d(t1), d(t2) for a parameter moving (u0, w0, kx, kz) by (du, dw, dkx, dkz)
+    auto dts = [&](float du, float dw, float dkx, float dkz, float& d1, float& d2) {
+        const float da = 2.0f * (kx * dkx * rz2 + kz * dkz * rx2);
+        const float db = (dkx * u0 + kx * du) * rz2 + (dkz * w0 + kz * dw) * rx2;
+        const float dc = 2.0f * (rz2 * u0 * du + rx2 * w0 * dw);
+        const float dsq = (2.0f * b * db - da * c - a * dc) * isq;
+        d1 = (-db - dsq - t1 * da) * ia;
+        d2 = (-db + dsq - t2 * da) * ia;
+    };
+    float x1, x2, z1, z2, p1, p2;
+    dts(-ct, st, 0.0f, 0.0f, x1, x2);           // xc: u0 = (x - xc) ct + ..., w0 = -(x - xc) st + ...
+    dts(-st, -ct, 0.0f, 0.0f, z1, z2);          // zc
+    dts(w0, -u0, kz, -kx, p1, p2);              // frame angle
+    if (!fl && !fr) {                           // side to side
+        gr = CylGrad{p2 - p1, x2 - x1, z2 - z1, 0.0f};
+    } else if (fl) {                            // cap y1 to side: t2 - ta
+        gr = CylGrad{p2, x2, z2, -1.0f / ky};
+    } else {                                    // side to cap y2: tb - t1
+        gr = CylGrad{-p1, -x1, -z1, 1.0f / ky};
+    }
+    return L;
+}
+
 // Walk state with the partials of att (index: theta order) and the current layer's sums of
 // hole-chord partials (radius, x, z, y, tilt).
 struct WalkGrad {
@@ -79,6 +139,7 @@ __device__ __forceinline__ void close_layers_grad(const DevGeom& g, WalkGrad& s,
     }
 }
 
+template <bool ELL>
 __device__ __forceinline__ void walk_round_grad(const DevGeom& g, const WarpSmem& ws, int nh, int nr, float xD,
                                                 float yD, float zD, float sa_a, float sa_b, float cosang,
                                                 RayCyl& rc, WalkGrad& s)
@@ -86,18 +147,31 @@ __device__ __forceinline__ void walk_round_grad(const DevGeom& g, const WarpSmem
     for (int j = 0; j < nh; ++j) {
         const int m = ws.rl[j];
         if (m != s.lay) close_layers_grad(g, s, m, cosang);
-        if (!in_rect(ws.rr[j], sa_a, sa_b)) continue;
+        if (!hole_in_reach(ws, j, sa_a, sa_b)) continue;
         const float4 A = ws.ra[j];               // x, z, R, mu of the hole
         const float4 B = ws.rb[j];
-        ray_cyl_caps(rc, B.x, B.y);
         CylGrad gr;
-        const float tmp = ray_cyl_chord_grad(rc, A.x, A.y, A.z, gr);
+        float tmp, dr = 0.0f, dth = 0.0f;        // radius and frame-angle partials
+        bool ell = false;
+        if constexpr (ELL) {
+            const float4 S = ws.rc[j];
+            if (S.x > 0.0f) {                    // elliptical hole: gr.dr holds the angle partial
+                tmp = ell_chord_grad(rc.xi, rc.yi, rc.zi, xD, yD, zD, A.x, B.x, B.y, A.y, S.x, S.y, S.z, S.w, gr);
+                dth = gr.dr;
+                ell = true;
+            }
+        }
+        if (!ell) {
+            ray_cyl_caps(rc, B.x, B.y);
+            tmp = ray_cyl_chord_grad(rc, A.x, A.y, A.z, gr);
+            dr = gr.dr;
+        }
         s.len = s.len + tmp;                                     // :1276-1278
         s.att = s.att + A.w * tmp;
         if (tmp != 0.0f) {
-            const float dp = -A.y * gr.dx + A.x * gr.dz;         // tilt about the y axis
-            s.lr += gr.dr; s.lx += gr.dx; s.lz += gr.dz; s.ly += gr.dy; s.lp += dp;
-            s.da[2] += A.w * gr.dr; s.da[3] += A.w * gr.dx; s.da[4] += A.w * gr.dy;
+            const float dp = -A.y * gr.dx + A.x * gr.dz + dth;   // tilt about the y axis
+            s.lr += dr; s.lx += gr.dx; s.lz += gr.dz; s.ly += gr.dy; s.lp += dp;
+            s.da[2] += A.w * dr; s.da[3] += A.w * gr.dx; s.da[4] += A.w * gr.dy;
             s.da[5] += A.w * gr.dz; s.da[6] += A.w * dp;
         }
     }
@@ -158,6 +232,7 @@ __device__ __forceinline__ float finish_sub_element_grad(const Elem& e, const Su
 
 // Value and theta-partials of element (d, v), summed over its sub-elements in double; every
 // lane returns the warp's totals in acc[0..7] (acc[kThetaN] = the value).
+template <bool ELL>
 __device__ __forceinline__ void pe_element_grad(const DevGeom& g, const BlockSmem& bs, WarpSmem& ws, int d, long long v,
                                 float cr, float sr, int lane, double* acc)
 {
@@ -207,8 +282,8 @@ __device__ __forceinline__ void pe_element_grad(const DevGeom& g, const BlockSme
             int k = 0;
             while (k < count) {
                 int next = count, nh = 0;
-                const int nr = fill_round<false>(g, ws, e, k, count, box, 0, lane, &next, &nh);
-                if (!skip) walk_round_grad(g, ws, nh, nr, q.xD, q.yD, q.zD, q.sa_a, q.sa_b, q.cosang, rc, s);
+                const int nr = fill_round<ELL>(g, ws, e, k, count, box, 0, lane, &next, &nh);
+                if (!skip) walk_round_grad<ELL>(g, ws, nh, nr, q.xD, q.yD, q.zD, q.sa_a, q.sa_b, q.cosang, rc, s);
                 __syncwarp();
                 k = next;
             }
@@ -238,7 +313,7 @@ struct AdjSmem {
 // KIND 1: grad[i] += sum_{d,v} u[d - det_begin] x[v] dA[d,v]/dtheta_i, grad[7] += u^T A x.
 // KIND 2: q[v] += sum_d A[d,v] u[d - det_begin] (back projection; x is not read).
 // Elements of zero weight are skipped, and so are bricks whose voxels all have x = 0.
-template <int KIND>
+template <int KIND, bool ELL>
 __global__ void __launch_bounds__(kThreads, 2) pe_adjoint_kernel(DevGeom g, AdjLaunch L)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -293,14 +368,14 @@ __global__ void __launch_bounds__(kThreads, 2) pe_adjoint_kernel(DevGeom g, AdjL
                 const float xv = KIND == 2 ? 1.0f : L.x[v];
                 if (xv == 0.0f || ud == 0.0f) continue;
                 if constexpr (KIND == 0) {
-                    const double val = pe_element<1, false>(g, bs, ws, d, v, cr, sr, lane, nullptr);
+                    const double val = pe_element<1, false, ELL>(g, bs, ws, d, v, cr, sr, lane, nullptr);
                     if (lane == 0) atomicAdd(&L.p[di], val * (double)xv);
                 } else if constexpr (KIND == 2) {
-                    const double val = pe_element<1, false>(g, bs, ws, d, v, cr, sr, lane, nullptr);
+                    const double val = pe_element<1, false, ELL>(g, bs, ws, d, v, cr, sr, lane, nullptr);
                     if (lane == 0) atomicAdd(&L.q[v], val * (double)ud);
                 } else {
                     double acc[kThetaN + 1];
-                    pe_element_grad(g, bs, ws, d, v, cr, sr, lane, acc);
+                    pe_element_grad<ELL>(g, bs, ws, d, v, cr, sr, lane, acc);
                     const double wgt = (double)ud * (double)xv;
                     if (lane == 0)
 #pragma unroll

@@ -186,7 +186,7 @@ __device__ __forceinline__ void walk_round64(const DevGeom& g, const WarpSmem& w
     for (int j = 0; j < nh; ++j) {
         const int m = ws.rl[j];
         if (m != s.lay) close_layers64(g, s, m, Q.cosang);
-        if (!in_rect(ws.rr[j], sa_a, sa_b)) continue;
+        if (!hole_in_reach(ws, j, sa_a, sa_b)) continue;
         const int id = __float_as_int(ws.ra[j].x);
         const D4 a = g.t64.hole_a[id], b = g.t64.hole_b[id];
         double tmp;

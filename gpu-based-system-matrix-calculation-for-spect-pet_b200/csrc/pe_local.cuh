@@ -27,6 +27,7 @@
 struct ElemL {
     Elem64 e64;                  // double constants of the cone test (init_elem64)
     double rxc, rzc;             // slopes dx/dy, dz/dy of the ray voxel -> crystal d's centre
+    double idyc;                 // 1 / dy of that ray
     float fdx, fdy, fdz;         // crystal d's centre minus the voxel
     float frxc, frzc;
     float cr, sr, cmr, smr;      // cos, sin of rot_d and of -rot_d
@@ -48,8 +49,9 @@ __device__ __forceinline__ void init_elem_local(const DevGeom& g, int d, long lo
     L.rfz = 1.0f / (float)nz;
     const Elem64& E = L.e64;
     const double dx = E.xd - E.xI, dy = E.yd - E.yI, dz = E.zd - E.zI;
-    L.rxc = dx / dy;
-    L.rzc = dz / dy;
+    L.idyc = 1.0 / dy;
+    L.rxc = dx * L.idyc;
+    L.rzc = dz * L.idyc;
     L.fdx = (float)dx;
     L.fdy = (float)dy;
     L.fdz = (float)dz;
@@ -278,11 +280,13 @@ __device__ __forceinline__ RayL ray_local(const ElemL& L, float xDs, float yDs, 
     r.rx = L.frxc + r.drx;
     r.rz = L.frzc + r.drz;
     const Elem64& E = L.e64;
-    const double dx = (E.xd - E.xI) + (double)r.ox, dy = (E.yd - E.yI) + (double)r.oy;
-    const double dz = (E.zd - E.zI) + (double)r.oz;
-    r.dsec = sqrt(dx * dx + dy * dy + dz * dz) / dy;
-    r.ddrx = ((double)r.ox * (E.yd - E.yI) - (E.xd - E.xI) * (double)r.oy) / (dy * (E.yd - E.yI));
-    r.ddrz = ((double)r.oz * (E.yd - E.yI) - (E.zd - E.zI) * (double)r.oy) / (dy * (E.yd - E.yI));
+    const double cx = E.xd - E.xI, cy = E.yd - E.yI, cz = E.zd - E.zI;   // voxel -> crystal d's centre
+    const double dx = cx + (double)r.ox, dy = cy + (double)r.oy, dz = cz + (double)r.oz;
+    const double idy = 1.0 / dy;
+    r.dsec = sqrt(dx * dx + dy * dy + dz * dz) * idy;
+    const double f = idy * L.idyc;
+    r.ddrx = ((double)r.ox * cy - cx * (double)r.oy) * f;
+    r.ddrz = ((double)r.oz * cy - cz * (double)r.oy) * f;
     r.drx_ = L.rxc + r.ddrx;
     r.drz_ = L.rzc + r.ddrz;
     r.da = r.drx_ * r.drx_ + r.drz_ * r.drz_;
@@ -429,7 +433,8 @@ __device__ __forceinline__ void neumaier_add(float& s, float& c, float x)
 }
 
 // The element of the local form.  smp: the crystal division (voxel centre sources only); nullptr
-// = the reference's 8 x 16 x 8.  Sub-elements go 32 to a round in (z, depth, x) order, x
+// = the reference's 8 x 16 x 8, whose rounds are the compact 2 z x 8 x x 2 depth patches of
+// the reference-order kernel; other divisions go 32 to a round in (z, depth, x) order, x
 // fastest.  sub_out: when set, each sub-element's contribution is also written there, at index
 // (iz * ny + iy) * nx + ix (the scatter grid's crystal-cell weights).
 __device__ double pe_element_local(const DevGeom& g, const BlockSmem& bs, WarpSmem& ws, int d, long long v, float cr,
@@ -459,9 +464,21 @@ __device__ double pe_element_local(const DevGeom& g, const BlockSmem& bs, WarpSm
     float sum = 0.0f, comp = 0.0f;
     for (int base = 0; base < n_sub; base += 32) {
         const bool dead = base + lane >= n_sub;
-        const int sidx = dead ? n_sub - 1 : base + lane;
-        const int iz = sidx / nxy, rem = sidx - iz * nxy;
-        const int iy = rem / nx, ix = rem - iy * nx;
+        int sidx, ix, iy, iz;
+        if (!smp) {                       // s = 128 iz + 16 ix + iy, as in pe_element's rounds
+            const int rr = base >> 5;
+            const int s = ((rr >> 3) * 2 + (lane >> 4)) * 128 + ((lane >> 1) & 7) * 16 + (rr & 7) * 2 + (lane & 1);
+            iz = s >> 7;
+            ix = (s >> 4) & 7;
+            iy = s & 15;
+            sidx = (iz * ny + iy) * nx + ix;
+        } else {
+            sidx = dead ? n_sub - 1 : base + lane;
+            iz = sidx / nxy;
+            const int rem = sidx - iz * nxy;
+            iy = rem / nx;
+            ix = rem - iy * nx;
+        }
         const float xDs = -L.w / 2.0f + ((float)ix + 0.5f) * gx * L.w;       // :1207-1217
         const float zDs = -L.h / 2.0f + ((float)iz + 0.5f) * gz * L.h;
         const float yDs = -L.t / 2.0f + ((float)iy + 0.5f) * gy * L.t;

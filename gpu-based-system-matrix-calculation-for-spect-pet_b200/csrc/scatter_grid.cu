@@ -59,10 +59,18 @@ constexpr int kGridMaxVox = 48;          // voxels per pass
 constexpr int kGridDetTile = 64;         // detectors per block
 constexpr int kGridChunksPerBlock = 8;
 
+
+// Septal cells are numbered brick by brick (bricks of 8 x 4 x 8 cells, x fastest inside a brick
+// and among bricks), so that a chunk of consecutive septal cells is a compact region: the
+// chunk's candidate holes and crystals (those near the segments from its points to a detector
+// or a voxel) are then found once per chunk.
+constexpr int kBrickX = 8, kBrickY = 4, kBrickZ = 8, kBrickCells = kBrickX * kBrickY * kBrickZ;
+
 struct GridLayer {
     double x0, y0, z0;                   // plate box corner
     double cx, cy, cz;                   // cell size
     int nx, ny, nz;
+    int nbx, nby, nbz;                   // bricks per axis
     int hole_begin, hole_count;
     float mu_t, mu_pe, mu_c;
 };
@@ -71,9 +79,23 @@ struct GridGeom {
     int n_layers;
     GridLayer layer[kMaxLayers];
     long long sep_begin[kMaxLayers + 1];   // septal cells of layer m: [sep_begin[m], sep_begin[m+1])
-    const int* sep_cell;                   // linear cell index (ix + nx (iy + ny iz)) within its layer
+    const int* sep_cell;                   // brick-ordered cell index within its layer (cell_of)
     const float* raw_col;                  // collimator parameters (hole media)
 };
+
+__device__ __forceinline__ void atomicMin_float(float* a, float v)
+{
+    v += 0.0f;                           // -0 -> +0: the integer orders below need one zero
+    if (v >= 0.0f) atomicMin((int*)a, __float_as_int(v));
+    else atomicMax((unsigned int*)a, __float_as_uint(v));
+}
+
+__device__ __forceinline__ void atomicMax_float(float* a, float v)
+{
+    v += 0.0f;
+    if (v >= 0.0f) atomicMax((int*)a, __float_as_int(v));
+    else atomicMin((unsigned int*)a, __float_as_uint(v));
+}
 
 __device__ __forceinline__ void voxel_centre64(const DevGeom& g, long long v, float rotation, double& x, double& y,
                                                double& z)
@@ -93,16 +115,132 @@ __device__ __forceinline__ void voxel_centre64(const DevGeom& g, long long v, fl
     z = ((double)iz - (double)g.nz / 2.0 + 0.5) * (double)g.wz + (double)g.shz;
 }
 
+// Cell (ix, iy, iz) of brick-ordered index c of layer L (cells of a partial brick past the
+// plate's edge have ix >= nx, iy >= ny or iz >= nz).
+__device__ __forceinline__ void cell_of(const GridLayer& L, int c, int& ix, int& iy, int& iz)
+{
+    const int b = c / kBrickCells, w = c - b * kBrickCells;
+    const int bx = b % L.nbx, by = (b / L.nbx) % L.nby, bz = b / (L.nbx * L.nby);
+    ix = bx * kBrickX + (w % kBrickX);
+    iy = by * kBrickY + (w / kBrickX) % kBrickY;
+    iz = bz * kBrickZ + w / (kBrickX * kBrickY);
+}
+
 __device__ __forceinline__ void septal_point(const GridGeom& G, long long j, int& m, double p[3])
 {
     m = 0;
     while (m + 1 < G.n_layers && j >= G.sep_begin[m + 1]) ++m;
     const GridLayer& L = G.layer[m];
-    const int c = __ldg(&G.sep_cell[j]);
-    const int ix = c % L.nx, iy = (c / L.nx) % L.ny, iz = c / (L.nx * L.ny);
+    int ix, iy, iz;
+    cell_of(L, __ldg(&G.sep_cell[j]), ix, iy, iz);
     p[0] = L.x0 + ((double)ix + 0.5) * L.cx;
     p[1] = L.y0 + ((double)iy + 0.5) * L.cy;
     p[2] = L.z0 + ((double)iz + 0.5) * L.cz;
+}
+
+// Candidate lists of a chunk of points (block shared memory): the crystals and, per layer, the
+// holes that may lie on a segment from one of the chunk's points to a common far end.  A list
+// longer than its capacity is not used (n = -1: scan everything).
+constexpr int kCandCry = 1024, kCandHole = 2048;
+
+struct Cands {
+    int n_cry;
+    int hole_off[kMaxLayers + 1];        // holes of layer m: hole[hole_off[m] .. hole_off[m+1]); -1 = all
+    int cry[kCandCry];
+    int hole[kCandHole];
+    int warp_cnt[kGridThreads / 32];
+    float lo[3], hi[3];                  // the chunk's bounding box
+};
+
+// Ordered compaction over the block of the items i in [0, n) with keep(i) into list[off ..]
+// (capacity cap); returns the number kept, or -1 past the capacity.
+template <class F>
+__device__ int block_select(int n, F keep, int* list, int off, int cap, int* warp_cnt)
+{
+    const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
+    int total = 0;
+    for (int base = 0; base < n; base += kGridThreads) {
+        const int i = base + t;
+        const bool k = i < n && keep(i);
+        const unsigned m = __ballot_sync(0xffffffffu, k);
+        if (lane == 0) warp_cnt[warp] = __popc(m);
+        __syncthreads();
+        int before = 0, all = 0;
+        for (int w = 0; w < kGridThreads / 32; ++w) {
+            const int c = warp_cnt[w];
+            if (w < warp) before += c;
+            all += c;
+        }
+        const int pos = total + before + __popc(m & ((1u << lane) - 1u));
+        if (k && pos < cap) list[off + pos] = i;
+        total += all;
+        __syncthreads();
+    }
+    return total <= cap ? total : -1;
+}
+
+// Bounding box of the block's points (threads without a point pass has = false).
+__device__ void block_bounds(Cands& C, bool has, const double p[3])
+{
+    const int t = threadIdx.x;
+    if (t < 3) { C.lo[t] = INFINITY; C.hi[t] = -INFINITY; }
+    __syncthreads();
+    if (has) {
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+            atomicMin_float(&C.lo[a], (float)p[a]);
+            atomicMax_float(&C.hi[a], (float)p[a]);
+        }
+    }
+    __syncthreads();
+}
+
+// Candidates for segments from the chunk's points to E (far end): crystals (bounding spheres)
+// when cry, and the holes of every layer when holes.  A point within r_c of the box centre c
+// has its segment within r_c of the segment c -> E, so the tests widen by r_c.
+__device__ void chunk_candidates(const DevGeom& g, const GridGeom& G, Cands& C, const double E[3], bool cry,
+                                 bool holes)
+{
+    const float cx = 0.5f * (C.lo[0] + C.hi[0]), cy = 0.5f * (C.lo[1] + C.hi[1]), cz = 0.5f * (C.lo[2] + C.hi[2]);
+    const float rc = 0.5f * sqrtf((C.hi[0] - C.lo[0]) * (C.hi[0] - C.lo[0]) + (C.hi[1] - C.lo[1]) * (C.hi[1] - C.lo[1]) +
+                                  (C.hi[2] - C.lo[2]) * (C.hi[2] - C.lo[2])) + 2e-3f;
+    const float ex = (float)E[0], ey = (float)E[1], ez = (float)E[2];
+    const float gx = ex - cx, gy = ey - cy, gz = ez - cz;
+    const float gl2 = gx * gx + gy * gy + gz * gz;
+    if (cry) {
+        const int n = block_select(g.n_det, [&](int a) {
+            const float4 pa = __ldg(&g.cry.pos[a]);
+            const float ra = 0.5f * __ldg(&g.cry.size[a].w) + 1e-3f + rc;
+            const float hx = pa.x - cx, hy = pa.y - cy, hz = pa.z - cz;
+            float u = gl2 > 0.0f ? (hx * gx + hy * gy + hz * gz) / gl2 : 0.0f;
+            u = fminf(fmaxf(u, 0.0f), 1.0f);
+            const float qx = hx - u * gx, qy = hy - u * gy, qz = hz - u * gz;
+            return qx * qx + qy * qy + qz * qz <= ra * ra;
+        }, C.cry, 0, kCandCry, C.warp_cnt);
+        if (threadIdx.x == 0) C.n_cry = n;
+    }
+    if (holes) {
+        int off = 0;
+        for (int m = 0; m < G.n_layers; ++m) {
+            const GridLayer& L = G.layer[m];
+            int n = -1;
+            if (off >= 0)
+                n = block_select(L.hole_count, [&](int j) {
+                    const float4 ha = __ldg(&g.hole.a[L.hole_begin + j]);
+                    const float r = __ldg(&g.hole.b[L.hole_begin + j].x) + rc + 1e-3f;
+                    const float hx = ha.x - cx, hz = ha.w - cz;
+                    const float l2 = gx * gx + gz * gz;
+                    float u = l2 > 0.0f ? (hx * gx + hz * gz) / l2 : 0.0f;
+                    u = fminf(fmaxf(u, 0.0f), 1.0f);
+                    const float qx = hx - u * gx, qz = hz - u * gz;
+                    return qx * qx + qz * qz <= r * r;
+                }, C.hole, off, kCandHole - off, C.warp_cnt);
+            if (threadIdx.x == 0) C.hole_off[m] = off < 0 || n < 0 ? -1 : off;
+            off = off < 0 || n < 0 ? -1 : off + n;
+        }
+        if (threadIdx.x == 0) C.hole_off[G.n_layers] = off;
+    }
+    __syncthreads();
 }
 
 // Hole h's axis (x, z) is farther than r from the xz projection of segment a -> b (with a
@@ -172,15 +310,19 @@ __device__ double seg_cyl64(const double A[3], const double B[3], double xc, dou
 // length in the plate box minus its lengths in the layer's holes, with the layer's
 // coefficients, plus its lengths in the holes with the holes' own coefficients.
 __device__ void layer_path64(const DevGeom& g, const GridGeom& G, int m, const double A[3], const double B[3],
-                             double& wt, double& wpe, double& wc)
+                             double& wt, double& wpe, double& wc, const Cands* C = nullptr)
 {
     const double* Ly = g.t64.layer + kLayer64 * m;
     const double lo[3] = {Ly[0], Ly[2], Ly[4]}, hi[3] = {Ly[1], Ly[3], Ly[5]};
     const double box = seg_box64(A, B, lo, hi);
     if (box == 0.0) return;
     const GridLayer& L = G.layer[m];
+    // candidate holes of the chunk (in hole order), or every hole of the layer
+    const bool listed = C && C->hole_off[m] >= 0 && C->hole_off[m + 1] >= 0;
+    const int n = listed ? C->hole_off[m + 1] - C->hole_off[m] : L.hole_count;
     double hsum = 0.0;
-    for (int j = L.hole_begin; j < L.hole_begin + L.hole_count; ++j) {
+    for (int q = 0; q < n; ++q) {
+        const int j = L.hole_begin + (listed ? C->hole[C->hole_off[m] + q] : q);
         const D4 a = g.t64.hole_a[j];
         const double r = g.t64.hole_b[j].x;
         if (hole_far(A[0], A[2], B[0], B[2], a.x, a.w, r)) continue;
@@ -201,31 +343,42 @@ __device__ void layer_path64(const DevGeom& g, const GridGeom& G, int m, const d
 }
 
 // Septal weight V / (4 pi r^2) exp(-A(v -> p)) mu_C for every (voxel, septal cell).
-__global__ void septal_weight_kernel(DevGeom g, GridGeom G, long long vox_begin, int nv, float rotation,
-                                     long long n_sep, float* __restrict__ ws)
+// Block (chunk of kGridThreads septal cells, voxel): the chunk's candidate holes for segments to
+// the voxel are found once, then each thread forms its cell's weight.
+__global__ void __launch_bounds__(kGridThreads) septal_weight_kernel(DevGeom g, GridGeom G, long long vox_begin,
+                                                                     float rotation, long long n_sep,
+                                                                     float* __restrict__ ws)
 {
-    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= (long long)nv * n_sep) return;
-    const int vi = (int)(i / n_sep);
-    const long long j = i - (long long)vi * n_sep;
-    int m;
-    double p[3], I3[3];
-    septal_point(G, j, m, p);
+    __shared__ Cands C;
+    const int vi = blockIdx.y;
+    const long long j = (long long)blockIdx.x * kGridThreads + threadIdx.x;
+    const bool has = j < n_sep;
+    int m = 0;
+    double p[3] = {0.0, 0.0, 0.0}, I3[3];
+    if (has) septal_point(G, j, m, p);
     voxel_centre64(g, vox_begin + vi, rotation, I3[0], I3[1], I3[2]);
+    block_bounds(C, has, p);
+    chunk_candidates(g, G, C, I3, false, true);
+    if (!has) return;
     double at = 0.0, ape = 0.0, ac = 0.0;
-    for (int mm = 0; mm < G.n_layers; ++mm) layer_path64(g, G, mm, I3, p, at, ape, ac);
+    for (int mm = 0; mm < G.n_layers; ++mm) layer_path64(g, G, mm, I3, p, at, ape, ac, &C);
     const GridLayer& L = G.layer[m];
     const double r2 = (p[0] - I3[0]) * (p[0] - I3[0]) + (p[1] - I3[1]) * (p[1] - I3[1]) + (p[2] - I3[2]) * (p[2] - I3[2]);
     const double vcell = L.cx * L.cy * L.cz;
-    ws[i] = (float)(vcell / (4.0 * 3.14159265358979323846 * r2) * exp(-at) * (double)L.mu_c);
+    ws[(long long)vi * n_sep + j] = (float)(vcell / (4.0 * 3.14159265358979323846 * r2) * exp(-at) * (double)L.mu_c);
 }
 
 // Septal cells of layer m: cell centre outside every hole of the layer.
-__global__ void septal_mark_kernel(DevGeom g, GridLayer L, unsigned char* __restrict__ flag)
+__global__ void septal_mark_kernel(DevGeom g, GridLayer L, int n_cells, unsigned char* __restrict__ flag)
 {
     const int c = blockIdx.x * blockDim.x + threadIdx.x;
-    if (c >= L.nx * L.ny * L.nz) return;
-    const int ix = c % L.nx, iy = (c / L.nx) % L.ny, iz = c / (L.nx * L.ny);
+    if (c >= n_cells) return;
+    int ix, iy, iz;
+    cell_of(L, c, ix, iy, iz);
+    if (ix >= L.nx || iy >= L.ny || iz >= L.nz) {           // past the plate's edge
+        flag[c] = 0;
+        return;
+    }
     const double x = L.x0 + ((double)ix + 0.5) * L.cx, y = L.y0 + ((double)iy + 0.5) * L.cy;
     const double z = L.z0 + ((double)iz + 0.5) * L.cz;
     unsigned char sep = 1;
@@ -255,18 +408,16 @@ struct GridSum {
     double kn_total;
 };
 
-// Detector-only terms of point p for detector d (double, rounded once): p in d's frame, the
-// absorption chord of the extended ray p -> d's centre in d, and the attenuation sums Lpe, Lc
-// of everything on the way (crystals other than d and the scattering crystal, and for septal
-// points the tungsten and hole media).  Returns false when the point does not scatter into d.
-__device__ bool point_terms(const DevGeom& g, const GridGeom& G, const GridSum& S, int d, long long pidx, float* out)
+// Scatter point pidx: its position; k = its crystal (crystal cells) or -1, m = its layer (septal
+// cells) or -1; conv = mu_C / mu_pe of its crystal (a crystal cell's weight is photoelectric).
+__device__ void grid_point(const DevGeom& g, const GridGeom& G, const GridSum& S, long long pidx, double p[3], int& k,
+                           int& m, double& conv)
 {
-    double p[3];
-    int k = -1, m = -1;
-    double conv = 1.0;
+    k = -1;
+    m = -1;
+    conv = 1.0;
     if (pidx < S.n_cry_pts) {
         k = (int)(pidx / S.n_sub);
-        if (k == d) return false;
         const int sidx = (int)(pidx - (long long)k * S.n_sub);
         const int nxy = S.snx * S.sny;
         const int iz = sidx / nxy, rem = sidx - iz * nxy, iy = rem / S.snx, ix = rem - iy * S.snx;
@@ -282,6 +433,17 @@ __device__ bool point_terms(const DevGeom& g, const GridGeom& G, const GridSum& 
     } else {
         septal_point(G, pidx - S.n_cry_pts, m, p);
     }
+}
+
+// Detector-only terms of point p for detector d (double, rounded once): p in d's frame, the
+// absorption chord of the extended ray p -> d's centre in d, and the attenuation sums Lpe, Lc
+// of everything on the way (crystals other than d and the scattering crystal, and for septal
+// points the tungsten and hole media), over the chunk's candidate crystals and holes C.
+// Returns false when the point does not scatter into d.
+__device__ bool point_terms(const DevGeom& g, const GridGeom& G, int d, const double p[3], int k, int m, double conv,
+                            const Cands& C, float* out)
+{
+    if (k == d) return false;
     const D4 Pd = g.t64.cry_pos[d], Zd = g.t64.cry_size[d], Td = g.t64.cry_trig[d];
     const double D3[3] = {Pd.x, Pd.y, Pd.z};                  // centre of the 1 x 1 x 1 division
     const double ex = p[0] - Pd.x, ez = p[2] - Pd.z;
@@ -296,7 +458,9 @@ __device__ bool point_terms(const DevGeom& g, const GridGeom& G, const GridSum& 
     const float fx = (float)p[0], fy = (float)p[1], fz = (float)p[2];
     const float gx = (float)D3[0] - fx, gy = (float)D3[1] - fy, gz = (float)D3[2] - fz;
     const float gl2 = gx * gx + gy * gy + gz * gz;
-    for (int a = 0; a < g.n_det; ++a) {
+    const int n_cry = C.n_cry >= 0 ? C.n_cry : g.n_det;
+    for (int q = 0; q < n_cry; ++q) {
+        const int a = C.n_cry >= 0 ? C.cry[q] : q;
         if (a == d || a == k) continue;
         const float4 pa = __ldg(&g.cry.pos[a]);
         const float ra = 0.5f * __ldg(&g.cry.size[a].w) + 1e-3f;
@@ -329,7 +493,7 @@ __device__ bool point_terms(const DevGeom& g, const GridGeom& G, const GridSum& 
     }
     if (m >= 0) {                                             // tungsten and hole media on the way
         double wt = 0.0;
-        for (int mm = 0; mm < G.n_layers; ++mm) layer_path64(g, G, mm, p, D3, wt, lpe, lc);
+        for (int mm = 0; mm < G.n_layers; ++mm) layer_path64(g, G, mm, p, D3, wt, lpe, lc, &C);
     }
     out[0] = (float)ps[0];
     out[1] = (float)ps[1];
@@ -359,6 +523,7 @@ __device__ __forceinline__ float cone_cos(float ax, float ay, float az, float la
 constexpr int kTerms = 8;
 
 struct GridSmem {
+    Cands cand;                                 // the chunk's candidates for the current detector
     double acc[kGridDetTile][kGridMaxVox];      // block sums per (detector, voxel)
     float wt[kGridMaxVox][kGridChunk];          // the chunk's weights
     float terms[kTerms][kGridChunk];            // the chunk's detector-only terms
@@ -385,6 +550,12 @@ __global__ void __launch_bounds__(kGridThreads) grid_sum_kernel(DevGeom g, GridG
         if (p0 >= S.n_pts) break;
         const long long pidx = p0 + t;
         __syncthreads();
+        double pt[3] = {0.0, 0.0, 0.0}, conv = 1.0;
+        int kc = -1, mc = -1;
+        const bool has = pidx < S.n_pts;
+        if (has) grid_point(g, G, S, pidx, pt, kc, mc, conv);
+        block_bounds(sm.cand, has, pt);
+        const bool any_sep = __syncthreads_or(has && mc >= 0);
         for (int vi = 0; vi < S.nv; ++vi) {                     // stage the chunk's weights
             float w = 0.0f;
             if (pidx < S.n_cry_pts) w = S.wc[(long long)vi * S.n_cry_pts + pidx];
@@ -396,8 +567,11 @@ __global__ void __launch_bounds__(kGridThreads) grid_sum_kernel(DevGeom g, GridG
             const float4 P = __ldg(&g.cry.pos[d]), T = __ldg(&g.cry.trig[d]), M = __ldg(&g.cry.mu[d]);
             const float4 Z = __ldg(&g.cry.size[d]);
             __syncthreads();                                    // previous detector's terms are consumed
+            const D4 Pd = g.t64.cry_pos[d];
+            const double E3[3] = {Pd.x, Pd.y, Pd.z};
+            chunk_candidates(g, G, sm.cand, E3, true, any_sep);
             float tv[kTerms];
-            const bool ok = pidx < S.n_pts && point_terms(g, G, S, d, pidx, tv);
+            const bool ok = has && point_terms(g, G, d, pt, kc, mc, conv, sm.cand, tv);
             if (!ok) tv[7] = 0.0f;                              // zero weight factor: no contribution
 #pragma unroll
             for (int q = 0; q < kTerms; ++q) terms[q][t] = ok ? tv[q] : (q == 3 ? 1.0f : 0.0f);
@@ -541,15 +715,19 @@ extern "C" SYSMAT_API int sysmat_scatter_grid(sysmat_ctx* ctx, int parts, float 
             L.ny = grid_division((float)(Ly[3] - Ly[2]), cell);
             L.nz = grid_division((float)(Ly[5] - Ly[4]), cell);
             L.cx = (Ly[1] - Ly[0]) / L.nx; L.cy = (Ly[3] - Ly[2]) / L.ny; L.cz = (Ly[5] - Ly[4]) / L.nz;
+            L.nbx = (L.nx + kBrickX - 1) / kBrickX;
+            L.nby = (L.ny + kBrickY - 1) / kBrickY;
+            L.nbz = (L.nz + kBrickZ - 1) / kBrickZ;
             L.hole_begin = g.layer[m].hole_begin;
             L.hole_count = g.layer[m].hole_count;
             L.mu_t = g.layer[m].mu_total; L.mu_pe = g.layer[m].mu_pe; L.mu_c = g.layer[m].mu_c;
-            const long long nc = (long long)L.nx * L.ny * L.nz;
+            const long long nc = (long long)L.nbx * L.nby * L.nbz * kBrickCells;   // brick-padded
             if (nc > (1ll << 30)) return SYSMAT_ERR_CAPACITY;
             cells_max = nc > cells_max ? nc : cells_max;
         }
         long long total_cells = 0;
-        for (int m = 0; m < g.n_layers; ++m) total_cells += (long long)G.layer[m].nx * G.layer[m].ny * G.layer[m].nz;
+        for (int m = 0; m < g.n_layers; ++m)
+            total_cells += (long long)G.layer[m].nbx * G.layer[m].nby * G.layer[m].nbz * kBrickCells;
         size_t temp = 0;
         cub::DeviceSelect::Flagged(nullptr, temp, thrust::counting_iterator<int>(0), (unsigned char*)nullptr,
                                    (int*)nullptr, (int*)nullptr, (int)cells_max, s);
@@ -561,8 +739,8 @@ extern "C" SYSMAT_API int sysmat_scatter_grid(sysmat_ctx* ctx, int parts, float 
         int* sep = (int*)sep_mem.p;
         for (int m = 0; m < g.n_layers; ++m) {
             const GridLayer& L = G.layer[m];
-            const int nc = L.nx * L.ny * L.nz;
-            septal_mark_kernel<<<(nc + 255) / 256, 256, 0, s>>>(g, L, (unsigned char*)flags.p);
+            const int nc = L.nbx * L.nby * L.nbz * kBrickCells;
+            septal_mark_kernel<<<(nc + 255) / 256, 256, 0, s>>>(g, L, nc, (unsigned char*)flags.p);
             size_t t2 = temp;
             cub::DeviceSelect::Flagged(tmp.p, t2, thrust::counting_iterator<int>(0), (unsigned char*)flags.p,
                                        sep + n_sep, (int*)cnt.p, nc, s);
@@ -645,9 +823,8 @@ extern "C" SYSMAT_API int sysmat_scatter_grid(sysmat_ctx* ctx, int parts, float 
             if (st & kStatusCapacity) return SYSMAT_ERR_CAPACITY;
         }
         if (n_sep) {                                              // septal-cell weights
-            const long long n = (long long)nv * n_sep;
-            septal_weight_kernel<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(g, G, vb, nv, rotation, n_sep,
-                                                                              (float*)ws.p);
+            const dim3 sgrid((unsigned)((n_sep + kGridThreads - 1) / kGridThreads), (unsigned)nv);
+            septal_weight_kernel<<<sgrid, kGridThreads, 0, s>>>(g, G, vb, rotation, n_sep, (float*)ws.p);
             if (cudaGetLastError() != cudaSuccess) return SYSMAT_ERR_CUDA;
         }
         S.vox_begin = vb;

@@ -315,6 +315,17 @@ def apply_theta(geo: Geometry, theta) -> Geometry:
                     dict(geo.meta, theta=tuple(float(t) for t in theta)))
 
 
+def apply_theta_shapes(shapes, theta) -> np.ndarray:
+    """Elliptical hole shapes (n_holes, 3) rows (rho_x, rho_z, theta_h) at parameters theta:
+    the tilt turns every elliptical hole's frame with the hole pattern (theta_h + tilt,
+    computed in double and rounded to float once); circular rows (rho_x <= 0) are kept."""
+    out = np.array(shapes, dtype=np.float32).reshape(-1, 3).copy()
+    tilt = float(theta[6])
+    ell = out[:, 0] > 0
+    out[ell, 2] = (out[ell, 2].astype(np.float64) + tilt).astype(np.float32)
+    return out
+
+
 def theta_of(geo: Geometry) -> np.ndarray:
     """Nominal theta of a system built here (layer 0 mu, crystal 0 mu, hole 0 radius, no
     shift or tilt)."""

@@ -30,9 +30,18 @@ CRY_HIT_FLOPS, CRY_HIT_MUFU = 45, 4
 SUB_FLOPS, SUB_MUFU = 104, 9
 
 # DRAM traffic of one pe_kernel launch, from one ncu capture (dram__bytes_read.sum +
-# dram__bytes_write.sum) of a configuration-2 launch whose output block exceeds L2, so the
-# matrix writes reach DRAM inside the captured launch.  None until such a capture exists.
-PE_DRAM_CAPTURE = None
+# dram__bytes_write.sum, --clock-control none) of the reference-mode kernel on crystals
+# 0..255 x z-plane 16 of configuration 2 (2359296 elements, 548.6 ms): 3779840 B read +
+# 226816 B written.  The block's output (9.4 MB) stays in L2 during the launch, so the figure
+# is the tables' and output lines' first touches, not the output's write-back.
+PE_DRAM_CAPTURE = {
+    "bytes": 3779840 + 226816,
+    "elements": 2359296,
+    "command": "ncu --metrics dram__bytes_read.sum,dram__bytes_write.sum,gpu__time_duration.sum "
+               "--clock-control none -k regex:pe_kernel -s 3 -c 1 python bench.py --steps 1 --warmup 3 "
+               "--det-count 256 --no-e2e --no-scatter --no-scatter2 --no-grid --no-batch --no-sampled --no-fp64 "
+               "--no-local --no-cpu-baseline",
+}
 
 
 def pe_work(counts: dict, n_layers: int) -> tuple[float, float]:

@@ -222,8 +222,8 @@ SYSMAT_API int sysmat_scatter(sysmat_ctx* ctx, int parts, int hole_model, float 
  * the reference's chord; rho_x[h] <= 0 keeps it circular.  The hole's radius field in
  * Params_Collimator must bound both semi-axes (the reference cone test and the kernel's
  * filters use it).  rho_x = NULL restores circular holes.  Applies to sysmat_pe (and the
- * entry points built on it) and to batch plans created afterwards; the adjoint entry points
- * reject such contexts. */
+ * entry points built on it), to the projection entry points and their vector-Jacobian
+ * product, and to batch plans created afterwards. */
 SYSMAT_API int sysmat_set_hole_shapes(sysmat_ctx* ctx, const float* rho_x, const float* rho_z, const float* theta);
 
 /* Whole photoelectric matrix of rotation `rotation` written to `path` in compressed form
@@ -286,9 +286,12 @@ SYSMAT_API int sysmat_batch(sysmat_ctx* const* ctxs, int n_ctx, const sysmat_bat
  *   4 dy          shift of every hole's caps and every layer plane along y
  *   5 dz          shift of every hole centre along z
  *   6 tilt        rotation of the hole pattern about the y axis, radians
- *                 (x' = x cos t - z sin t, z' = x sin t + z cos t)
+ *                 (x' = x cos t - z sin t, z' = x sin t + z cos t); it turns the frame of an
+ *                 elliptical hole with the pattern (theta[h] + t)
  * Thresholds of the reference's program (plate penalty, eps cut-offs) are piecewise constant
- * and contribute nothing to the derivative. */
+ * and contribute nothing to the derivative.  An elliptical hole's chord does not read the
+ * radius field (which only bounds the ellipse), so such holes add nothing to the radius
+ * partial. */
 #define SYSMAT_THETA_N 7
 
 /* d_p[i] = sum_v A[det_begin + i, v] * d_x[v] in double (precise-mode elements).

@@ -103,6 +103,13 @@ def cases():
     out.append(("config2_strip", geometry.voxel_slab(geometry.config2(), 16, 47, 2), ()))
     out.append(("config3_z8", geometry.voxel_slab(geometry.config3(), 8),
                 ("combined", "collimator")))
+    # configuration 4 (design sweep): two instances at one of their rotations, voxel row 16 of
+    # z-plane 8 x all crystals; configuration 5 (calibration system at nominal theta): voxel
+    # row 32 of z-plane 8 x all crystals
+    g4 = geometry.config4()
+    for k, r in ((7, 5), (40, 11)):
+        out.append((f"config4_i{k}r{r}", geometry.voxel_slab(g4[k].with_rotation(r), 8, 16, 1), ()))
+    out.append(("config5_z8", geometry.voxel_slab(geometry.config5()[0], 8, 32, 1), ()))
     return out
 
 

@@ -34,15 +34,33 @@ def _dense(torch, ctx, rotation=0.0):
     return out.cpu().numpy().astype(np.float64)
 
 
-@pytest.mark.parametrize("case", ["mini_rot", "config1"])
+def _ellipses(geo, every=2):
+    """Every `every`-th hole elliptical (semi-axes 0.8 and 0.55 of its radius, seeded frame
+    angles in [0.3, 3.5) rad); the others circular."""
+    r = geo.collimator[104:104 + 9 * geo.n_holes:9]
+    sh = np.zeros((geo.n_holes, 3), dtype=np.float32)
+    k = np.arange(geo.n_holes)
+    e = k % every == 0
+    sh[e, 0] = 0.8 * r[e]
+    sh[e, 1] = 0.55 * r[e]
+    sh[e, 2] = (0.3 + (0.37 * k[e]) % 3.2).astype(np.float32)
+    return sh
+
+
+@pytest.mark.parametrize("case", ["mini_rot", "config1", "mini_ell"])
 def test_products_equal_dense_matrix_products(gpu, case):
     torch = gpu
     if case == "mini_rot":
         geo = geometry.mini(seed=31, rotated=True, layers=2, n_rot=8, nvox=(6, 5, 3), ncry=(5, 4))
         rot = 3.0
+    elif case == "mini_ell":
+        geo = geometry.mini(seed=31, rotated=True, layers=2, n_rot=8, nvox=(6, 5, 3), ncry=(5, 4))
+        rot = 5.0
     else:
         geo, rot = geometry.config1(), 0.0
     ctx = sysmat.Context(geo)
+    if case == "mini_ell":
+        ctx.set_hole_shapes(_ellipses(geo))
     A = _dense(torch, ctx, rot)
     rng = np.random.default_rng(7)
     x = rng.uniform(0.0, 2.0, ctx.n_vox).astype(np.float32)
@@ -94,6 +112,52 @@ def test_vjp_matches_fp64_oracle_gradient(gpu):
             d.append((s_of(geometry.Geometry(geo.name, cp, geo.detector, geo.image, geo.physics)) -
                       s_of(geometry.Geometry(geo.name, cm, geo.detector, geo.image, geo.physics))) / (2 * h))
         tilt += -float(geo.collimator[103 + 9 * k]) * d[0] + float(geo.collimator[100 + 9 * k]) * d[1]
+    assert abs(g[6] - tilt) <= 1e-3 * abs(tilt), (g[6], tilt)
+
+
+def test_vjp_with_elliptical_holes_matches_fp64_oracle_gradient(gpu):
+    """Elliptical holes: the VJP against central differences of the FP64 oracle with the same
+    shapes; the tilt against the identity sum_h (-z_h d/dx_h + x_h d/dz_h) plus the frame
+    angle d/dtheta_h of every elliptical hole (the tilt turns their frames)."""
+    torch = gpu
+    geo = geometry.mini(seed=41, layers=2, nvox=(6, 5, 2), ncry=(4, 4), nholes=3)
+    shapes = _ellipses(geo)
+    rng = np.random.default_rng(1)
+    x = rng.uniform(0.5, 2.0, geo.n_vox).astype(np.float32)
+    u = rng.normal(size=geo.n_det).astype(np.float32)
+    x64, u64 = x.astype(np.float64), u.astype(np.float64)
+    P = adjoint.Projector(geo, shapes=shapes)
+    t0 = geometry.theta_of(geo)
+    g = P.vjp(torch.from_numpy(x).cuda(), torch.from_numpy(u).cuda(), t0).cpu().numpy()
+
+    def s_of(gg, sh=shapes):
+        return float(u64 @ oracle.pe(gg, prec=64, shapes=sh) @ x64)
+
+    assert abs(g[sysmat.THETA_N] - s_of(geo)) <= 1e-6 * abs(s_of(geo))
+    h = 2.0 ** -20
+    for i in range(6):                                   # mu_W .. dz
+        tp, tm = t0.copy(), t0.copy()
+        tp[i] += h
+        tm[i] -= h
+        fd = (s_of(geometry.apply_theta(geo, tp)) - s_of(geometry.apply_theta(geo, tm))) / (2 * h)
+        if i == 2:                                       # circular holes only move with the radius
+            assert abs(g[i] - fd) <= 1e-3 * abs(fd) + 1e-9 * abs(s_of(geo)), (g[i], fd)
+        else:
+            assert abs(g[i] - fd) <= 1e-3 * abs(fd), (sysmat.THETA_NAMES[i], g[i], fd)
+    tilt = 0.0
+    for k in range(geo.n_holes):
+        for col, wgt in ((100 + 9 * k, -float(geo.collimator[103 + 9 * k])),
+                         (103 + 9 * k, float(geo.collimator[100 + 9 * k]))):
+            cp, cm = geo.collimator.copy(), geo.collimator.copy()
+            cp[col] += np.float32(h)
+            cm[col] -= np.float32(h)
+            tilt += wgt * (s_of(geometry.Geometry(geo.name, cp, geo.detector, geo.image, geo.physics)) -
+                           s_of(geometry.Geometry(geo.name, cm, geo.detector, geo.image, geo.physics))) / (2 * h)
+        if shapes[k, 0] > 0:                             # the frame turns with the pattern
+            sp, sm = shapes.copy(), shapes.copy()
+            sp[k, 2] += np.float32(h)
+            sm[k, 2] -= np.float32(h)
+            tilt += (s_of(geo, sp) - s_of(geo, sm)) / (2 * h)
     assert abs(g[6] - tilt) <= 1e-3 * abs(tilt), (g[6], tilt)
 
 
