@@ -371,7 +371,10 @@ __device__ __forceinline__ bool in_capsule(const float4& c, float rho2, float in
 // the round buffer from position n, with their geometry (one entry per lane); returns the
 // new count.  Stops before the buffer could overflow; *next receives the first entry not
 // examined.  IDS: store each entry's object id (as the bits of ra.x) instead of its float
-// geometry, for walks that read their own geometry tables (FP64 mode).
+// geometry, for walks that read their own geometry tables (FP64 mode), and a hole entry's
+// capsule in place of its rectangle for the lanes' test (hole_in_reach).  The float walks
+// test the rectangle: the warp runs an entry's chord whenever any lane needs it, and the
+// tighter lane test measured slower there (its cost without fewer warp-level evaluations).
 template <bool ELL, bool IDS = false>
 __device__ __forceinline__ int fill_round(const DevGeom& g, WarpSmem& ws, const Elem& e, int k0, int k1,
                                           float4 box, int n, int lane, int* next, int* nh)
@@ -420,9 +423,9 @@ __device__ __forceinline__ int fill_round(const DevGeom& g, WarpSmem& ws, const 
             } else if (id < g.n_holes) {
                 const float4 ha = __ldg(&g.hole.a[id]);
                 const float4 hb = __ldg(&g.hole.b[id]);
-                ws.rr[pos] = cap;
+                ws.rr[pos] = rect;
                 ws.ra[pos] = make_float4(ha.x, ha.w, hb.x, hb.y);
-                ws.rb[pos] = make_float4(ha.y, ha.z, rho2, inv_len2);
+                ws.rb[pos] = make_float4(ha.y, ha.z, 0.0f, 0.0f);
                 if constexpr (ELL) {        // rho_x, rho_z, cos, sin; a batch may mix in circular systems
                     ws.rc[pos] = g.hole_shape ? __ldg(&g.hole_shape[id]) : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
                 }
@@ -449,7 +452,7 @@ __device__ __forceinline__ int fill_round(const DevGeom& g, WarpSmem& ws, const 
     return n;
 }
 
-// Lane test of round-buffer hole entry j (see in_capsule).
+// Lane test of round-buffer hole entry j of a fill_round<…, IDS> buffer (see in_capsule).
 __device__ __forceinline__ bool hole_in_reach(const WarpSmem& ws, int j, float sa, float sb)
 {
     const float4 b = ws.rb[j];
@@ -467,7 +470,7 @@ __device__ __forceinline__ void walk_round(const DevGeom& g, const WarpSmem& ws,
     for (int j = 0; j < nh; ++j) {
         const int m = ws.rl[j];
         if (m != s.lay) close_layers(g, s, m, cosang);
-        if (!hole_in_reach(ws, j, sa_a, sa_b)) continue;
+        if (!in_rect(ws.rr[j], sa_a, sa_b)) continue;
         const float4 A = ws.ra[j];
         const float4 B = ws.rb[j];
         float tmp;

@@ -147,7 +147,7 @@ __device__ __forceinline__ void walk_round_grad(const DevGeom& g, const WarpSmem
     for (int j = 0; j < nh; ++j) {
         const int m = ws.rl[j];
         if (m != s.lay) close_layers_grad(g, s, m, cosang);
-        if (!hole_in_reach(ws, j, sa_a, sa_b)) continue;
+        if (!in_rect(ws.rr[j], sa_a, sa_b)) continue;
         const float4 A = ws.ra[j];               // x, z, R, mu of the hole
         const float4 B = ws.rb[j];
         CylGrad gr;

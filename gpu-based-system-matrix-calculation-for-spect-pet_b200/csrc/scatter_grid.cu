@@ -513,13 +513,6 @@ __device__ __forceinline__ double kn_integral(const double* __restrict__ tab, do
     return G;
 }
 
-__device__ __forceinline__ float cone_cos(float ax, float ay, float az, float la, float bx, float by, float bz)
-{
-    const float lb = sqrtf(bx * bx + by * by + bz * bz);
-    float c = (ax * bx + ay * by + az * bz) / (la * lb);
-    return fminf(fmaxf(c, -1.0f), 1.0f);
-}
-
 constexpr int kTerms = 8;
 
 struct GridSmem {
@@ -527,6 +520,7 @@ struct GridSmem {
     double acc[kGridDetTile][kGridMaxVox];      // block sums per (detector, voxel)
     float wt[kGridMaxVox][kGridChunk];          // the chunk's weights
     float terms[kTerms][kGridChunk];            // the chunk's detector-only terms
+    float rlb[9][kGridChunk];                   // 1 / |corner c of d - p| (c < 8), 1 / |p - d|
     float4 vox_s[kGridMaxVox];                  // voxels in the current detector's frame
 };
 
@@ -575,6 +569,17 @@ __global__ void __launch_bounds__(kGridThreads) grid_sum_kernel(DevGeom g, GridG
             if (!ok) tv[7] = 0.0f;                              // zero weight factor: no contribution
 #pragma unroll
             for (int q = 0; q < kTerms; ++q) terms[q][t] = ok ? tv[q] : (q == 3 ? 1.0f : 0.0f);
+            {                                                   // point -> corner distances of d
+                const float hw = 0.5f * Z.x, ht = 0.5f * Z.y, hh = 0.5f * Z.z;
+                const float px = ok ? tv[0] : 0.0f, py = ok ? tv[1] : 0.0f, pz = ok ? tv[2] : 0.0f;
+#pragma unroll
+                for (int c = 0; c < 8; ++c) {
+                    const float bx = ((c & 1) ? hw : -hw) - px, by = ((c & 2) ? ht : -ht) - py;
+                    const float bz = ((c & 4) ? hh : -hh) - pz;
+                    sm.rlb[c][t] = 1.0f / sqrtf(bx * bx + by * by + bz * bz);
+                }
+                sm.rlb[8][t] = ok ? 1.0f / tv[3] : 0.0f;
+            }
             if (t < S.nv) {
                 float x, y, z, xs, ys, zs;
                 voxel_centre(g, S.vox_begin + t, crot, srot, x, y, z);
@@ -596,7 +601,9 @@ __global__ void __launch_bounds__(kGridThreads) grid_sum_kernel(DevGeom g, GridG
                     const float px = terms[0][j], py = terms[1][j], pz = terms[2][j], lsd = terms[3][j];
                     const float ax = px - I.x, ay = py - I.y, az = pz - I.z;      // v -> p
                     const float la = sqrtf(ax * ax + ay * ay + az * az);
-                    const float cc = cone_cos(ax, ay, az, la, -px, -py, -pz);     // angle v -> p -> d
+                    const float rla = 1.0f / la;
+                    // angle v -> p -> d (cosines as dot products times reciprocal lengths)
+                    const float cc = fminf(fmaxf(-(ax * px + ay * py + az * pz) * rla * sm.rlb[8][j], -1.0f), 1.0f);
                     const float es = e0 / (1.0f + (e0 / 511.0f) * (1.0f - cc));
                     const float res = M.w * sqrtf(es / e0);
                     if ((es * (1 + 2 * res / 2.35482f)) <= lo || (es * (1 - 2 * res / 2.35482f)) >= hi) continue;
@@ -606,17 +613,18 @@ __global__ void __launch_bounds__(kGridThreads) grid_sum_kernel(DevGeom g, GridG
                     if (lsd * sc * 2.0f <= rdet) phi = (float)(2.0 * 3.14159265358979323846);
                     else phi = 4.0f * asinf(fminf(rdet / 2.0f / lsd / sc, 1.0f));
                     // polar range over the corners of d, seen from p along v -> p (:1305-1335)
-                    float cmin = 2.0f, cmax = -2.0f;
+                    float cmin = INFINITY, cmax = -INFINITY;
 #pragma unroll
                     for (int c = 0; c < 8; ++c) {
-                        const float ck = cone_cos(ax, ay, az, la, ((c & 1) ? hw : -hw) - px,
-                                                  ((c & 2) ? ht : -ht) - py, ((c & 4) ? hh : -hh) - pz);
+                        const float ck = (ax * (((c & 1) ? hw : -hw) - px) + ay * (((c & 2) ? ht : -ht) - py) +
+                                          az * (((c & 4) ? hh : -hh) - pz)) * sm.rlb[c][j];
                         cmin = fminf(cmin, ck);
                         cmax = fmaxf(cmax, ck);
                     }
-                    float tmin = acosf(cmax), tmax = acosf(cmin);
-                    const float lthr = box_chord(I.x, I.y, I.z, px + 1000.0f * ax / la, py + 1000.0f * ay / la,
-                                                 pz + 1000.0f * az / la, -hw, -ht, -hh, hw, ht, hh);
+                    float tmin = acosf(fminf(fmaxf(cmax * rla, -1.0f), 1.0f));
+                    const float tmax = acosf(fminf(fmaxf(cmin * rla, -1.0f), 1.0f));
+                    const float lthr = box_chord(I.x, I.y, I.z, px + 1000.0f * ax * rla, py + 1000.0f * ay * rla,
+                                                 pz + 1000.0f * az * rla, -hw, -ht, -hh, hw, ht, hh);
                     if (lthr > 0.001f) tmin = 0.0f;
                     const double ratio = (kn_integral(S.kn_tab, (double)tmax) - kn_integral(S.kn_tab, (double)tmin)) /
                                          S.kn_total;

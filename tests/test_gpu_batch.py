@@ -6,7 +6,7 @@ brick shapes, graph replays and the autotuner."""
 import numpy as np
 import pytest
 
-from conftest import geometry, sysmat
+from conftest import TOL, geometry, golden, rel_err, sysmat
 
 pytestmark = pytest.mark.gpu
 
@@ -105,6 +105,25 @@ def test_config4_instances_sample(gpu):
     torch.cuda.synchronize()
     _check(outs, exp, tasks)
     assert all(e.max() > 0 for e in exp)
+
+
+def test_batch_matches_reference_on_config4_goldens(gpu):
+    """Two configuration-4 designs at one of their rotations (the reference's own PESysMatGen
+    output on voxel row 16 of z-plane 8), computed together in one batch."""
+    torch = gpu
+    pairs = [golden(n) for n in ("config4_i7r5", "config4_i40r11")]
+    ctxs = [sysmat.Context(geo) for geo, _ in pairs]
+    outs = [torch.empty((c.n_det, c.n_vox), dtype=torch.float32, device="cuda") for c in ctxs]
+    items = [(k, float(geo.image[20]), 0, ctxs[k].n_det, 0, ctxs[k].n_vox, outs[k])
+             for k, (geo, _) in enumerate(pairs)]
+    plan = sysmat.BatchPlan(ctxs, items)
+    plan.run()
+    torch.cuda.synchronize()
+    for o, (geo, z) in zip(outs, pairs):
+        a = o.cpu().numpy()[z["rows"]]
+        r = rel_err(a, z["pe"])
+        assert a.max() > 0 and r.max() <= TOL, (geo.name, r.max())
+        assert np.mean(a == z["pe"]) > 0.5
 
 
 def test_invalid_batches_raise(gpu):

@@ -78,7 +78,7 @@ def test_all_circular_shape_table_is_bit_identical(gpu):
     assert np.array_equal(_pe(gpu, ctx, 1.0), plain)
 
 
-def test_invalid_shapes_and_the_adjoint_raise(gpu):
+def test_invalid_shapes_raise_and_the_projection_takes_valid_ones(gpu):
     geo, shapes = _system_and_shapes(54)
     ctx = sysmat.Context(geo)
     bad = shapes.copy()
@@ -91,8 +91,11 @@ def test_invalid_shapes_and_the_adjoint_raise(gpu):
         ctx.set_hole_shapes(bad)
     ctx.set_hole_shapes(shapes)
     x = gpu.ones(ctx.n_vox, dtype=gpu.float32, device="cuda")
-    with pytest.raises(sysmat.SysmatError):
-        ctx.project(x)
+    p = ctx.project(x).cpu().numpy()
+    out = gpu.empty((ctx.n_det, ctx.n_vox), dtype=gpu.float32, device="cuda")
+    ctx.pe(out, mode=sysmat.MODE_PRECISE)
+    dense = out.cpu().numpy().astype(np.float64).sum(axis=1)
+    assert np.abs(p - dense).max() <= 1e-6 * np.abs(dense).max()
 
 
 def test_batched_launch_with_elliptical_holes_equals_single_calls(gpu):

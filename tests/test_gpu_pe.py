@@ -10,7 +10,8 @@ from conftest import TOL, geometry, golden, oracle, rel_err, sysmat
 
 pytestmark = pytest.mark.gpu
 
-GOLDENS = ["mini0", "mini1r2", "mini2w", "config1", "config2_strip", "config3_z8"]
+GOLDENS = ["mini0", "mini1r2", "mini2w", "config1", "config2_strip", "config3_z8", "config4_i7r5",
+           "config4_i40r11", "config5_z8"]
 
 
 def pe_matrix(torch, geo, mode=sysmat.MODE_REFERENCE, ctx=None):

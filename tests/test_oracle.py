@@ -146,7 +146,8 @@ def test_kn_normalisation_known_value():
 
 PE_CASES = [("mini0", None), ("mini1r2", None), ("mini2w", None),
             ("config1", slice(0, 256, 37)), ("config2_strip", slice(0, 2)),
-            ("config3_z8", slice(0, 2))]
+            ("config3_z8", slice(0, 2)), ("config4_i7r5", slice(0, 1024, 61)),
+            ("config4_i40r11", slice(0, 1024, 67)), ("config5_z8", slice(0, 2304, 97))]
 
 
 @pytest.mark.parametrize("name,rows", PE_CASES)
