@@ -60,6 +60,27 @@ def rel_err(a, b, scale=None):
 TOL = 1e-5
 
 
+def check_pe_vs_reference(a, geo, z):
+    """Photoelectric elements `a` (the golden's rows) against the reference's own output z["pe"]:
+    most elements bit-identical (the same float program), every element within 1e-5, except
+    heavily attenuated ones of thick-plate systems, where the float program's own rounding
+    (attenuation sums of ~10-20) reaches ~1e-5 and another contraction order lands elsewhere:
+    those must be few and no further from the FP64 oracle than twice the reference's own worst
+    error on the same elements."""
+    ref = z["pe"]
+    r = rel_err(a, ref)
+    assert a.max() > 0
+    assert np.mean(a == ref) > 0.5, np.mean(a == ref)
+    out = r > TOL
+    if out.any():
+        o64 = oracle.pe(geo, prec=64, dets=z["rows"])
+        bound = 2.0 * rel_err(ref, o64).max()
+        assert np.mean(out) < 5e-3, np.mean(out)
+        assert rel_err(a, o64)[out].max() <= bound, (rel_err(a, o64)[out].max(), bound)
+        assert np.all(np.abs(ref[out]) < 3e-3 * np.abs(ref).max())
+    return r
+
+
 @pytest.fixture(scope="session")
 def gpu():
     """A CUDA device; GPU tests fail loudly (not skip) when it or the library is missing."""
