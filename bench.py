@@ -22,7 +22,8 @@ the reference-compatible scatter() with host buffers and bitmap files), `scatter
 the same on a configuration-2 voxel row, `scatter_grid` = configuration 3 as stated (scatter
 points on a 0.25 mm grid inside the crystals and the tungsten, FP64 sums), `batch` = the configuration-4 design sweep in one
 batched launch against one launch per task, `sampled` = configuration 2 with the sampling it
-states (2x2x2 voxel sub-samples, 2x8x2 crystal sub-elements), `fp64` = the FP64 mode (the
+states (2x2x2 voxel sub-samples, 2x8x2 crystal sub-elements), in the reference's float
+program and (`sampled.local`) in the local-coordinate FP32 form, `fp64` = the FP64 mode (the
 element program in double) on the headline plane, `local` = the local-coordinate FP32 mode
 (within 1e-5 of FP64) on the same plane.
 
@@ -572,19 +573,24 @@ def run_sampled(args, sysmat, torch, keep, rows=512):
     d0 = ctx.n_det // 2 - rows // 2
     out = torch.empty((rows, nxy), dtype=torch.float32, device="cuda")
 
-    def step():
-        ctx.pe_sampled(out, (2, 8, 2), (2, 2, 2), det_begin=d0, det_count=rows, vox_begin=16 * nxy, vox_count=nxy)
+    def step(mode):
+        ctx.pe_sampled(out, (2, 8, 2), (2, 2, 2), det_begin=d0, det_count=rows, vox_begin=16 * nxy, vox_count=nxy,
+                       mode=mode)
 
-    step()
-    ms = _events(torch, step, n=2)
     nx = int(g.image[0])
-    keep["sampled"] = {"d0": d0, "out": out[:, SAMPLE_ROW * nx:(SAMPLE_ROW + 1) * nx].cpu().numpy(),
-                       "max": float(out.max().item())}
+    res = {}
+    for key, mode in (("sampled", sysmat.MODE_PRECISE), ("sampled_local", sysmat.MODE_LOCAL)):
+        step(mode)
+        ms = _events(torch, lambda: step(mode), n=2)
+        keep[key] = {"d0": d0, "out": out[:, SAMPLE_ROW * nx:(SAMPLE_ROW + 1) * nx].cpu().numpy(),
+                     "max": float(out.max().item())}
+        res[key] = {"value": rows * nxy / (ms * 1e-3), "unit": UNIT, "ms_per_step": ms, "rays_per_element": 8 * 32,
+                    "arithmetic": "f32, FP64 sums" if key == "sampled" else "f32 (local), compensated sums",
+                    "workload": f"config2 as stated: 2x2x2 voxel sub-samples, 2x8x2 crystal sub-elements; crystals "
+                                f"{d0}..{d0 + rows - 1} x z-plane 16 ({rows * nxy} elements)"}
     ctx.close()
-    return {"value": rows * nxy / (ms * 1e-3), "unit": UNIT, "ms_per_step": ms, "rays_per_element": 8 * 32,
-            "summation": "FP64",
-            "workload": f"config2 as stated: 2x2x2 voxel sub-samples, 2x8x2 crystal sub-elements; crystals "
-                        f"{d0}..{d0 + rows - 1} x z-plane 16 ({rows * nxy} elements)"}
+    res["sampled"]["local"] = res.pop("sampled_local")
+    return res["sampled"]
 
 
 def run_fp64(args, sysmat, torch, keep):
@@ -777,6 +783,11 @@ def cpu_baseline(args, g, n_planes, keep):
                                  threads=threads)
         acc["sampled"] = dict(rel_err_stats(s["out"][sel - s["d0"]], os64, s["max"]), vs="FP64 oracle (sampled form)",
                               sample=f"crystals {sel.tolist()} x voxel row {SAMPLE_ROW} of z-plane 16")
+        if "sampled_local" in keep:
+            s = keep["sampled_local"]
+            acc["sampled_local"] = dict(rel_err_stats(s["out"][sel - s["d0"]], os64, s["max"]),
+                                        vs="FP64 oracle (sampled form)",
+                                        sample=f"crystals {sel.tolist()} x voxel row {SAMPLE_ROW} of z-plane 16")
     if "scatter" in keep:
         s = keep["scatter"]
         gs = s["geo"]

@@ -390,13 +390,16 @@ extern "C" SYSMAT_API int sysmat_pe(sysmat_ctx* ctx, float rotation, int det_beg
     return run_pe_block(ctx, L, s, [&](const PeLaunch& l) { return launch_pe(ctx->g, l, mode, ctx->num_sms, s); });
 }
 
-extern "C" SYSMAT_API int sysmat_pe_sampled(sysmat_ctx* ctx, float rotation, int det_begin, int det_count,
-                                            long long vox_begin, long long vox_count, const int* crystal_div,
-                                            const int* voxel_sub, float* d_out, long long ld, void* stream)
+extern "C" SYSMAT_API int sysmat_pe_sampled_mode(sysmat_ctx* ctx, float rotation, int det_begin, int det_count,
+                                                 long long vox_begin, long long vox_count, const int* crystal_div,
+                                                 const int* voxel_sub, int mode, float* d_out, long long ld,
+                                                 void* stream)
 {
     int rc = check_block(ctx, det_begin, det_count, vox_begin, vox_count, d_out, ld);
     if (rc) return rc;
     if (!crystal_div || !voxel_sub) return SYSMAT_ERR_ARG;
+    if (mode != SYSMAT_MODE_PRECISE && mode != SYSMAT_MODE_LOCAL) return SYSMAT_ERR_ARG;
+    if (mode == SYSMAT_MODE_LOCAL && ctx->g.hole_shape) return SYSMAT_ERR_ARG;     // circular holes only
     Sampling smp;
     smp.nx = crystal_div[0]; smp.ny = crystal_div[1]; smp.nz = crystal_div[2];
     smp.sx = voxel_sub[0]; smp.sy = voxel_sub[1]; smp.sz = voxel_sub[2];
@@ -411,7 +414,18 @@ extern "C" SYSMAT_API int sysmat_pe_sampled(sysmat_ctx* ctx, float rotation, int
     cudaStream_t s = (cudaStream_t)stream;
     PeLaunch L = pe_block(ctx, rotation, det_begin, det_count, vox_begin, vox_count, d_out, ld);
     L.smp = smp;
+    if (mode == SYSMAT_MODE_LOCAL)
+        return run_pe_block(ctx, L, s,
+                            [&](const PeLaunch& l) { return launch_pe_local_sampled(ctx->g, l, ctx->num_sms, s); });
     return run_pe_block(ctx, L, s, [&](const PeLaunch& l) { return launch_pe_sampled(ctx->g, l, ctx->num_sms, s); });
+}
+
+extern "C" SYSMAT_API int sysmat_pe_sampled(sysmat_ctx* ctx, float rotation, int det_begin, int det_count,
+                                            long long vox_begin, long long vox_count, const int* crystal_div,
+                                            const int* voxel_sub, float* d_out, long long ld, void* stream)
+{
+    return sysmat_pe_sampled_mode(ctx, rotation, det_begin, det_count, vox_begin, vox_count, crystal_div, voxel_sub,
+                                  SYSMAT_MODE_PRECISE, d_out, ld, stream);
 }
 
 extern "C" SYSMAT_API long long sysmat_bitmap_crystal_words(const sysmat_ctx* ctx)

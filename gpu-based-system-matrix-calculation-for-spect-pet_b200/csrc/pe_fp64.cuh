@@ -23,7 +23,10 @@ struct Elem64 {
     double ux, uy, uz, crit_self; // cone test (:1110-1116)
 };
 
-__device__ __forceinline__ void init_elem64(const DevGeom& g, int d, long long v, float rotation, Elem64& E)
+// Element constants for the source point at fractions (fx, fy, fz) of voxel v's extent (1/2:
+// the voxel centre, the reference's source).
+__device__ __forceinline__ void init_elem64(const DevGeom& g, int d, long long v, float rotation, Elem64& E,
+                                            double fx = 0.5, double fy = 0.5, double fz = 0.5)
 {
     const long long nxy = (long long)g.nx * g.ny;
     const int iz = (int)(v / nxy);
@@ -33,9 +36,9 @@ __device__ __forceinline__ void init_elem64(const DevGeom& g, int d, long long v
     const double ang = (double)rotation * (double)g.angle_step;   // :1006
     double sa, ca;
     sincos(ang, &sa, &ca);
-    double x = ((double)ix - (double)g.nx / 2.0 + 0.5) * (double)g.wx;
-    double y = ((double)iy - (double)g.ny / 2.0 + 0.5) * (double)g.wy;
-    const double z = ((double)iz - (double)g.nz / 2.0 + 0.5) * (double)g.wz + (double)g.shz;
+    double x = ((double)ix - (double)g.nx / 2.0 + fx) * (double)g.wx;
+    double y = ((double)iy - (double)g.ny / 2.0 + fy) * (double)g.wy;
+    const double z = ((double)iz - (double)g.nz / 2.0 + fz) * (double)g.wz + (double)g.shz;
     x = x + (double)g.shx;
     y = y + (double)g.shy;
     E.xI = x * ca - y * sa;

@@ -38,9 +38,9 @@ struct ElemL {
 };
 
 __device__ __forceinline__ void init_elem_local(const DevGeom& g, int d, long long v, float rotation, int nx, int ny,
-                                                int nz, ElemL& L)
+                                                int nz, ElemL& L, double fx = 0.5, double fy = 0.5, double fz = 0.5)
 {
-    init_elem64(g, d, v, rotation, L.e64);
+    init_elem64(g, d, v, rotation, L.e64, fx, fy, fz);
     L.nx = nx;
     L.ny = ny;
     L.nz = nz;
@@ -432,103 +432,113 @@ __device__ __forceinline__ void neumaier_add(float& s, float& c, float x)
     s = t;
 }
 
-// The element of the local form.  smp: the crystal division (voxel centre sources only); nullptr
-// = the reference's 8 x 16 x 8, whose rounds are the compact 2 z x 8 x x 2 depth patches of
-// the reference-order kernel; other divisions go 32 to a round in (z, depth, x) order, x
-// fastest.  sub_out: when set, each sub-element's contribution is also written there, at index
-// (iz * ny + iy) * nx + ix (the scatter grid's crystal-cell weights).
+// The element of the local form.  smp: the crystal division and the voxel's source points (the
+// element is the mean over the centres of an sx x sy x sz grid over the voxel, as in the
+// sampled form); nullptr = the reference's 8 x 16 x 8 division and the voxel centre.  The
+// reference division's rounds are the compact 2 z x 8 x x 2 depth patches of the
+// reference-order kernel; other divisions go 32 to a round in (z, depth, x) order, x fastest.
+// sub_out (one source point only): each sub-element's contribution is also written there, at
+// index (iz * ny + iy) * nx + ix (the scatter grid's crystal-cell weights).
 __device__ double pe_element_local(const DevGeom& g, const BlockSmem& bs, WarpSmem& ws, int d, long long v, float cr,
                                    float sr, float rotation, int lane, const Sampling* smp = nullptr,
                                    float* sub_out = nullptr)
 {
-    Elem e;
-    if (!init_element(g, ws, d, v, cr, sr, lane, e)) {              // mu_t <= 0.01 (:1107, :1194)
-        if (sub_out) {
-            const int n = smp ? smp->nx * smp->ny * smp->nz : 1024;
-            for (int i = lane; i < n; i += 32) sub_out[i] = 0.0f;
-        }
-        return 0.0;
-    }
     static_assert(sizeof(ElemL) <= sizeof(ws.chain), "ElemL exceeds its shared-memory slot");
     ElemL& L = *reinterpret_cast<ElemL*>(ws.chain);
     const int nx = smp ? smp->nx : 8, ny = smp ? smp->ny : 16, nz = smp ? smp->nz : 8;
     const int n_sub = nx * ny * nz, nxy = nx * ny;
-    if (lane == 0) init_elem_local(g, d, v, rotation, nx, ny, nz, L);
-    __syncwarp();
-    const bool from_super = bs.s_count >= 0;
-    const int n_src = from_super ? bs.s_count : g.n_holes + g.n_det;
-    int count = 0;
-    const int cursor = build_chunk64(g, bs, ws, e, L.e64, d, 0, n_src, from_super, lane, &count);
-    const bool single = cursor >= n_src;
-    const float gx = L.rfx, gy = L.rfy, gz = L.rfz;
+    const int sxn = smp ? smp->sx : 1, syn = smp ? smp->sy : 1, szn = smp ? smp->sz : 1;
+    const int n_pts = sxn * syn * szn;
     float sum = 0.0f, comp = 0.0f;
-    for (int base = 0; base < n_sub; base += 32) {
-        const bool dead = base + lane >= n_sub;
-        int sidx, ix, iy, iz;
-        if (!smp) {                       // s = 128 iz + 16 ix + iy, as in pe_element's rounds
-            const int rr = base >> 5;
-            const int s = ((rr >> 3) * 2 + (lane >> 4)) * 128 + ((lane >> 1) & 7) * 16 + (rr & 7) * 2 + (lane & 1);
-            iz = s >> 7;
-            ix = (s >> 4) & 7;
-            iy = s & 15;
-            sidx = (iz * ny + iy) * nx + ix;
-        } else {
-            sidx = dead ? n_sub - 1 : base + lane;
-            iz = sidx / nxy;
-            const int rem = sidx - iz * nxy;
-            iy = rem / nx;
-            ix = rem - iy * nx;
-        }
-        const float xDs = -L.w / 2.0f + ((float)ix + 0.5f) * gx * L.w;       // :1207-1217
-        const float zDs = -L.h / 2.0f + ((float)iz + 0.5f) * gz * L.h;
-        const float yDs = -L.t / 2.0f + ((float)iy + 0.5f) * gy * L.t;
-        const RayL r = ray_local(L, xDs, yDs, zDs);
-        const float sa_a = e.filt ? r.rx : 0.0f, sa_b = e.filt ? r.rz : 0.0f;
-        WalkL s{0.0, 0.0f, 0.0f, 0};
-        bool blocked = false;
-        for (int m = 0; m < g.n_layers; ++m) {                             // plate penalty :1240-1254
-            if (in_rect(ws.inner[m], sa_a, sa_b)) continue;
-            const float* pb = L.plate[m];
-            const float tl = box_chord(0.0f, 0.0f, 0.0f, r.qx, r.qy, r.qz, pb[0], pb[1], pb[2], pb[3], pb[4], pb[5]);
-            if (tl < 0.1f) { s.att = s.att + 100000.0; blocked = true; }
-        }
-        const bool skip = dead || (blocked && g.nonneg_mu);
-        float4 box = make_float4(skip ? INFINITY : sa_a, skip ? -INFINITY : sa_a, skip ? INFINITY : sa_b,
-                                 skip ? -INFINITY : sa_b);
-#pragma unroll
-        for (int off = 16; off > 0; off >>= 1) {
-            box.x = fminf(box.x, __shfl_xor_sync(0xffffffffu, box.x, off));
-            box.y = fmaxf(box.y, __shfl_xor_sync(0xffffffffu, box.y, off));
-            box.z = fminf(box.z, __shfl_xor_sync(0xffffffffu, box.z, off));
-            box.w = fmaxf(box.w, __shfl_xor_sync(0xffffffffu, box.w, off));
-        }
-        int cur = 0;
-        bool first_chunk = true;
-        while (true) {
-            if (!single && !first_chunk) {
-                cur = build_chunk64(g, bs, ws, e, L.e64, d, cur, n_src, from_super, lane, &count);
-            } else if (!single) {
-                if (base > 0) cur = build_chunk64(g, bs, ws, e, L.e64, d, 0, n_src, from_super, lane, &count);
-                else cur = cursor;
+    for (int src = 0; src < n_pts; ++src) {
+        // source point at fractions ((j + 0.5) / n) of the voxel along x, y, z
+        const int jx = src % sxn, jy = (src / sxn) % syn, jz = src / (sxn * syn);
+        const double fxd = ((double)jx + 0.5) / (double)sxn, fyd = ((double)jy + 0.5) / (double)syn;
+        const double fzd = ((double)jz + 0.5) / (double)szn;
+        __syncwarp();                                    // the previous point's ElemL and plate rectangles are done
+        Elem e;
+        if (!init_element(g, ws, d, v, cr, sr, lane, e, (float)fxd, (float)fyd, (float)fzd)) {   // mu_t <= 0.01
+            if (sub_out) {                                                                     // (:1107, :1194)
+                for (int i = lane; i < n_sub; i += 32) sub_out[i] = 0.0f;
             }
-            first_chunk = false;
-            int k = 0;
-            while (k < count) {
-                int next = count, nh = 0;
-                const int nr = fill_round_local(g, ws, e, L, k, count, box, 0, lane, &next, &nh);
-                if (!skip) walk_round_local(g, ws, nh, nr, r, sa_a, sa_b, s);
-                __syncwarp();
-                k = next;
+            return 0.0;
+        }
+        if (lane == 0) init_elem_local(g, d, v, rotation, nx, ny, nz, L, fxd, fyd, fzd);
+        __syncwarp();
+        const bool from_super = bs.s_count >= 0;
+        const int n_src = from_super ? bs.s_count : g.n_holes + g.n_det;
+        int count = 0;
+        const int cursor = build_chunk64(g, bs, ws, e, L.e64, d, 0, n_src, from_super, lane, &count);
+        const bool single = cursor >= n_src;
+        const float gx = L.rfx, gy = L.rfy, gz = L.rfz;
+        for (int base = 0; base < n_sub; base += 32) {
+            const bool dead = base + lane >= n_sub;
+            int sidx, ix, iy, iz;
+            if (!smp) {                       // s = 128 iz + 16 ix + iy, as in pe_element's rounds
+                const int rr = base >> 5;
+                const int s = ((rr >> 3) * 2 + (lane >> 4)) * 128 + ((lane >> 1) & 7) * 16 + (rr & 7) * 2 + (lane & 1);
+                iz = s >> 7;
+                ix = (s >> 4) & 7;
+                iy = s & 15;
+                sidx = (iz * ny + iy) * nx + ix;
+            } else {
+                sidx = dead ? n_sub - 1 : base + lane;
+                iz = sidx / nxy;
+                const int rem = sidx - iz * nxy;
+                iy = rem / nx;
+                ix = rem - iy * nx;
             }
-            if (single || cur >= n_src) break;
+            const float xDs = -L.w / 2.0f + ((float)ix + 0.5f) * gx * L.w;       // :1207-1217
+            const float zDs = -L.h / 2.0f + ((float)iz + 0.5f) * gz * L.h;
+            const float yDs = -L.t / 2.0f + ((float)iy + 0.5f) * gy * L.t;
+            const RayL r = ray_local(L, xDs, yDs, zDs);
+            const float sa_a = e.filt ? r.rx : 0.0f, sa_b = e.filt ? r.rz : 0.0f;
+            WalkL s{0.0, 0.0f, 0.0f, 0};
+            bool blocked = false;
+            for (int m = 0; m < g.n_layers; ++m) {                             // plate penalty :1240-1254
+                if (in_rect(ws.inner[m], sa_a, sa_b)) continue;
+                const float* pb = L.plate[m];
+                const float tl = box_chord(0.0f, 0.0f, 0.0f, r.qx, r.qy, r.qz, pb[0], pb[1], pb[2], pb[3], pb[4], pb[5]);
+                if (tl < 0.1f) { s.att = s.att + 100000.0; blocked = true; }
+            }
+            const bool skip = dead || (blocked && g.nonneg_mu);
+            float4 box = make_float4(skip ? INFINITY : sa_a, skip ? -INFINITY : sa_a, skip ? INFINITY : sa_b,
+                                     skip ? -INFINITY : sa_b);
+    #pragma unroll
+            for (int off = 16; off > 0; off >>= 1) {
+                box.x = fminf(box.x, __shfl_xor_sync(0xffffffffu, box.x, off));
+                box.y = fmaxf(box.y, __shfl_xor_sync(0xffffffffu, box.y, off));
+                box.z = fminf(box.z, __shfl_xor_sync(0xffffffffu, box.z, off));
+                box.w = fmaxf(box.w, __shfl_xor_sync(0xffffffffu, box.w, off));
+            }
+            int cur = 0;
+            bool first_chunk = true;
+            while (true) {
+                if (!single && !first_chunk) {
+                    cur = build_chunk64(g, bs, ws, e, L.e64, d, cur, n_src, from_super, lane, &count);
+                } else if (!single) {
+                    if (base > 0) cur = build_chunk64(g, bs, ws, e, L.e64, d, 0, n_src, from_super, lane, &count);
+                    else cur = cursor;
+                }
+                first_chunk = false;
+                int k = 0;
+                while (k < count) {
+                    int next = count, nh = 0;
+                    const int nr = fill_round_local(g, ws, e, L, k, count, box, 0, lane, &next, &nh);
+                    if (!skip) walk_round_local(g, ws, nh, nr, r, sa_a, sa_b, s);
+                    __syncwarp();
+                    k = next;
+                }
+                if (single || cur >= n_src) break;
+            }
+            float term = 0.0f;
+            if (!skip) {
+                if (s.lay < g.n_layers) close_layers_local(g, s, g.n_layers, r.dsec);
+                term = finish_local(L, r, ix, iy, iz, xDs, yDs, zDs, s.att);
+                neumaier_add(sum, comp, term);
+            }
+            if (sub_out && !dead) sub_out[sidx] = term;
         }
-        float term = 0.0f;
-        if (!skip) {
-            if (s.lay < g.n_layers) close_layers_local(g, s, g.n_layers, r.dsec);
-            term = finish_local(L, r, ix, iy, iz, xDs, yDs, zDs, s.att);
-            neumaier_add(sum, comp, term);
-        }
-        if (sub_out && !dead) sub_out[sidx] = term;
     }
     // warp sum of the (sum, compensation) pairs, compensated as well
 #pragma unroll
@@ -539,5 +549,5 @@ __device__ double pe_element_local(const DevGeom& g, const BlockSmem& bs, WarpSm
         comp += oc;
     }
     __syncwarp();                                    // L is rewritten by the warp's next element
-    return (double)sum + (double)comp;
+    return ((double)sum + (double)comp) / (double)n_pts;
 }

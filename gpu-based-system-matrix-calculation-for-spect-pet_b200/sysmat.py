@@ -39,7 +39,8 @@ EXPORTS = ("PESysMatGen", "scatter", "scatter_collimator", "scatter_crystal", "s
            "sysmat_csr_fill", "sysmat_pe_work", "sysmat_batch_create", "sysmat_batch_set_tiles",
            "sysmat_batch_get_tiles", "sysmat_batch_tune", "sysmat_batch_run", "sysmat_batch_destroy",
            "sysmat_batch", "sysmat_scatter_prepare_native", "sysmat_set_hole_shapes", "sysmat_pe_csr_file", "sysmat_project", "sysmat_vjp", "sysmat_backproject",
-           "sysmat_measure_peaks", "sysmat_ell_chords", "sysmat_pe_sampled", "sysmat_scatter_grid",
+           "sysmat_measure_peaks", "sysmat_ell_chords", "sysmat_pe_sampled", "sysmat_pe_sampled_mode",
+           "sysmat_scatter_grid",
            "sysmat_scatter_batch_create", "sysmat_scatter_batch_run", "sysmat_scatter_batch_destroy",
            "sysmat_error_string", "sysmat_version")
 
@@ -86,6 +87,10 @@ def lib():
             "sysmat_pe_sampled": ([_vp, ctypes.c_float, ctypes.c_int, ctypes.c_int, ctypes.c_longlong,
                                    ctypes.c_longlong, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int),
                                    _vp, ctypes.c_longlong, _vp], ctypes.c_int),
+            "sysmat_pe_sampled_mode": ([_vp, ctypes.c_float, ctypes.c_int, ctypes.c_int, ctypes.c_longlong,
+                                        ctypes.c_longlong, ctypes.POINTER(ctypes.c_int),
+                                        ctypes.POINTER(ctypes.c_int), ctypes.c_int, _vp, ctypes.c_longlong, _vp],
+                                       ctypes.c_int),
             "sysmat_bitmap_crystal_words": ([_vp], ctypes.c_longlong),
             "sysmat_bitmap_collimator_words": ([_vp], ctypes.c_longlong),
             "sysmat_bitmap_crystal": ([_vp, _vp, _vp], ctypes.c_int),
@@ -252,17 +257,20 @@ class Context:
         return out
 
     def pe_sampled(self, out, crystal_div=(8, 16, 8), voxel_sub=(1, 1, 1), rotation=0.0, det_begin=0,
-                   det_count=None, vox_begin=0, vox_count=None, stream=None):
+                   det_count=None, vox_begin=0, vox_count=None, stream=None, mode=MODE_PRECISE):
         """Fill `out` with the PE block of the sampled form: crystal_div sub-elements of each
         crystal along x, depth, z and voxel_sub source points per voxel along x, y, z; each
-        element is the mean over its source points, summed in FP64 (sysmat_pe_sampled)."""
+        element is the mean over its source points (sysmat_pe_sampled_mode).  mode: MODE_PRECISE
+        (the reference's float program, FP64 sums) or MODE_LOCAL (the local-coordinate FP32
+        form, within 1e-5 of FP64)."""
         det_count = self.n_det - det_begin if det_count is None else det_count
         vox_count = self.n_vox - vox_begin if vox_count is None else vox_count
         ld = out.stride(0) if out.dim() == 2 else vox_count
         dv = (ctypes.c_int * 3)(*[int(x) for x in crystal_div])
         sv = (ctypes.c_int * 3)(*[int(x) for x in voxel_sub])
-        _check(lib().sysmat_pe_sampled(self.handle, float(rotation), det_begin, det_count, vox_begin, vox_count,
-                                       dv, sv, _ptr(out), ld, _stream(stream)), "sysmat_pe_sampled")
+        _check(lib().sysmat_pe_sampled_mode(self.handle, float(rotation), det_begin, det_count, vox_begin,
+                                            vox_count, dv, sv, int(mode), _ptr(out), ld, _stream(stream)),
+               "sysmat_pe_sampled_mode")
         return out
 
     def pe_work(self, out, rotation=0.0, det_begin=0, det_count=None, vox_begin=0, vox_count=None,

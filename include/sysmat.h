@@ -139,6 +139,15 @@ SYSMAT_API int sysmat_pe_sampled(sysmat_ctx* ctx, float rotation, int det_begin,
                                  long long vox_begin, long long vox_count, const int* crystal_div,
                                  const int* voxel_sub, float* d_out, long long ld, void* stream);
 
+/* The sampled form in a chosen arithmetic: SYSMAT_MODE_PRECISE (the reference's float program,
+ * exactly what sysmat_pe_sampled computes) or SYSMAT_MODE_LOCAL (the local-coordinate FP32 form
+ * of SYSMAT_MODE_LOCAL at each source point, contributions summed with compensation: within 1e-5
+ * of the sampled form's FP64 evaluation; circular holes only).  Other arguments and errors as
+ * sysmat_pe_sampled. */
+SYSMAT_API int sysmat_pe_sampled_mode(sysmat_ctx* ctx, float rotation, int det_begin, int det_count,
+                                      long long vox_begin, long long vox_count, const int* crystal_div,
+                                      const int* voxel_sub, int mode, float* d_out, long long ld, void* stream);
+
 /* Relationship bitmaps in the reference's word layout (scatter.cu:1040-1074).
  * Word counts: crystal ceil(D(D+1)/2*D/32), collimator ceil(H0*D*D/32). */
 SYSMAT_API long long sysmat_bitmap_crystal_words(const sysmat_ctx* ctx);

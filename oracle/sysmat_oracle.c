@@ -182,13 +182,20 @@ int oracle_pe_sampled(const float* C, const float* D, const float* I, const floa
     return run_pe(&g, prec, dets, ndet, v0, nv, out, NULL, nthreads);
 }
 
-/* PE elements of the local-coordinate FP32 form (oracle_local.h; the reference's sampling:
- * 8 x 16 x 8 sub-elements, voxel centres), as float values widened to double. */
-int oracle_pe_local(const float* C, const float* D, const float* I, const int* dets, int ndet, long long v0,
-                    long long nv, double* out, int nthreads)
+/* PE elements of the local-coordinate FP32 form (oracle_local.h) with div[3] crystal
+ * sub-elements along x, depth, z and vsub[3] source points per voxel along x, y, z (the element
+ * is the mean over the source points, in double), as float values widened to double. */
+int oracle_pe_local_sampled(const float* C, const float* D, const float* I, const int* div, const int* vsub,
+                            const int* dets, int ndet, long long v0, long long nv, double* out, int nthreads)
 {
     ogeo g;
     if (parse(&g, C, D, I, NULL)) return -1;
+    for (int k = 0; k < 3; ++k) {
+        if (div[k] < 1 || vsub[k] < 1) return -1;
+        g.div[k] = div[k];
+        g.vsub[k] = vsub[k];
+    }
+    const int sx = vsub[0], sy = vsub[1], sz = vsub[2];
     if (nthreads > 0) omp_set_num_threads(nthreads);
     long long total = (long long)ndet * nv;
     int err = 0;
@@ -205,9 +212,16 @@ int oracle_pe_local(const float* C, const float* D, const float* I, const int* d
             if (!cc || !ch || !lh || !lc) continue;
             int d = dets[e / nv];
             long long v = v0 + e % nv;
-            double xI, yI, zI;
-            voxel_centre_f64(&g, v, &xI, &yI, &zI);
-            out[e] = (double)pe_element_local(&g, d, xI, yI, zI, cc, ch, nch, lh, lc, NULL);
+            double acc = 0.0;
+            for (int jz = 0; jz < sz; ++jz)
+            for (int jy = 0; jy < sy; ++jy)
+            for (int jx = 0; jx < sx; ++jx) {
+                double xI, yI, zI;
+                voxel_point_f64(&g, v, ((double)jx + 0.5) / (double)sx, ((double)jy + 0.5) / (double)sy,
+                                ((double)jz + 0.5) / (double)sz, &xI, &yI, &zI);
+                acc += (double)pe_element_local(&g, d, xI, yI, zI, cc, ch, nch, lh, lc, NULL);
+            }
+            out[e] = acc / (double)(sx * sy * sz);
         }
         free(cc);
         free(ch);
@@ -215,6 +229,14 @@ int oracle_pe_local(const float* C, const float* D, const float* I, const int* d
         free(lc);
     }
     return err ? -2 : 0;
+}
+
+/* The local form at the reference's sampling (8 x 16 x 8 sub-elements, voxel centres). */
+int oracle_pe_local(const float* C, const float* D, const float* I, const int* dets, int ndet, long long v0,
+                    long long nv, double* out, int nthreads)
+{
+    const int div[3] = {8, 16, 8}, vsub[3] = {1, 1, 1};
+    return oracle_pe_local_sampled(C, D, I, div, vsub, dets, ndet, v0, nv, out, nthreads);
 }
 
 /* Elements of the grid scatter model (oracle_grid.h) for detectors dets[0..ndet) and voxels

@@ -60,6 +60,30 @@ def rel_err(a, b, scale=None):
 TOL = 1e-5
 
 
+def shifted(geo, axis, delta):
+    """The system with its image moved by `delta` mm along axis 0/1/2 (x, y, z)."""
+    img = geo.image.astype(np.float64).copy()
+    img[8 + axis] += delta
+    return geometry.Geometry(geo.name, geo.collimator, geo.detector, img.astype(np.float32), geo.physics)
+
+
+def within_knife_edge(a, geo, fp64_of, r, deltas=(1e-6, -1e-6, 3e-6, -3e-6)):
+    """Elements of `a` whose error r exceeds TOL lie in the range their FP64 value spans when the
+    image moves by `deltas` mm along x, y and z: a sub-element ray passes within that distance
+    of a threshold of the program (a hole rim, a cap plane, the 0.1 mm penalty), where an
+    evaluation's last bits decide the branch.  fp64_of(geometry) gives the FP64 elements.
+    Returns the number of such elements."""
+    out = r > TOL
+    if not out.any():
+        return 0
+    vals = np.stack([fp64_of(shifted(geo, k, dl)) for k in range(3) for dl in deltas])
+    lo, hi = vals.min(axis=0), vals.max(axis=0)
+    slack = 1e-7 * np.abs(hi)
+    ok = (a >= lo - slack) & (a <= hi + slack)
+    assert np.all(ok[out]), (np.argwhere(out & ~ok)[:5], a[out & ~ok][:5])
+    return int(out.sum())
+
+
 def check_pe_vs_reference(a, geo, z):
     """Photoelectric elements `a` (the golden's rows) against the reference's own output z["pe"]:
     most elements bit-identical (the same float program), every element within 1e-5, except

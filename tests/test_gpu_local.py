@@ -1,4 +1,6 @@
-"""GPU tests of the local-coordinate FP32 mode (SYSMAT_MODE_LOCAL), through the C ABI.
+"""GPU tests of the local-coordinate FP32 mode (SYSMAT_MODE_LOCAL), through the C ABI, at the
+reference's sampling (sysmat_pe) and at other crystal divisions and voxel source points
+(sysmat_pe_sampled_mode).
 
 The mode evaluates the reference's element program in float arithmetic arranged so that only
 small, local quantities are rounded (oracle/oracle_local.h states the scheme; its CPU twin is
@@ -9,7 +11,7 @@ those rare elements are bounded separately."""
 import numpy as np
 import pytest
 
-from conftest import TOL, geometry, golden, oracle, rel_err, sysmat
+from conftest import TOL, geometry, golden, oracle, rel_err, sysmat, within_knife_edge
 
 pytestmark = pytest.mark.gpu
 
@@ -126,3 +128,71 @@ def test_local_mode_rejects_elliptical_holes(gpu):
     out = torch.empty((ctx.n_det, ctx.n_vox), dtype=torch.float32, device="cuda")
     with pytest.raises(sysmat.SysmatError):
         ctx.pe(out, mode=sysmat.MODE_LOCAL)
+
+
+def _local_sampled(torch, ctx, div, sub, rotation=0.0, **blk):
+    nd = blk.get("det_count", ctx.n_det)
+    nv = blk.get("vox_count", ctx.n_vox)
+    out = torch.empty((nd, nv), dtype=torch.float32, device="cuda")
+    ctx.pe_sampled(out, div, sub, rotation=rotation, mode=sysmat.MODE_LOCAL, **blk)
+    torch.cuda.synchronize()
+    return out.cpu().numpy()
+
+
+SAMPLINGS = [((2, 8, 2), (2, 2, 2)), ((3, 5, 3), (2, 1, 3)), ((4, 4, 4), (1, 1, 1))]
+
+
+@pytest.mark.parametrize("name", ["mini0", "mini1r2", "mini2w"])
+@pytest.mark.parametrize("div,sub", SAMPLINGS)
+def test_local_sampled_within_1e5_of_fp64(gpu, name, div, sub):
+    """The sampled form (crystal divisions, voxel source points) in the local arithmetic: within
+    1e-5 of the sampled form's FP64 evaluation but for knife-edge elements (a few per thousand
+    at coarse divisions, where one sub-element is a larger share of the element)."""
+    geo, _ = golden(name)
+    ctx = sysmat.Context(geo)
+    rot = float(geo.image[20])
+    a = _local_sampled(gpu, ctx, div, sub, rotation=rot)
+    o64 = oracle.pe_sampled(geo, div, sub, prec=64)
+    r = rel_err(a, o64)
+    assert a.max() > 0 and np.median(r) < 1e-6, np.median(r)
+    # past 1e-5: only knife-edge elements (a sub-element ray within ~1e-6 mm of a threshold)
+    n = within_knife_edge(a, geo, lambda g: oracle.pe_sampled(g, div, sub, prec=64), r)
+    assert n <= 0.005 * r.size, n
+    twin = oracle.pe_local(geo, crystal_div=div, voxel_sub=sub)
+    assert np.median(rel_err(a, twin)) < 1e-6
+
+
+def test_local_sampled_config1_4x4x4_and_config2_as_stated(gpu):
+    """Configuration 1 at 4x4x4 sub-elements (moved off its exact grid) and a configuration-2
+    sample at its stated sampling (2x8x2 sub-elements, 2x2x2 source points): within 1e-5 of FP64
+    but for knife-edge elements, and closer than the float program's sampled form on the same
+    elements."""
+    torch = gpu
+    cases = [(_config1_shifted(), (4, 4, 4), (1, 1, 1), None, 0, None),
+             (geometry.config2(), (2, 8, 2), (2, 2, 2), np.array([100, 1000, 2080, 3000, 4000]),
+              96 * 96 * 16 + 96 * 48, 96)]
+    for geo, div, sub, dets, v0, nv in cases:
+        ctx = sysmat.Context(geo)
+        nv = ctx.n_vox if nv is None else nv
+        dets = np.arange(0, ctx.n_det, 7) if dets is None else dets
+        a = np.concatenate([_local_sampled(torch, ctx, div, sub, det_begin=int(d), det_count=1, vox_begin=v0,
+                                           vox_count=nv) for d in dets])
+        o64 = oracle.pe_sampled(geo, div, sub, prec=64, dets=dets, v0=v0, nv=nv)
+        o32 = oracle.pe_sampled(geo, div, sub, prec=32, dets=dets, v0=v0, nv=nv)
+        r, r32 = rel_err(a, o64), rel_err(o32, o64)
+        assert a.max() > 0 and np.median(r) < 1e-6, (geo.name, np.median(r))
+        n = within_knife_edge(a, geo, lambda g: oracle.pe_sampled(g, div, sub, prec=64, dets=dets, v0=v0, nv=nv), r)
+        assert n <= 0.005 * r.size, (geo.name, n)
+        assert r.max() < r32.max(), (geo.name, r.max(), r32.max())
+
+
+def test_local_sampled_blocks_equal_the_full_matrix(gpu):
+    torch = gpu
+    geo, _ = golden("mini1r2")
+    ctx = sysmat.Context(geo)
+    rot = float(geo.image[20])
+    full = _local_sampled(torch, ctx, (2, 8, 2), (2, 2, 2), rotation=rot)
+    for (d0, nd, v0, nv) in ((0, 3, 0, 17), (7, 5, 31, 40), (ctx.n_det - 1, 1, ctx.n_vox - 1, 1)):
+        blk = _local_sampled(torch, ctx, (2, 8, 2), (2, 2, 2), rotation=rot, det_begin=d0, det_count=nd,
+                             vox_begin=v0, vox_count=nv)
+        assert np.array_equal(blk, full[d0:d0 + nd, v0:v0 + nv])
