@@ -29,6 +29,7 @@ def test_pe_reference_mode_matches_reference(gpu, name):
     r = check_pe_vs_reference(a, geo, z)
     if not name.startswith("config4"):           # thin plates and config 5: every element
         assert r.max() <= TOL, (name, r.max())
+        assert np.mean(a == z["pe"]) > 0.5, (name, np.mean(a == z["pe"]))
 
 
 @pytest.mark.parametrize("name", ["mini0", "mini1r2", "mini2w"])
