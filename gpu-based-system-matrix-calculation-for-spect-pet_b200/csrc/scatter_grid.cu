@@ -537,6 +537,7 @@ __global__ void __launch_bounds__(kGridThreads) grid_sum_kernel(DevGeom g, GridG
     const int nd = min(kGridDetTile, S.det_begin + S.det_count - d0);
     for (int i = t; i < kGridDetTile * kGridMaxVox; i += kGridThreads) (&acc[0][0])[i] = 0.0;
     const float e0 = S.e0;
+    const double inv_kn_total = 1.0 / S.kn_total;
     const float ang = S.rotation * g.angle_step;
     const float crot = cosf(ang), srot = sinf(ang);
     for (int ch = 0; ch < kGridChunksPerBlock; ++ch) {
@@ -604,14 +605,18 @@ __global__ void __launch_bounds__(kGridThreads) grid_sum_kernel(DevGeom g, GridG
                     const float rla = 1.0f / la;
                     // angle v -> p -> d (cosines as dot products times reciprocal lengths)
                     const float cc = fminf(fmaxf(-(ax * px + ay * py + az * pz) * rla * sm.rlb[8][j], -1.0f), 1.0f);
-                    const float es = e0 / (1.0f + (e0 / 511.0f) * (1.0f - cc));
-                    const float res = M.w * sqrtf(es / e0);
+                    // the model restated in float with reciprocals where the reference's program
+                    // divides (no bit-parity target here: the definition is the FP64 oracle)
+                    const float r1 = 1.0f + (e0 / 511.0f) * (1.0f - cc);          // E0 / E'
+                    const float es = __fdividef(e0, r1);
+                    const float res = M.w * sqrtf(__fdividef(es, e0));
                     if ((es * (1 + 2 * res / 2.35482f)) <= lo || (es * (1 - 2 * res / 2.35482f)) >= hi) continue;
-                    const float pwin = window_prob(es, res, lo, hi);
+                    const float rs2 = __frcp_rn(res / 2.35482f * es * 1.41421356f);
+                    const float pwin = 0.5f * (erff((hi - es) * rs2) - erff((lo - es) * rs2));
                     const float sc = sqrtf(fmaxf(1.0f - cc * cc, 0.0f));
                     float phi;
                     if (lsd * sc * 2.0f <= rdet) phi = (float)(2.0 * 3.14159265358979323846);
-                    else phi = 4.0f * asinf(fminf(rdet / 2.0f / lsd / sc, 1.0f));
+                    else phi = 4.0f * asinf(fminf(0.5f * rdet * sm.rlb[8][j] * __frcp_rn(sc), 1.0f));
                     // polar range over the corners of d, seen from p along v -> p (:1305-1335)
                     float cmin = INFINITY, cmax = -INFINITY;
 #pragma unroll
@@ -626,14 +631,14 @@ __global__ void __launch_bounds__(kGridThreads) grid_sum_kernel(DevGeom g, GridG
                     const float lthr = box_chord(I.x, I.y, I.z, px + 1000.0f * ax * rla, py + 1000.0f * ay * rla,
                                                  pz + 1000.0f * az * rla, -hw, -ht, -hh, hw, ht, hh);
                     if (lthr > 0.001f) tmin = 0.0f;
-                    const double ratio = (kn_integral(S.kn_tab, (double)tmax) - kn_integral(S.kn_tab, (double)tmin)) /
-                                         S.kn_total;
-                    const float r1 = e0 / es, r3 = r1 * r1 * r1;
+                    const double ratio = (kn_integral(S.kn_tab, (double)tmax) - kn_integral(S.kn_tab, (double)tmin)) *
+                                         inv_kn_total;
+                    const float r3 = r1 * r1 * r1;
                     const float att = terms[5][j] * r3 + terms[6][j] * r1;
                     const float mpe_s = M.y * r3, mt_s = mpe_s + M.z * r1;
-                    const float absf = -expm1f(-terms[4][j] * mt_s) * mpe_s / mt_s;
-                    sum += (double)(w * phi / 2.0f) / 3.14159265358979323846 * ratio * (double)pwin *
-                           (double)expf(-att) * (double)absf;
+                    const float absf = -expm1f(-terms[4][j] * mt_s) * __fdividef(mpe_s, mt_s);
+                    sum += (double)(w * phi * (float)(0.5 / 3.14159265358979323846) * pwin * expf(-att) * absf) *
+                           ratio;
                 }
 #pragma unroll
                 for (int off = 16; off > 0; off >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, off);

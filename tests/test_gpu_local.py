@@ -196,3 +196,21 @@ def test_local_sampled_blocks_equal_the_full_matrix(gpu):
         blk = _local_sampled(torch, ctx, (2, 8, 2), (2, 2, 2), rotation=rot, det_begin=d0, det_count=nd,
                              vox_begin=v0, vox_count=nv)
         assert np.array_equal(blk, full[d0:d0 + nd, v0:v0 + nv])
+
+
+def test_local_sampled_rejects_other_modes_and_elliptical_holes(gpu):
+    torch = gpu
+    geo, _ = golden("mini0")
+    ctx = sysmat.Context(geo)
+    out = torch.empty((ctx.n_det, ctx.n_vox), dtype=torch.float32, device="cuda")
+    for mode in (sysmat.MODE_REFERENCE, sysmat.MODE_FP64, 7):
+        with pytest.raises(sysmat.SysmatError):
+            ctx.pe_sampled(out, (2, 8, 2), (2, 2, 2), mode=mode)
+    shapes = np.zeros((geo.n_holes, 3), dtype=np.float32)
+    shapes[0] = (0.4, 0.3, 0.5)
+    ctx.set_hole_shapes(shapes)
+    with pytest.raises(sysmat.SysmatError):
+        ctx.pe_sampled(out, (2, 8, 2), (2, 2, 2), mode=sysmat.MODE_LOCAL)
+    ctx.pe_sampled(out, (2, 8, 2), (2, 2, 2), mode=sysmat.MODE_PRECISE)     # the float form takes them
+    torch.cuda.synchronize()
+    assert out.max().item() > 0
