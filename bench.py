@@ -623,19 +623,21 @@ def run_local(args, sysmat, torch, keep):
     g = geometry.config2()
     ctx = sysmat.Context(g)
     nxy = int(g.image[0]) * int(g.image[1])
-    out = torch.empty((ctx.n_det, nxy), dtype=torch.float32, device="cuda")
+    D = ctx.n_det if args.det_count is None else min(args.det_count, ctx.n_det)
+    out = torch.empty((D, nxy), dtype=torch.float32, device="cuda")
 
     def step():
-        ctx.pe(out, vox_begin=16 * nxy, vox_count=nxy, mode=sysmat.MODE_LOCAL)
+        ctx.pe(out, det_count=D, vox_begin=16 * nxy, vox_count=nxy, mode=sysmat.MODE_LOCAL)
 
     step()
     ms = _events(torch, step, n=2)
     nx = int(g.image[0])
-    keep["local"] = {"d0": 0, "out": out[:, SAMPLE_ROW * nx:(SAMPLE_ROW + 1) * nx].cpu().numpy()}
+    if D == ctx.n_det:
+        keep["local"] = {"d0": 0, "out": out[:, SAMPLE_ROW * nx:(SAMPLE_ROW + 1) * nx].cpu().numpy()}
     ctx.close()
-    return {"value": ctx.n_det * nxy / (ms * 1e-3), "unit": UNIT, "ms_per_step": ms, "arithmetic": "f32 (local)",
-            "workload": f"config2 PE, local-coordinate FP32 mode: all crystals x z-plane 16 ({ctx.n_det * nxy} "
-                        "elements)"}
+    what = "all crystals" if D == ctx.n_det else f"crystals 0..{D - 1}"
+    return {"value": D * nxy / (ms * 1e-3), "unit": UNIT, "ms_per_step": ms, "arithmetic": "f32 (local)",
+            "workload": f"config2 PE, local-coordinate FP32 mode: {what} x z-plane 16 ({D * nxy} elements)"}
 
 
 def run_batch(args, sysmat, torch, n_instances=64, rows=8, sweep=True):
