@@ -383,7 +383,6 @@ extern "C" SYSMAT_API int sysmat_pe(sysmat_ctx* ctx, float rotation, int det_beg
     if (mode != SYSMAT_MODE_REFERENCE && mode != SYSMAT_MODE_PRECISE && mode != SYSMAT_MODE_FP64 &&
         mode != SYSMAT_MODE_LOCAL)
         return SYSMAT_ERR_ARG;
-    if (mode == SYSMAT_MODE_LOCAL && ctx->g.hole_shape) return SYSMAT_ERR_ARG;   // circular holes only
     if (det_count == 0 || vox_count == 0) return SYSMAT_OK;
     cudaStream_t s = (cudaStream_t)stream;
     const PeLaunch L = pe_block(ctx, rotation, det_begin, det_count, vox_begin, vox_count, d_out, ld);
@@ -399,7 +398,6 @@ extern "C" SYSMAT_API int sysmat_pe_sampled_mode(sysmat_ctx* ctx, float rotation
     if (rc) return rc;
     if (!crystal_div || !voxel_sub) return SYSMAT_ERR_ARG;
     if (mode != SYSMAT_MODE_PRECISE && mode != SYSMAT_MODE_LOCAL) return SYSMAT_ERR_ARG;
-    if (mode == SYSMAT_MODE_LOCAL && ctx->g.hole_shape) return SYSMAT_ERR_ARG;     // circular holes only
     Sampling smp;
     smp.nx = crystal_div[0]; smp.ny = crystal_div[1]; smp.nz = crystal_div[2];
     smp.sx = voxel_sub[0]; smp.sy = voxel_sub[1]; smp.sz = voxel_sub[2];

@@ -43,7 +43,6 @@ extern "C" SYSMAT_API int sysmat_pe_csr_file(sysmat_ctx* ctx, float rotation, co
     if (mode != SYSMAT_MODE_REFERENCE && mode != SYSMAT_MODE_PRECISE && mode != SYSMAT_MODE_FP64 &&
         mode != SYSMAT_MODE_LOCAL)
         return SYSMAT_ERR_ARG;
-    if (mode == SYSMAT_MODE_LOCAL && ctx->g.hole_shape) return SYSMAT_ERR_ARG;
     int cur = -1;
     if (cudaGetDevice(&cur) != cudaSuccess || cur != ctx->device) return SYSMAT_ERR_ARG;
     const long long D = ctx->g.n_det, V = ctx->g.nvox;

@@ -980,7 +980,7 @@ __device__ __forceinline__ void pe_brick(const DevGeom& g, BlockSmem& bs, WarpSm
             float* so = nullptr;
             if (SAMPLED && O.sub_out)
                 so = O.sub_out + ((v - O.vox_begin) * O.det_count + di) * (long long)(smp->nx * smp->ny * smp->nz);
-            val = (float)pe_element_local(g, bs, ws, d, v, cr, sr, rotation, lane, SAMPLED ? smp : nullptr, so);
+            val = (float)pe_element_local<ELL>(g, bs, ws, d, v, cr, sr, rotation, lane, SAMPLED ? smp : nullptr, so);
         } else if constexpr (SAMPLED) val = (float)pe_element_sampled<ELL>(g, bs, ws, d, v, cr, sr, lane, *smp);
         else if constexpr (MODE == 2) val = (float)pe_element64(g, bs, ws, d, v, cr, sr, rotation, lane);
         else val = (float)pe_element<MODE, COUNT, ELL>(g, bs, ws, d, v, cr, sr, lane, counters);
@@ -1194,7 +1194,11 @@ int launch_pe_batch(const BatchLaunch& B, int mode, bool ell, int grid, cudaStre
 int launch_pe(const DevGeom& g, const PeLaunch& L, int mode, int num_sms, cudaStream_t stream)
 {
     if (mode == 2) return g.t64.cry_pos ? launch_mode<2, false, false>(g, L, num_sms, stream) : -1;
-    if (mode == 3) return (g.t64.cry_pos && !g.hole_shape) ? launch_mode<3, false, false>(g, L, num_sms, stream) : -1;
+    if (mode == 3) {
+        if (!g.t64.cry_pos) return -1;
+        return g.hole_shape ? launch_mode<3, false, true>(g, L, num_sms, stream)
+                            : launch_mode<3, false, false>(g, L, num_sms, stream);
+    }
     if (g.hole_shape) {                   // systems with elliptical holes
         if (L.counters) return launch_mode<0, true, true>(g, L, num_sms, stream);
         return mode == 0 ? launch_mode<0, false, true>(g, L, num_sms, stream)
@@ -1207,8 +1211,9 @@ int launch_pe(const DevGeom& g, const PeLaunch& L, int mode, int num_sms, cudaSt
 
 int launch_pe_local_sampled(const DevGeom& g, const PeLaunch& L, int num_sms, cudaStream_t stream)
 {
-    if (!g.t64.cry_pos || g.hole_shape) return -1;
-    return launch_mode<3, false, false, true>(g, L, num_sms, stream);
+    if (!g.t64.cry_pos) return -1;
+    return g.hole_shape ? launch_mode<3, false, true, true>(g, L, num_sms, stream)
+                        : launch_mode<3, false, false, true>(g, L, num_sms, stream);
 }
 
 int launch_pe_sampled(const DevGeom& g, const PeLaunch& L, int num_sms, cudaStream_t stream)

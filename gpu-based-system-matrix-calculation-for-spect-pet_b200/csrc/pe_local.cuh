@@ -16,7 +16,7 @@
 //     relative to crystal d's, in its own frame;
 //   - per ray, in float: the sub-element's offset from crystal d's centre, the slope
 //     difference to the central ray (formed without cancellation), hole chords as y-extents
-//     inside the hole's circle in the hole's frame, the septal length (T - sum of extents) /
+//     inside the hole's circle (or ellipse) in the hole's frame, the septal length (T - sum of extents) /
 //     cos, crystal chords measured from the sub-element, self-attenuation and absorption
 //     chords from the sub-element centre in crystal d's frame;
 //   - the 1024 contributions are summed with Neumaier's compensated summation, per lane and
@@ -145,8 +145,11 @@ __device__ __forceinline__ float box_chord_near(const float P[3], const float q[
 // voxel: ta = dy * sec, ...) enter only its threshold tests.  Offsets, slopes and the roots are
 // in double: near a tangent, and for a hole met far from where the ray enters the plate, the
 // chord is ill-conditioned in them, and float offsets or slopes would move it by ~1e-5 mm.
+// tq scales the reference's discriminant threshold (1 for a circle; an ellipse passes its
+// offsets and slopes divided by its semi-axes with r = 1, and tq = rho_x^4 rho_z^4).
 __device__ __forceinline__ float hole_extent(double u0d, double w0d, double rxd, double rzd, double ad, double iad,
-                                             float r, float th, float dy, float sec, float tio, float ky)
+                                             float r, float th, float dy, float sec, float tio, float ky,
+                                             double tq = 1.0)
 {
     if (fabsf(th) < kEps) return 0.0f;
     const double u1d = u0d + rxd * (double)th, w1d = w0d + rzd * (double)th;
@@ -161,7 +164,7 @@ __device__ __forceinline__ float hole_extent(double u0d, double w0d, double rxd,
     }
     const double cross = u0d * rzd - w0d * rxd;
     const double qd = ad * r2 - cross * cross;                 // b^2 - a c (Lagrange identity)
-    if ((double)(ky * ky) * qd <= (double)0.00001f) return 0.0f;   // the reference's discriminant
+    if ((double)(ky * ky) * tq * qd <= (double)0.00001f) return 0.0f;   // the reference's discriminant
     const double bd = u0d * rxd + w0d * rzd;
     const double sq = (double)sqrtf((float)qd);
     const double s1 = (-bd - sq) * iad, s2 = (-bd + sq) * iad;
@@ -178,13 +181,39 @@ __device__ __forceinline__ float hole_extent(double u0d, double w0d, double rxd,
     return (float)(eb - ea);
 }
 
+// Elliptical hole (length_ellipticalcylinder_ray, PESysMatGen.cu:801-947, the y-parallel
+// cylinder ((u'/rho_x)^2 + (w'/rho_z)^2 <= 1 in the hole's frame turned by theta): the ray's
+// offset (u, w) and slopes (rx, rz) turned into that frame (u' = u cos + w sin,
+// w' = -u sin + w cos, as the reference turns the segment's points) and divided by the
+// semi-axes reduce it to the unit circle, whose y-extent hole_extent gives with the
+// discriminant threshold rescaled: the reference's b^2 - a c equals rho_x^4 rho_z^4 ky^2 times
+// the unit circle's.  Rewrites the arguments of hole_extent in place.
+__device__ __forceinline__ void to_unit_circle(double& u, double& w, double& rx, double& rz, double& a, double& ia,
+                                               float& r, double& tq, float ex, float ez, float ct, float st)
+{
+    const double c = (double)ct, s = (double)st, iex = 1.0 / (double)ex, iez = 1.0 / (double)ez;
+    const double p = (u * c + w * s) * iex, q = (-u * s + w * c) * iez;
+    const double al = (rx * c + rz * s) * iex, be = (-rx * s + rz * c) * iez;
+    u = p;
+    w = q;
+    rx = al;
+    rz = be;
+    a = al * al + be * be;
+    ia = 1.0 / a;
+    r = 1.0f;
+    const double e2 = (double)ex * (double)ex * (double)ez * (double)ez;
+    tq = e2 * e2;
+}
+
 // Copy kept entries [k0, k1) whose rectangle and capsule meet the round's slope box into the
 // round buffer with their local geometry (one entry per lane):
-//   hole:    ra = (offset of the central ray from the axis at y1: x, z; radius; mu),
-//            rb = (y1 - yI, y2 - y1, -, -)
+//   hole:    ra = (semi-axes rho_x, rho_z of an elliptical hole, 0 for a circle; radius; mu),
+//            rb = (y1 - yI, y2 - y1, offset of the central ray from the axis at y1: x as the two
+//            halves of a double), rc = (z the same way; cos, sin of the ellipse's angle)
 //   crystal: ra = (crystal d's centre minus this crystal's centre in its frame: x, y, z; mu),
 //            rb = (cos(-rot), sin(-rot), w, t), rc = (h, -, -, -)
 // Returns the new count; *next receives the first entry not examined.
+template <bool ELL>
 __device__ __forceinline__ int fill_round_local(const DevGeom& g, WarpSmem& ws, const Elem& e, const ElemL& L,
                                                 int k0, int k1, float4 box, int n, int lane, int* next, int* nh)
 {
@@ -223,12 +252,14 @@ __device__ __forceinline__ int fill_round_local(const DevGeom& g, WarpSmem& ws, 
                 const float4 hb = __ldg(&g.hole.b[id]);
                 const double dy = a.y - E.yI;
                 const double hx = (E.xI - a.x) + L.rxc * dy, hz = (E.zI - a.w) + L.rzc * dy;
-                ws.ra[pos] = make_float4((float)hx, (float)hz, hb.x, hb.y);
+                // elliptical: semi-axes and the cos, sin of the float angle in double, rounded once
+                const D4 S = (ELL && g.t64.hole_shape) ? g.t64.hole_shape[id] : D4{0.0, 0.0, 1.0, 0.0};
+                ws.ra[pos] = make_float4((float)S.x, (float)S.y, hb.x, hb.y);
                 // the offsets in double, as the bit patterns of two floats each
                 ws.rb[pos] = make_float4((float)dy, (float)(a.z - a.y), __int_as_float(__double2hiint(hx)),
                                          __int_as_float(__double2loint(hx)));
                 ws.rc[pos] = make_float4(__int_as_float(__double2hiint(hz)), __int_as_float(__double2loint(hz)),
-                                         0.0f, 0.0f);
+                                         (float)S.z, (float)S.w);
                 ws.rl[pos] = layer_of_hole(g, id);
             } else {
                 const int o = id - g.n_holes;
@@ -316,6 +347,7 @@ __device__ __forceinline__ void close_layers_local(const DevGeom& g, WalkL& s, i
     }
 }
 
+template <bool ELL>
 __device__ __forceinline__ void walk_round_local(const DevGeom& g, const WarpSmem& ws, int nh, int nr, const RayL& r,
                                                  float sa_a, float sa_b, WalkL& s)
 {
@@ -328,8 +360,11 @@ __device__ __forceinline__ void walk_round_local(const DevGeom& g, const WarpSme
         const float4 Cc = ws.rc[j];
         const double hx = __hiloint2double(__float_as_int(B.z), __float_as_int(B.w));
         const double hz = __hiloint2double(__float_as_int(Cc.x), __float_as_int(Cc.y));
-        const double u0 = hx + r.ddrx * (double)B.x, w0 = hz + r.ddrz * (double)B.x;
-        const float ext = hole_extent(u0, w0, r.drx_, r.drz_, r.da, r.dia, A.z, B.y, B.x, r.sec, r.sq, r.ky);
+        double u0 = hx + r.ddrx * (double)B.x, w0 = hz + r.ddrz * (double)B.x;
+        double rx = r.drx_, rz = r.drz_, a = r.da, ia = r.dia, tq = 1.0;
+        float rad = A.z;
+        if (ELL && A.x > 0.0f) to_unit_circle(u0, w0, rx, rz, a, ia, rad, tq, A.x, A.y, Cc.z, Cc.w);   // elliptical
+        const float ext = hole_extent(u0, w0, rx, rz, a, ia, rad, B.y, B.x, r.sec, r.sq, r.ky, tq);
         s.ext = s.ext + ext;
         s.hatt = s.hatt + A.w * ext;
     }
@@ -439,6 +474,7 @@ __device__ __forceinline__ void neumaier_add(float& s, float& c, float x)
 // reference-order kernel; other divisions go 32 to a round in (z, depth, x) order, x fastest.
 // sub_out (one source point only): each sub-element's contribution is also written there, at
 // index (iz * ny + iy) * nx + ix (the scatter grid's crystal-cell weights).
+template <bool ELL>
 __device__ double pe_element_local(const DevGeom& g, const BlockSmem& bs, WarpSmem& ws, int d, long long v, float cr,
                                    float sr, float rotation, int lane, const Sampling* smp = nullptr,
                                    float* sub_out = nullptr)
@@ -524,8 +560,8 @@ __device__ double pe_element_local(const DevGeom& g, const BlockSmem& bs, WarpSm
                 int k = 0;
                 while (k < count) {
                     int next = count, nh = 0;
-                    const int nr = fill_round_local(g, ws, e, L, k, count, box, 0, lane, &next, &nh);
-                    if (!skip) walk_round_local(g, ws, nh, nr, r, sa_a, sa_b, s);
+                    const int nr = fill_round_local<ELL>(g, ws, e, L, k, count, box, 0, lane, &next, &nh);
+                    if (!skip) walk_round_local<ELL>(g, ws, nh, nr, r, sa_a, sa_b, s);
                     __syncwarp();
                     k = next;
                 }

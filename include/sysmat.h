@@ -55,9 +55,9 @@ extern "C" {
  * ray) are formed in double once per element, hole chords are y-extents in the hole's own
  * frame, the septal length is (T - sum of extents) / cos, crystal and self-attenuation chords
  * are measured from the sub-element, and the sub-element contributions are summed with
- * compensated (Neumaier) summation.  No reference counterpart.  Taken by sysmat_pe and
- * sysmat_pe_csr_file, for circular holes (a context with elliptical hole shapes returns
- * SYSMAT_ERR_ARG). */
+ * compensated (Neumaier) summation; an elliptical hole's extent is the unit circle's in its
+ * frame scaled by the semi-axes.  No reference counterpart.  Taken by sysmat_pe,
+ * sysmat_pe_sampled_mode and sysmat_pe_csr_file. */
 #define SYSMAT_MODE_LOCAL 3
 
 /* Scatter parts (bit mask) and collimator solid-angle models. */
@@ -142,8 +142,7 @@ SYSMAT_API int sysmat_pe_sampled(sysmat_ctx* ctx, float rotation, int det_begin,
 /* The sampled form in a chosen arithmetic: SYSMAT_MODE_PRECISE (the reference's float program,
  * exactly what sysmat_pe_sampled computes) or SYSMAT_MODE_LOCAL (the local-coordinate FP32 form
  * of SYSMAT_MODE_LOCAL at each source point, contributions summed with compensation: within 1e-5
- * of the sampled form's FP64 evaluation; circular holes only).  Other arguments and errors as
- * sysmat_pe_sampled. */
+ * of the sampled form's FP64 evaluation).  Other arguments and errors as sysmat_pe_sampled. */
 SYSMAT_API int sysmat_pe_sampled_mode(sysmat_ctx* ctx, float rotation, int det_begin, int det_count,
                                       long long vox_begin, long long vox_count, const int* crystal_div,
                                       const int* voxel_sub, int mode, float* d_out, long long ld, void* stream);

@@ -55,7 +55,7 @@ def lib():
         L.oracle_pe_local.argtypes = [_fp, _fp, _fp, _ip, ctypes.c_int, ctypes.c_longlong, ctypes.c_longlong, _dp,
                                       ctypes.c_int]
         L.oracle_pe_local.restype = ctypes.c_int
-        L.oracle_pe_local_sampled.argtypes = [_fp, _fp, _fp, _ip, _ip, _ip, ctypes.c_int, ctypes.c_longlong,
+        L.oracle_pe_local_sampled.argtypes = [_fp, _fp, _fp, _fp, _ip, _ip, _ip, ctypes.c_int, ctypes.c_longlong,
                                               ctypes.c_longlong, _dp, ctypes.c_int]
         L.oracle_pe_local_sampled.restype = ctypes.c_int
         L.oracle_pe_subelements.argtypes = [_fp, _fp, _fp, ctypes.c_int, ctypes.c_int, ctypes.c_longlong, _dp]
@@ -111,10 +111,10 @@ def pe(geo, prec=64, dets=None, v0=0, nv=None, threads=0, counts=False, shapes=N
     return (out, cnt) if counts else out
 
 
-def pe_local(geo, dets=None, v0=0, nv=None, threads=0, crystal_div=(8, 16, 8), voxel_sub=(1, 1, 1)):
+def pe_local(geo, dets=None, v0=0, nv=None, threads=0, crystal_div=(8, 16, 8), voxel_sub=(1, 1, 1), shapes=None):
     """PE elements (len(dets), nv) of the local-coordinate FP32 form (oracle_local.h) with the
     given crystal division and voxel source points (the element is the mean over the source
-    points), as float values widened to float64."""
+    points), as float values widened to float64.  shapes: optional elliptical holes, as in pe."""
     nv = geo.n_vox - v0 if nv is None else nv
     c, pc = _f32(geo.collimator)
     d, pd = _f32(geo.detector)
@@ -123,8 +123,11 @@ def pe_local(geo, dets=None, v0=0, nv=None, threads=0, crystal_div=(8, 16, 8), v
     dv = np.ascontiguousarray(crystal_div, dtype=np.int32)
     sv = np.ascontiguousarray(voxel_sub, dtype=np.int32)
     out = np.zeros((dd.size, nv), dtype=np.float64)
-    rc = lib().oracle_pe_local_sampled(pc, pd, pi, dv.ctypes.data_as(_ip), sv.ctypes.data_as(_ip), pdd, dd.size,
-                                       v0, nv, out.ctypes.data_as(_dp), threads)
+    psh = None
+    if shapes is not None:
+        sh, psh = _f32(np.asarray(shapes, dtype=np.float32).reshape(-1))
+    rc = lib().oracle_pe_local_sampled(pc, pd, pi, psh, dv.ctypes.data_as(_ip), sv.ctypes.data_as(_ip), pdd,
+                                       dd.size, v0, nv, out.ctypes.data_as(_dp), threads)
     if rc:
         raise RuntimeError(f"oracle_pe_local_sampled failed ({rc})")
     return out

@@ -27,6 +27,8 @@ typedef struct {
     float dy;         /* y1 - yI */
     float th;         /* y2 - y1 */
     float r, mu;
+    float ex, ez;     /* semi-axes of an elliptical hole (ex = 0: circle) */
+    float ct, st;     /* cos, sin of its angle (double of the float angle, rounded once) */
 } lhole;
 
 typedef struct {
@@ -106,7 +108,7 @@ static float box_chord_near_f(const float P[3], const float q[3], const float lo
  * in double: near a tangent, and for a hole met far from where the ray enters the plate, the
  * chord is ill-conditioned in them. */
 static float hole_extent_f(double u0d, double w0d, double rxd, double rzd, double ad, double iad, float r, float th,
-                           float dy, float sec, float tio, float ky)
+                           float dy, float sec, float tio, float ky, double tq)
 {
     if (fabsf(th) < 0.001f) return 0;
     const double u1d = u0d + rxd * (double)th, w1d = w0d + rzd * (double)th;
@@ -121,7 +123,7 @@ static float hole_extent_f(double u0d, double w0d, double rxd, double rzd, doubl
     }
     const double cross = u0d * rzd - w0d * rxd;
     const double qd = ad * r2 - cross * cross;          /* b^2 - a c (Lagrange identity) */
-    if ((double)(ky * ky) * qd <= (double)0.00001f) return 0;   /* the reference's discriminant */
+    if ((double)(ky * ky) * tq * qd <= (double)0.00001f) return 0;   /* the reference's discriminant */
     const double bd = u0d * rxd + w0d * rzd;
     const double sq = (double)sqrtf((float)qd);
     const double s1 = (-bd - sq) * iad, s2 = (-bd + sq) * iad;
@@ -198,6 +200,16 @@ static float pe_element_local(const ogeo* g, int d, double xI, double yI, double
                 e->th = (float)(hy2 - hy1);
                 e->r = (float)hr;
                 e->mu = (float)C[hid * 9 + 105];
+                e->ex = 0;
+                e->ez = 0;
+                e->ct = 1;
+                e->st = 0;
+                if (g->S && g->S[3 * hid] > 0.0f) {            /* elliptical hole (extension) */
+                    e->ex = g->S[3 * hid];
+                    e->ez = g->S[3 * hid + 1];
+                    e->ct = (float)cos((double)g->S[3 * hid + 2]);
+                    e->st = (float)sin((double)g->S[3 * hid + 2]);
+                }
                 cand_h[hoff + n++] = hid;
             }
         }
@@ -264,8 +276,25 @@ static float pe_element_local(const ogeo* g, int d, double xI, double yI, double
             float ext = 0, hatt = 0;
             for (int j = 0; j < ncand_h[m]; ++j) {
                 const lhole* e = &lh[hoff + j];
-                const double u0 = e->hx + ddrx * (double)e->dy, w0 = e->hz + ddrz * (double)e->dy;
-                const float s = hole_extent_f(u0, w0, rxd, rzd, ad, iad, e->r, e->th, e->dy, sec, sq, ky);
+                double u0 = e->hx + ddrx * (double)e->dy, w0 = e->hz + ddrz * (double)e->dy;
+                double rx = rxd, rz = rzd, a = ad, ia = iad, tq = 1.0;
+                float rad = e->r;
+                if (e->ex > 0.0f) {
+                    /* elliptical: the ray's offset and slopes turned into the hole's frame and
+                     * divided by the semi-axes (the unit circle); the reference's discriminant
+                     * b^2 - a c is rho_x^4 rho_z^4 ky^2 times the unit circle's */
+                    const double c = (double)e->ct, sn = (double)e->st;
+                    const double iex = 1.0 / (double)e->ex, iez = 1.0 / (double)e->ez;
+                    const double p = (u0 * c + w0 * sn) * iex, q = (-u0 * sn + w0 * c) * iez;
+                    const double al = (rxd * c + rzd * sn) * iex, be = (-rxd * sn + rzd * c) * iez;
+                    u0 = p; w0 = q; rx = al; rz = be;
+                    a = al * al + be * be;
+                    ia = 1.0 / a;
+                    rad = 1.0f;
+                    const double e2 = (double)e->ex * (double)e->ex * (double)e->ez * (double)e->ez;
+                    tq = e2 * e2;
+                }
+                const float s = hole_extent_f(u0, w0, rx, rz, a, ia, rad, e->th, e->dy, sec, sq, ky, tq);
                 ext = ext + s;
                 hatt = hatt + e->mu * s;
             }

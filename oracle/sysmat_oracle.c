@@ -184,12 +184,15 @@ int oracle_pe_sampled(const float* C, const float* D, const float* I, const floa
 
 /* PE elements of the local-coordinate FP32 form (oracle_local.h) with div[3] crystal
  * sub-elements along x, depth, z and vsub[3] source points per voxel along x, y, z (the element
- * is the mean over the source points, in double), as float values widened to double. */
-int oracle_pe_local_sampled(const float* C, const float* D, const float* I, const int* div, const int* vsub,
-                            const int* dets, int ndet, long long v0, long long nv, double* out, int nthreads)
+ * is the mean over the source points, in double), as float values widened to double.  S:
+ * optional hole shapes (rho_x, rho_z, theta per hole; NULL: every hole circular). */
+int oracle_pe_local_sampled(const float* C, const float* D, const float* I, const float* S, const int* div,
+                            const int* vsub, const int* dets, int ndet, long long v0, long long nv, double* out,
+                            int nthreads)
 {
     ogeo g;
     if (parse(&g, C, D, I, NULL)) return -1;
+    g.S = S;
     for (int k = 0; k < 3; ++k) {
         if (div[k] < 1 || vsub[k] < 1) return -1;
         g.div[k] = div[k];
@@ -236,7 +239,7 @@ int oracle_pe_local(const float* C, const float* D, const float* I, const int* d
                     long long nv, double* out, int nthreads)
 {
     const int div[3] = {8, 16, 8}, vsub[3] = {1, 1, 1};
-    return oracle_pe_local_sampled(C, D, I, div, vsub, dets, ndet, v0, nv, out, nthreads);
+    return oracle_pe_local_sampled(C, D, I, NULL, div, vsub, dets, ndet, v0, nv, out, nthreads);
 }
 
 /* Elements of the grid scatter model (oracle_grid.h) for detectors dets[0..ndet) and voxels

@@ -118,16 +118,40 @@ def test_local_blocks_equal_the_full_matrix(gpu):
         assert np.all(blk[:, nv:] == -1.0)
 
 
-def test_local_mode_rejects_elliptical_holes(gpu):
+def _elliptical(seed):
+    geo = geometry.mini(seed=seed, rotated=True, layers=2, n_rot=8, nvox=(6, 5, 3), ncry=(5, 4)).with_rotation(2)
+    H = geo.n_holes
+    rng = np.random.default_rng(seed)
+    r = geo.collimator[100:100 + 9 * H].reshape(H, 9)[:, 4].astype(np.float64)
+    shapes = np.stack([r * rng.uniform(0.5, 1.0, H), r * rng.uniform(0.5, 1.0, H),
+                       rng.uniform(0.0, np.pi, H)], 1).astype(np.float32)
+    shapes[rng.random(H) < 0.2, 0] = 0.0                 # some holes stay circular
+    return geo, shapes
+
+
+@pytest.mark.parametrize("seed", [51, 52])
+def test_local_mode_with_elliptical_holes_within_1e5_of_fp64(gpu, seed):
+    """Elliptical holes in the local arithmetic (the unit circle in each hole's turned, scaled
+    frame): within 1e-5 of FP64, where the reference's float elliptical chord (ill-conditioned
+    in b^2 - a c) is up to ~1e-4 away on many elements; at the reference's sampling and at
+    configuration 2's."""
     torch = gpu
-    geo, _ = golden("mini0")
+    geo, shapes = _elliptical(seed)
     ctx = sysmat.Context(geo)
-    shapes = np.zeros((geo.n_holes, 3), dtype=np.float32)
-    shapes[0] = (0.4, 0.3, 0.5)
     ctx.set_hole_shapes(shapes)
-    out = torch.empty((ctx.n_det, ctx.n_vox), dtype=torch.float32, device="cuda")
-    with pytest.raises(sysmat.SysmatError):
-        ctx.pe(out, mode=sysmat.MODE_LOCAL)
+    a = _local(torch, ctx, rotation=2.0)
+    o64 = oracle.pe(geo, prec=64, shapes=shapes)
+    r = rel_err(a, o64)
+    assert a.max() > 0 and r.max() <= TOL and np.median(r) < 1e-6, (r.max(), np.median(r))
+    assert r.max() < rel_err(oracle.pe(geo, prec=32, shapes=shapes), o64).max()
+    assert np.median(rel_err(a, oracle.pe_local(geo, shapes=shapes))) < 1e-6
+    b = _local_sampled(torch, ctx, (2, 8, 2), (2, 2, 2), rotation=2.0)
+    s64 = oracle.pe_sampled(geo, (2, 8, 2), (2, 2, 2), prec=64, shapes=shapes)
+    rs = rel_err(b, s64)
+    n = within_knife_edge(b, geo, lambda g: oracle.pe_sampled(g, (2, 8, 2), (2, 2, 2), prec=64, shapes=shapes), rs)
+    assert np.median(rs) < 1e-6 and n <= 0.005 * rs.size, (np.median(rs), n)
+    ctx.set_hole_shapes(None)                            # back to circles: the circular instance
+    assert np.array_equal(_local(torch, ctx, rotation=2.0), _local(torch, sysmat.Context(geo), rotation=2.0))
 
 
 def _local_sampled(torch, ctx, div, sub, rotation=0.0, **blk):
@@ -198,7 +222,7 @@ def test_local_sampled_blocks_equal_the_full_matrix(gpu):
         assert np.array_equal(blk, full[d0:d0 + nd, v0:v0 + nv])
 
 
-def test_local_sampled_rejects_other_modes_and_elliptical_holes(gpu):
+def test_local_sampled_rejects_other_modes(gpu):
     torch = gpu
     geo, _ = golden("mini0")
     ctx = sysmat.Context(geo)
@@ -206,11 +230,3 @@ def test_local_sampled_rejects_other_modes_and_elliptical_holes(gpu):
     for mode in (sysmat.MODE_REFERENCE, sysmat.MODE_FP64, 7):
         with pytest.raises(sysmat.SysmatError):
             ctx.pe_sampled(out, (2, 8, 2), (2, 2, 2), mode=mode)
-    shapes = np.zeros((geo.n_holes, 3), dtype=np.float32)
-    shapes[0] = (0.4, 0.3, 0.5)
-    ctx.set_hole_shapes(shapes)
-    with pytest.raises(sysmat.SysmatError):
-        ctx.pe_sampled(out, (2, 8, 2), (2, 2, 2), mode=sysmat.MODE_LOCAL)
-    ctx.pe_sampled(out, (2, 8, 2), (2, 2, 2), mode=sysmat.MODE_PRECISE)     # the float form takes them
-    torch.cuda.synchronize()
-    assert out.max().item() > 0

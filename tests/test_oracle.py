@@ -371,3 +371,24 @@ def test_local_sampled_twin_within_1e5_of_fp64_sampled(div, sub):
     assert n <= 0.005 * r.size, n
     assert r.max() < rel_err(oracle.pe_sampled(geo, div, sub, prec=32), o64).max()
     assert np.array_equal(oracle.pe_local(geo), oracle.pe_local(geo, crystal_div=(8, 16, 8), voxel_sub=(1, 1, 1)))
+
+
+@pytest.mark.parametrize("seed", [51, 52])
+def test_local_twin_with_elliptical_holes_within_1e5_of_fp64(seed):
+    """The local twin with elliptical holes (some circular): within 1e-5 of FP64 at the
+    reference's sampling and at configuration 2's, where the float program's elliptical chord
+    is up to ~1e-4 away."""
+    geo = geometry.mini(seed=seed, rotated=True, layers=2, n_rot=8, nvox=(6, 5, 3), ncry=(5, 4)).with_rotation(2)
+    H = geo.n_holes
+    rng = np.random.default_rng(seed)
+    rr = geo.collimator[100:100 + 9 * H].reshape(H, 9)[:, 4].astype(np.float64)
+    shapes = np.stack([rr * rng.uniform(0.5, 1.0, H), rr * rng.uniform(0.5, 1.0, H),
+                       rng.uniform(0.0, np.pi, H)], 1).astype(np.float32)
+    shapes[rng.random(H) < 0.2, 0] = 0.0
+    o64 = oracle.pe(geo, prec=64, shapes=shapes)
+    r = rel_err(oracle.pe_local(geo, shapes=shapes), o64)
+    assert r.max() <= 1e-5 and np.median(r) < 1e-6, (r.max(), np.median(r))
+    assert rel_err(oracle.pe(geo, prec=32, shapes=shapes), o64).max() > 1e-5
+    s64 = oracle.pe_sampled(geo, (2, 8, 2), (2, 2, 2), prec=64, shapes=shapes)
+    rs = rel_err(oracle.pe_local(geo, shapes=shapes, crystal_div=(2, 8, 2), voxel_sub=(2, 2, 2)), s64)
+    assert rs.max() <= 1e-5, rs.max()
