@@ -980,7 +980,7 @@ __device__ __forceinline__ void pe_brick(const DevGeom& g, BlockSmem& bs, WarpSm
             float* so = nullptr;
             if (SAMPLED && O.sub_out)
                 so = O.sub_out + ((v - O.vox_begin) * O.det_count + di) * (long long)(smp->nx * smp->ny * smp->nz);
-            val = (float)pe_element_local<ELL>(g, bs, ws, d, v, cr, sr, rotation, lane, SAMPLED ? smp : nullptr, so);
+            val = (float)pe_element_local<ELL, SAMPLED>(g, bs, ws, d, v, cr, sr, rotation, lane, smp, so);
         } else if constexpr (SAMPLED) val = (float)pe_element_sampled<ELL>(g, bs, ws, d, v, cr, sr, lane, *smp);
         else if constexpr (MODE == 2) val = (float)pe_element64(g, bs, ws, d, v, cr, sr, rotation, lane);
         else val = (float)pe_element<MODE, COUNT, ELL>(g, bs, ws, d, v, cr, sr, lane, counters);

@@ -474,16 +474,17 @@ __device__ __forceinline__ void neumaier_add(float& s, float& c, float x)
 // reference-order kernel; other divisions go 32 to a round in (z, depth, x) order, x fastest.
 // sub_out (one source point only): each sub-element's contribution is also written there, at
 // index (iz * ny + iy) * nx + ix (the scatter grid's crystal-cell weights).
-template <bool ELL>
+template <bool ELL, bool SMP>
 __device__ double pe_element_local(const DevGeom& g, const BlockSmem& bs, WarpSmem& ws, int d, long long v, float cr,
                                    float sr, float rotation, int lane, const Sampling* smp = nullptr,
                                    float* sub_out = nullptr)
 {
     static_assert(sizeof(ElemL) <= sizeof(ws.chain), "ElemL exceeds its shared-memory slot");
     ElemL& L = *reinterpret_cast<ElemL*>(ws.chain);
-    const int nx = smp ? smp->nx : 8, ny = smp ? smp->ny : 16, nz = smp ? smp->nz : 8;
+    if constexpr (!SMP) smp = nullptr;               // the reference's sampling: constants below
+    const int nx = SMP ? smp->nx : 8, ny = SMP ? smp->ny : 16, nz = SMP ? smp->nz : 8;
     const int n_sub = nx * ny * nz, nxy = nx * ny;
-    const int sxn = smp ? smp->sx : 1, syn = smp ? smp->sy : 1, szn = smp ? smp->sz : 1;
+    const int sxn = SMP ? smp->sx : 1, syn = SMP ? smp->sy : 1, szn = SMP ? smp->sz : 1;
     const int n_pts = sxn * syn * szn;
     float sum = 0.0f, comp = 0.0f;
     for (int src = 0; src < n_pts; ++src) {
@@ -510,7 +511,7 @@ __device__ double pe_element_local(const DevGeom& g, const BlockSmem& bs, WarpSm
         for (int base = 0; base < n_sub; base += 32) {
             const bool dead = base + lane >= n_sub;
             int sidx, ix, iy, iz;
-            if (!smp) {                       // s = 128 iz + 16 ix + iy, as in pe_element's rounds
+            if constexpr (!SMP) {             // s = 128 iz + 16 ix + iy, as in pe_element's rounds
                 const int rr = base >> 5;
                 const int s = ((rr >> 3) * 2 + (lane >> 4)) * 128 + ((lane >> 1) & 7) * 16 + (rr & 7) * 2 + (lane & 1);
                 iz = s >> 7;
