@@ -40,7 +40,7 @@ struct sysmat_batch_plan {
     unsigned long long* d_counter = nullptr;
     BatchLaunch launch{};                  // current task table
     cudaStream_t capture = nullptr;
-    cudaGraphExec_t exec[3] = {nullptr, nullptr, nullptr};   // one graph per mode
+    cudaGraphExec_t exec[4] = {nullptr, nullptr, nullptr, nullptr};   // one graph per mode
 };
 
 namespace {
@@ -203,7 +203,8 @@ extern "C" SYSMAT_API int sysmat_batch_get_tiles(const sysmat_batch_plan* p, int
 
 bool plan_mode_ok(const sysmat_batch_plan*, int mode)
 {
-    return mode == SYSMAT_MODE_REFERENCE || mode == SYSMAT_MODE_PRECISE || mode == SYSMAT_MODE_FP64;
+    return mode == SYSMAT_MODE_REFERENCE || mode == SYSMAT_MODE_PRECISE || mode == SYSMAT_MODE_FP64 ||
+           mode == SYSMAT_MODE_LOCAL;
 }
 
 extern "C" SYSMAT_API int sysmat_batch_run(sysmat_batch_plan* p, int mode, void* stream)
@@ -300,7 +301,8 @@ extern "C" SYSMAT_API int sysmat_batch_tune(sysmat_batch_plan* p, int mode, void
 extern "C" SYSMAT_API int sysmat_batch(sysmat_ctx* const* ctxs, int n_ctx, const sysmat_batch_item* items,
                                        int n_items, int mode, void* stream)
 {
-    if (mode != SYSMAT_MODE_REFERENCE && mode != SYSMAT_MODE_PRECISE && mode != SYSMAT_MODE_FP64)
+    if (mode != SYSMAT_MODE_REFERENCE && mode != SYSMAT_MODE_PRECISE && mode != SYSMAT_MODE_FP64 &&
+        mode != SYSMAT_MODE_LOCAL)
         return SYSMAT_ERR_ARG;
     sysmat_batch_plan* p = nullptr;
     int rc = sysmat_batch_create(&p, ctxs, n_ctx, items, n_items);

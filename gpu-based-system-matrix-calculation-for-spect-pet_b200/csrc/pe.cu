@@ -1168,6 +1168,7 @@ static int configure_batch_mode(int* per_sm)
 int configure_pe_batch(int mode, bool ell, int* blocks_per_sm)
 {
     if (mode == 2) return configure_batch_mode<2, false>(blocks_per_sm);   // shapes read at run time
+    if (mode == 3) return ell ? configure_batch_mode<3, true>(blocks_per_sm) : configure_batch_mode<3, false>(blocks_per_sm);
     if (ell) {
         return mode == 0 ? configure_batch_mode<0, true>(blocks_per_sm)
                          : configure_batch_mode<1, true>(blocks_per_sm);
@@ -1181,6 +1182,9 @@ int launch_pe_batch(const BatchLaunch& B, int mode, bool ell, int grid, cudaStre
     const int smem = (int)sizeof(BatchSmem);
     if (mode == 2) {                              // FP64: shapes read at run time
         pe_batch_kernel<2, false><<<grid, kThreads, smem, stream>>>(B);
+    } else if (mode == 3) {
+        if (ell) pe_batch_kernel<3, true><<<grid, kThreads, smem, stream>>>(B);
+        else pe_batch_kernel<3, false><<<grid, kThreads, smem, stream>>>(B);
     } else if (ell) {
         if (mode == 0) pe_batch_kernel<0, true><<<grid, kThreads, smem, stream>>>(B);
         else pe_batch_kernel<1, true><<<grid, kThreads, smem, stream>>>(B);

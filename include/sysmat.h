@@ -272,8 +272,9 @@ SYSMAT_API int sysmat_batch_get_tiles(const sysmat_batch_plan* plan, int* tiles)
 /* Time candidate bricks on a probe subset of the batch (synchronises `stream`), keep the
  * fastest and return it in tiles[4] (may be NULL). */
 SYSMAT_API int sysmat_batch_tune(sysmat_batch_plan* plan, int mode, void* stream, int* tiles);
-/* Run the whole batch on `stream` (asynchronous).  The first run per mode captures the
- * launch into a CUDA graph on a plan-owned stream; later runs replay it. */
+/* Run the whole batch on `stream` (asynchronous) in `mode` (SYSMAT_MODE_REFERENCE, _PRECISE,
+ * _FP64 or _LOCAL; every element equals sysmat_pe's in that mode).  The first run per mode
+ * captures the launch into a CUDA graph on a plan-owned stream; later runs replay it. */
 SYSMAT_API int sysmat_batch_run(sysmat_batch_plan* plan, int mode, void* stream);
 SYSMAT_API int sysmat_batch_destroy(sysmat_batch_plan* plan);
 /* One-shot: create, run once without a graph, synchronise `stream`, destroy. */

@@ -107,6 +107,30 @@ def test_config4_instances_sample(gpu):
     assert all(e.max() > 0 for e in exp)
 
 
+@pytest.mark.parametrize("mode", [sysmat.MODE_LOCAL, sysmat.MODE_FP64])
+def test_batch_precision_modes_equal_single_calls(gpu, mode):
+    """The FP64 and local FP32 forms in a batch, a system with elliptical holes among them:
+    every element equals the per-task sysmat_pe element in the same mode bit for bit."""
+    torch = gpu
+    systems = _systems()
+    ell = geometry.mini(seed=57, rotated=True, layers=2, n_rot=8, nvox=(6, 5, 3), ncry=(5, 4))
+    H = ell.n_holes
+    r = ell.collimator[100:100 + 9 * H].reshape(H, 9)[:, 4]
+    shapes = np.stack([0.8 * r, 0.6 * r, np.linspace(0.1, 3.0, H)], 1).astype(np.float32)
+    ctxs = [sysmat.Context(g) for g in systems[:2]] + [sysmat.Context(ell)]
+    ctxs[2].set_hole_shapes(shapes)
+    tasks = [(0, 3.0, 2, 7, 11, 61), (1, 1.0, 0, ctxs[1].n_det, 5, 40), (2, 5.0, 0, ctxs[2].n_det, 0, ctxs[2].n_vox),
+             (2, 2.0, 19, 1, 89, 1)]
+    exp = _expected(torch, ctxs, tasks, mode=mode)
+    outs = _alloc(torch, tasks)
+    plan = sysmat.BatchPlan(ctxs, [t + (o[:, :t[5]],) for t, o in zip(tasks, outs)])
+    for _ in range(2):                                  # captured run, then a replay
+        plan.run(mode=mode)
+        torch.cuda.synchronize()
+        _check(outs, exp, tasks)
+    assert all(e.max() > 0 for e in exp)
+
+
 def test_batch_matches_reference_on_config4_goldens(gpu):
     """Two configuration-4 designs at one of their rotations (the reference's own PESysMatGen
     output on voxel row 16 of z-plane 8), computed together in one batch."""
