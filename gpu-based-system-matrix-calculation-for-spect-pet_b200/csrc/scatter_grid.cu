@@ -278,8 +278,11 @@ __device__ double seg_box64(const double A[3], const double B[3], const double l
 }
 
 // Length of segment A -> B inside the y-parallel cylinder (x - xc)^2 + (z - zc)^2 <= r^2,
-// y in [y1, y2] (exact overlap).
-__device__ double seg_cyl64(const double A[3], const double B[3], double xc, double zc, double y1, double y2, double r)
+// y in [y1, y2] (exact overlap).  S: an elliptical hole's (rho_x, rho_z, cos, sin) (S.x > 0), in
+// whose frame (u = dx cos + dz sin, w = -dx sin + dz cos, as the reference turns points),
+// divided by the semi-axes, the segment meets the unit circle over the same parameter range.
+__device__ double seg_cyl64(const double A[3], const double B[3], double xc, double zc, double y1, double y2, double r,
+                            const D4& S)
 {
     double t0 = 0.0, t1 = 1.0;
     const double dy = B[1] - A[1];
@@ -291,7 +294,14 @@ __device__ double seg_cyl64(const double A[3], const double B[3], double xc, dou
         t0 = fmax(t0, u);
         t1 = fmin(t1, v);
     }
-    const double dx = B[0] - A[0], dz = B[2] - A[2], ox = A[0] - xc, oz = A[2] - zc;
+    const double dx0 = B[0] - A[0], dz0 = B[2] - A[2];
+    double dx = dx0, dz = dz0, ox = A[0] - xc, oz = A[2] - zc;
+    if (S.x > 0.0) {
+        const double pdx = (dx * S.z + dz * S.w) / S.x, pdz = (-dx * S.w + dz * S.z) / S.y;
+        const double pox = (ox * S.z + oz * S.w) / S.x, poz = (-ox * S.w + oz * S.z) / S.y;
+        dx = pdx; dz = pdz; ox = pox; oz = poz;
+        r = 1.0;
+    }
     const double a = dx * dx + dz * dz, b = ox * dx + oz * dz, c = ox * ox + oz * oz - r * r;
     if (a == 0.0) {
         if (c > 0.0) return 0.0;
@@ -303,7 +313,7 @@ __device__ double seg_cyl64(const double A[3], const double B[3], double xc, dou
         t1 = fmin(t1, (-b + sq) / a);
     }
     if (t1 <= t0) return 0.0;
-    return (t1 - t0) * sqrt(a + dy * dy);
+    return (t1 - t0) * sqrt(dx0 * dx0 + dz0 * dz0 + dy * dy);
 }
 
 // Attenuation sums (mu_total, mu_pe, mu_C times length) of layer m along segment A -> B: its
@@ -326,7 +336,8 @@ __device__ void layer_path64(const DevGeom& g, const GridGeom& G, int m, const d
         const D4 a = g.t64.hole_a[j];
         const double r = g.t64.hole_b[j].x;
         if (hole_far(A[0], A[2], B[0], B[2], a.x, a.w, r)) continue;
-        const double l = seg_cyl64(A, B, a.x, a.w, a.y, a.z, r);
+        const D4 S = g.t64.hole_shape ? g.t64.hole_shape[j] : D4{0.0, 0.0, 1.0, 0.0};
+        const double l = seg_cyl64(A, B, a.x, a.w, a.y, a.z, r, S);
         if (l == 0.0) continue;
         const float* hp = G.raw_col + 100 + 9 * j;
         hsum += l;
@@ -386,7 +397,14 @@ __global__ void septal_mark_kernel(DevGeom g, GridLayer L, int n_cells, unsigned
         const D4 a = g.t64.hole_a[j];
         const double r = g.t64.hole_b[j].x;
         const double dx = x - a.x, dz = z - a.w;
-        if (dx * dx + dz * dz <= r * r && y >= a.y && y <= a.z) sep = 0;
+        if (!(y >= a.y && y <= a.z)) continue;
+        const D4 S = g.t64.hole_shape ? g.t64.hole_shape[j] : D4{0.0, 0.0, 1.0, 0.0};
+        if (S.x > 0.0) {                                    // elliptical hole
+            const double u = (dx * S.z + dz * S.w) / S.x, w = (-dx * S.w + dz * S.z) / S.y;
+            if (u * u + w * w <= 1.0) sep = 0;
+        } else if (dx * dx + dz * dz <= r * r) {
+            sep = 0;
+        }
     }
     flag[c] = sep;
 }
@@ -689,7 +707,6 @@ extern "C" SYSMAT_API int sysmat_scatter_grid(sysmat_ctx* ctx, int parts, float 
     if (parts < 1 || parts > 3 || !(cell > 0.0f)) return SYSMAT_ERR_ARG;
     if (ctx->h_phys.size() != (size_t)kNPhysics || ctx->h_det.size() != (size_t)kNDetector) return SYSMAT_ERR_ARG;
     if ((parts & 2) && ctx->g.n_layers < 1) return SYSMAT_ERR_ARG;
-    if (ctx->g.hole_shape) return SYSMAT_ERR_ARG;               // circular holes only
     if (det_count == 0 || vox_count == 0) return SYSMAT_OK;
     cudaStream_t s = (cudaStream_t)stream;
     const DevGeom& g = ctx->g;

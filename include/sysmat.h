@@ -182,9 +182,10 @@ SYSMAT_API int sysmat_scatter_prepare_native(sysmat_ctx* ctx, int parts, const u
  * exp(-attenuation to the cell) mu_C).  Each item is the reference's scatter item with that
  * scatter point, every crystal on the way (and the tungsten, for septal points) as
  * attenuator at the scattered energy, and the exact Klein-Nishina fraction; each element
- * sums its ~10^6 items in FP64.  Every crystal must have the same cell division; circular
- * holes only.  Needs no PE matrix or bitmaps.  Synchronous on `stream` (it allocates and
- * frees its scratch). */
+ * sums its ~10^6 items in FP64.  Every crystal must have the same cell division.  Elliptical
+ * holes (sysmat_set_hole_shapes) bound the septal cells and the hole media by their ellipses.
+ * Needs no PE matrix or bitmaps.  Synchronous on `stream` (it allocates and frees its
+ * scratch). */
 /* Batched scatter (no reference counterpart; the reference computes one geometry per call,
  * scatter.cu:2169-2194, :2303-2329): many scatter tasks, each what one sysmat_scatter call
  * takes, in one persistent launch over a work queue, replayed as a CUDA graph.  Every element

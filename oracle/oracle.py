@@ -60,7 +60,7 @@ def lib():
         L.oracle_pe_local_sampled.restype = ctypes.c_int
         L.oracle_pe_subelements.argtypes = [_fp, _fp, _fp, ctypes.c_int, ctypes.c_int, ctypes.c_longlong, _dp]
         L.oracle_pe_subelements.restype = ctypes.c_int
-        L.oracle_scatter_grid.argtypes = [_fp, _fp, _fp, _fp, ctypes.c_int, ctypes.c_double, _ip, ctypes.c_int,
+        L.oracle_scatter_grid.argtypes = [_fp, _fp, _fp, _fp, _fp, ctypes.c_int, ctypes.c_double, _ip, ctypes.c_int,
                                           ctypes.c_longlong, ctypes.c_longlong, _dp, ctypes.c_int]
         L.oracle_scatter_grid.restype = ctypes.c_int
         for name in ("oracle_box_chord", "oracle_box_chord_inside", "oracle_cyl_chord", "oracle_ell_chord"):
@@ -214,9 +214,10 @@ def pe_subelements(geo, d, v, which=64):
     return out
 
 
-def scatter_grid(geo, parts=3, cell=0.25, dets=None, v0=0, nv=None, threads=0):
+def scatter_grid(geo, parts=3, cell=0.25, dets=None, v0=0, nv=None, threads=0, shapes=None):
     """Elements (len(dets), nv) of the grid scatter model (oracle_grid.h) in double: parts 1 =
-    crystal cells, 2 = septal cells; cell = grid step in mm."""
+    crystal cells, 2 = septal cells; cell = grid step in mm; shapes: optional elliptical holes,
+    as in pe."""
     nv = geo.n_vox - v0 if nv is None else nv
     c, pc = _f32(geo.collimator)
     d, pd = _f32(geo.detector)
@@ -224,7 +225,10 @@ def scatter_grid(geo, parts=3, cell=0.25, dets=None, v0=0, nv=None, threads=0):
     p, pp = _f32(geo.physics)
     dd, pdd = _dets(geo, dets)
     out = np.zeros((dd.size, nv), dtype=np.float64)
-    rc = lib().oracle_scatter_grid(pc, pd, pi, pp, int(parts), float(cell), pdd, dd.size, v0, nv,
+    psh = None
+    if shapes is not None:
+        sh, psh = _f32(np.asarray(shapes, dtype=np.float32).reshape(-1))
+    rc = lib().oracle_scatter_grid(pc, pd, pi, pp, psh, int(parts), float(cell), pdd, dd.size, v0, nv,
                                    out.ctypes.data_as(_dp), threads)
     if rc:
         raise RuntimeError(f"oracle_scatter_grid failed ({rc})")

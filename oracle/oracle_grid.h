@@ -70,9 +70,24 @@ static double seg_box(const double A[3], const double B[3], const double lo[3], 
     return (t1 - t0) * len;
 }
 
+/* Elliptical hole j (g->S, an extension): semi-axes and cos, sin of its angle in double. */
+static int grid_ellipse(const ogeo* g, int j, double* ex, double* ez, double* c, double* s)
+{
+    if (!g->S || !(g->S[3 * j] > 0.0f)) return 0;
+    *ex = (double)g->S[3 * j];
+    *ez = (double)g->S[3 * j + 1];
+    *c = cos((double)g->S[3 * j + 2]);
+    *s = sin((double)g->S[3 * j + 2]);
+    return 1;
+}
+
 /* Length of segment A -> B inside the y-parallel cylinder (x - xc)^2 + (z - zc)^2 <= r^2,
- * y in [y1, y2] (exact overlap). */
-static double seg_cyl(const double A[3], const double B[3], double xc, double zc, double y1, double y2, double r)
+ * y in [y1, y2] (exact overlap); with ell, inside the elliptical cylinder of semi-axes ex, ez
+ * in the hole's frame turned by (c, s) (u = dx c + dz s, w = -dx s + dz c, as the reference
+ * turns points): the segment's offsets mapped to that frame and divided by the semi-axes meet
+ * the unit circle over the same parameter range. */
+static double seg_cyl_shape(const double A[3], const double B[3], double xc, double zc, double y1, double y2,
+                            double r, int ell, double ex, double ez, double c, double s)
 {
     double t0 = 0, t1 = 1;
     const double dy = B[1] - A[1];
@@ -84,12 +99,18 @@ static double seg_cyl(const double A[3], const double B[3], double xc, double zc
         if (u > t0) t0 = u;
         if (v < t1) t1 = v;
     }
-    const double dx = B[0] - A[0], dz = B[2] - A[2], ox = A[0] - xc, oz = A[2] - zc;
-    const double a = dx * dx + dz * dz, b = ox * dx + oz * dz, c = ox * ox + oz * oz - r * r;
+    const double dx0 = B[0] - A[0], dz0 = B[2] - A[2];
+    double dx = dx0, dz = dz0, ox = A[0] - xc, oz = A[2] - zc;
+    if (ell) {
+        const double pdx = (dx * c + dz * s) / ex, pdz = (-dx * s + dz * c) / ez;
+        const double pox = (ox * c + oz * s) / ex, poz = (-ox * s + oz * c) / ez;
+        dx = pdx; dz = pdz; ox = pox; oz = poz; r = 1.0;
+    }
+    const double a = dx * dx + dz * dz, b = ox * dx + oz * dz, cc = ox * ox + oz * oz - r * r;
     if (a == 0) {
-        if (c > 0) return 0;
+        if (cc > 0) return 0;
     } else {
-        const double disc = b * b - a * c;
+        const double disc = b * b - a * cc;
         if (disc <= 0) return 0;
         const double sq = sqrt(disc);
         const double u = (-b - sq) / a, v = (-b + sq) / a;
@@ -97,7 +118,12 @@ static double seg_cyl(const double A[3], const double B[3], double xc, double zc
         if (v < t1) t1 = v;
     }
     if (t1 <= t0) return 0;
-    return (t1 - t0) * sqrt(a + dy * dy);
+    return (t1 - t0) * sqrt(dx0 * dx0 + dz0 * dz0 + dy * dy);
+}
+
+static double seg_cyl(const double A[3], const double B[3], double xc, double zc, double y1, double y2, double r)
+{
+    return seg_cyl_shape(A, B, xc, zc, y1, y2, r, 0, 1, 1, 1, 0);
 }
 
 static void grid_plate_box(const ogeo* g, int m, double b[6])
@@ -133,8 +159,10 @@ static void grid_layer_path(const ogeo* g, int m, int hole_begin, const double A
         t = t < 0 ? 0 : (t > 1 ? 1 : t);
         const double dx = A[0] + t * ex - (double)h[0], dz = A[2] + t * ez - (double)h[3];
         if (dx * dx + dz * dz > ((double)h[4] + 1e-6) * ((double)h[4] + 1e-6)) continue;
-        const double l = seg_cyl(A, B, (double)h[0], (double)h[3], (double)h[1] + fov, (double)h[2] + fov,
-                                 (double)h[4]);
+        double ex = 1, ez = 1, c = 1, s = 0;
+        const int ell = grid_ellipse(g, j, &ex, &ez, &c, &s);
+        const double l = seg_cyl_shape(A, B, (double)h[0], (double)h[3], (double)h[1] + fov, (double)h[2] + fov,
+                                       (double)h[4], ell, ex, ez, c, s);
         if (l == 0) continue;
         hsum += l;
         *wt += (double)h[5] * l;
@@ -270,7 +298,14 @@ static int grid_in_hole(const ogeo* g, int hole_begin, int m, const double p[3])
     for (int j = hole_begin; j < hole_begin + g->nh[m]; ++j) {
         const float* h = C + 100 + 9 * j;
         const double dx = p[0] - (double)h[0], dz = p[2] - (double)h[3], r = (double)h[4];
-        if (dx * dx + dz * dz <= r * r && p[1] >= (double)h[1] + fov && p[1] <= (double)h[2] + fov) return 1;
+        if (!(p[1] >= (double)h[1] + fov && p[1] <= (double)h[2] + fov)) continue;
+        double ex, ez, c, s;
+        if (grid_ellipse(g, j, &ex, &ez, &c, &s)) {
+            const double u = (dx * c + dz * s) / ex, w = (-dx * s + dz * c) / ez;
+            if (u * u + w * w <= 1.0) return 1;
+        } else if (dx * dx + dz * dz <= r * r) {
+            return 1;
+        }
     }
     return 0;
 }

@@ -243,13 +243,15 @@ int oracle_pe_local(const float* C, const float* D, const float* I, const int* d
 }
 
 /* Elements of the grid scatter model (oracle_grid.h) for detectors dets[0..ndet) and voxels
- * [v0, v0+nv), in double; parts: 1 crystal cells, 2 septal cells; cell: grid step (mm).  Each
- * element spreads its cells over the threads. */
-int oracle_scatter_grid(const float* C, const float* D, const float* I, const float* P, int parts, double cell,
-                        const int* dets, int ndet, long long v0, long long nv, double* out, int nthreads)
+ * [v0, v0+nv), in double; parts: 1 crystal cells, 2 septal cells; cell: grid step (mm); S:
+ * optional hole shapes (NULL: circular holes).  Each element spreads its cells over the
+ * threads. */
+int oracle_scatter_grid(const float* C, const float* D, const float* I, const float* P, const float* S, int parts,
+                        double cell, const int* dets, int ndet, long long v0, long long nv, double* out, int nthreads)
 {
     ogeo g;
     if (parse(&g, C, D, I, P)) return -1;
+    g.S = S;
     if (!(cell > 0)) return -1;
     for (long long e = 0; e < (long long)ndet * nv; ++e)
         out[e] = grid_element(&g, parts, dets[e / nv], v0 + e % nv, cell, nthreads);
