@@ -161,5 +161,6 @@ def test_invalid_batches_raise(gpu):
     plan.run()
     with pytest.raises(sysmat.SysmatError):
         plan.set_tiles(0, 4, 4)
-    with pytest.raises(sysmat.SysmatError):
-        plan.run(mode=3)
+    for mode in (4, -1):                                                      # no such mode
+        with pytest.raises(sysmat.SysmatError):
+            plan.run(mode=mode)
