@@ -467,10 +467,19 @@ __device__ __forceinline__ void walk_round(const DevGeom& g, const WarpSmem& ws,
                                            float xD, float yD, float zD, float sa_a, float sa_b,
                                            float cosang, RayCyl& rc, Walk& s)
 {
+    // the next entry's layer and rectangle are loaded one iteration ahead (shared-memory
+    // latency off the dependency chain: 4-5 % on the reference mode, same results)
+    int m_next = nh > 0 ? ws.rl[0] : 0;
+    float4 r_next = nh > 0 ? ws.rr[0] : make_float4(0.f, 0.f, 0.f, 0.f);
     for (int j = 0; j < nh; ++j) {
-        const int m = ws.rl[j];
+        const int m = m_next;
+        const float4 R = r_next;
+        if (j + 1 < nh) {
+            m_next = ws.rl[j + 1];
+            r_next = ws.rr[j + 1];
+        }
         if (m != s.lay) close_layers(g, s, m, cosang);
-        if (!in_rect(ws.rr[j], sa_a, sa_b)) continue;
+        if (!in_rect(R, sa_a, sa_b)) continue;
         const float4 A = ws.ra[j];
         const float4 B = ws.rb[j];
         float tmp;
@@ -493,8 +502,11 @@ __device__ __forceinline__ void walk_round(const DevGeom& g, const WarpSmem& ws,
     }
     if (nr <= nh) return;
     if (s.lay < g.n_layers) close_layers(g, s, g.n_layers, cosang);
+    float4 c_next = ws.rr[nh];
     for (int j = nh; j < nr; ++j) {
-        if (!in_rect(ws.rr[j], sa_a, sa_b)) continue;
+        const float4 R = c_next;
+        if (j + 1 < nr) c_next = ws.rr[j + 1];
+        if (!in_rect(R, sa_a, sa_b)) continue;
         const float4 A = ws.ra[j];
         const float4 B = ws.rb[j];
         const float4 C = ws.rc[j];
