@@ -10,9 +10,15 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <algorithm>
 #include <mutex>
 #include <string>
+#include <thread>
 #include <vector>
+
+#include <fcntl.h>
+#include <sys/stat.h>
+#include <unistd.h>
 
 #include "../../include/sysmat.h"
 #include "geom.cuh"
@@ -617,6 +623,36 @@ struct DevBuf {
     }
 };
 
+// Pinned staging for the bitmap file reader: per reader thread two pieces, a stream and an
+// event per piece.  Made on the first file read of a device and kept (128 MB pinned), since
+// pinning that much memory costs more than reading a config-3 bitmap file.
+struct FileStaging {
+    static constexpr int kReaders = 4;
+    static constexpr size_t kPiece = 16u << 20;
+    unsigned char* piece[kReaders][2] = {};
+    cudaEvent_t done[kReaders][2] = {};
+    cudaStream_t stream[kReaders] = {};
+    bool ready = false;
+    int ensure()
+    {
+        if (ready) return SYSMAT_OK;
+        for (int t = 0; t < kReaders; ++t) {
+            if (!stream[t] && cudaStreamCreateWithFlags(&stream[t], cudaStreamNonBlocking) != cudaSuccess)
+                return SYSMAT_ERR_CUDA;
+            for (int b = 0; b < 2; ++b) {
+                if (!piece[t][b] && cudaHostAlloc((void**)&piece[t][b], kPiece, cudaHostAllocDefault) != cudaSuccess) {
+                    piece[t][b] = nullptr;
+                    return SYSMAT_ERR_NOMEM;
+                }
+                if (!done[t][b] && cudaEventCreateWithFlags(&done[t][b], cudaEventDisableTiming) != cudaSuccess)
+                    return SYSMAT_ERR_CUDA;
+            }
+        }
+        ready = true;
+        return SYSMAT_OK;
+    }
+};
+
 struct LegacySlot {
     std::mutex mu;
     uint64_t key = 0;
@@ -624,6 +660,7 @@ struct LegacySlot {
     float* d_out = nullptr;
     size_t out_cap = 0;
     DevBuf pe, bm_crystal, bm_collimator;
+    FileStaging staging;
 };
 
 LegacySlot& slot_for(int device)
@@ -717,25 +754,78 @@ int bitmap_to_file(const char* fname, const uint32_t* d_words, long long n)
 }
 
 // Read a bitmap file into device memory.  Like the reference (zero-initialised buffer and an
-// unchecked fread, scatter.cu:2156-2159), a short file leaves the remaining words zero.
-int bitmap_from_file(const char* fname, uint32_t* d_words, long long n)
+// unchecked fread, scatter.cu:2156-2159), a short file leaves the remaining words zero.  The
+// file (gigabytes for a large system) streams through a pipeline: reader threads, each with two
+// pinned staging pieces and its own stream, read interleaved pieces with pread and copy each
+// to the device while reading the next, so the read, the copy and the other readers overlap.
+int bitmap_from_file(const char* fname, uint32_t* d_words, long long n, int device, FileStaging& stg)
 {
     if (!fname) return SYSMAT_ERR_ARG;
-    FILE* f = std::fopen(fname, "rb");
-    if (!f) return SYSMAT_ERR_IO;
-    std::vector<uint32_t> h((size_t)n, 0u);
-    const size_t r = std::fread(h.data(), sizeof(uint32_t), (size_t)n, f);
-    std::fclose(f);
-    if (r != (size_t)n)
-        std::fprintf(stderr, "sysmat: %s holds %zu of %lld bitmap words; the rest read as 0\n", fname, r, n);
-    if (cudaMemcpy(d_words, h.data(), sizeof(uint32_t) * (size_t)n, cudaMemcpyHostToDevice) != cudaSuccess)
-        return SYSMAT_ERR_CUDA;
+    const int fd = ::open(fname, O_RDONLY);
+    if (fd < 0) return SYSMAT_ERR_IO;
+    struct stat st;
+    if (::fstat(fd, &st) != 0) {
+        ::close(fd);
+        return SYSMAT_ERR_IO;
+    }
+    const size_t want = sizeof(uint32_t) * (size_t)n;
+    const size_t have = (size_t)st.st_size < want ? (size_t)st.st_size / sizeof(uint32_t) * sizeof(uint32_t) : want;
+    int rc = stg.ensure();
+    if (!rc && have < want) {
+        std::fprintf(stderr, "sysmat: %s holds %zu of %lld bitmap words; the rest read as 0\n", fname,
+                     have / sizeof(uint32_t), n);
+        if (cudaMemset((unsigned char*)d_words + have, 0, want - have) != cudaSuccess) rc = SYSMAT_ERR_CUDA;
+    }
+    if (rc) {
+        ::close(fd);
+        return rc;
+    }
+    constexpr size_t kPiece = FileStaging::kPiece;
+    const size_t n_pieces = (have + kPiece - 1) / kPiece;
+    const int n_readers = (int)std::min<size_t>(n_pieces, FileStaging::kReaders);
+    int status[FileStaging::kReaders] = {};
+    auto reader = [&](int t) {
+        int r = cudaSetDevice(device) == cudaSuccess ? SYSMAT_OK : SYSMAT_ERR_CUDA;
+        int use = 0;
+        for (size_t k = (size_t)t; k < n_pieces && r == SYSMAT_OK; k += (size_t)n_readers, ++use) {
+            const int b = use & 1;
+            unsigned char* h = stg.piece[t][b];
+            const size_t off = k * kPiece, len = std::min(kPiece, have - off);
+            if (cudaEventSynchronize(stg.done[t][b]) != cudaSuccess) {   // the piece's last copy is done
+                r = SYSMAT_ERR_CUDA;
+                break;
+            }
+            size_t got = 0;
+            while (got < len) {
+                const ssize_t q = ::pread(fd, h + got, len - got, (off_t)(off + got));
+                if (q <= 0) break;
+                got += (size_t)q;
+            }
+            if (got != len) {
+                r = SYSMAT_ERR_IO;
+                break;
+            }
+            if (cudaMemcpyAsync((unsigned char*)d_words + off, h, len, cudaMemcpyHostToDevice, stg.stream[t]) != cudaSuccess ||
+                cudaEventRecord(stg.done[t][b], stg.stream[t]) != cudaSuccess)
+                r = SYSMAT_ERR_CUDA;
+        }
+        if (cudaStreamSynchronize(stg.stream[t]) != cudaSuccess && r == SYSMAT_OK) r = SYSMAT_ERR_CUDA;
+        status[t] = r;
+    };
+    std::vector<std::thread> pool;
+    for (int t = 1; t < n_readers; ++t) pool.emplace_back(reader, t);
+    if (n_readers > 0) reader(0);
+    for (auto& th : pool) th.join();
+    ::close(fd);
+    for (int t = 0; t < n_readers; ++t)
+        if (status[t]) return status[t];
     return SYSMAT_OK;
 }
 
 // Compute (flag set) or load a relationship bitmap for the reference-compatible scatter
 // programs (scatter.cu:2116-2167, :2246-2301).
-int legacy_bitmap(sysmat_ctx* ctx, bool crystal, bool compute, const char* fname, DevBuf& buf)
+int legacy_bitmap(sysmat_ctx* ctx, bool crystal, bool compute, const char* fname, DevBuf& buf,
+                  FileStaging& stg)
 {
     const long long n = crystal ? sysmat_bitmap_crystal_words(ctx) : sysmat_bitmap_collimator_words(ctx);
     if (n < 0) return (int)n;
@@ -747,7 +837,7 @@ int legacy_bitmap(sysmat_ctx* ctx, bool crystal, bool compute, const char* fname
         if (rc) return rc;
         return bitmap_to_file(fname, words, n);
     }
-    return bitmap_from_file(fname, words, n);
+    return bitmap_from_file(fname, words, n, ctx->device, stg);
 }
 
 int legacy_scatter(int cuda_id, float* pC, float* pD, float* pI, float* pP, float* pe,
@@ -768,14 +858,14 @@ int legacy_scatter(int cuda_id, float* pC, float* pD, float* pI, float* pP, floa
     const long long V = ctx->g.nvox;
     const size_t nel = (size_t)D * (size_t)V;
     if (parts & SYSMAT_SCATTER_CRYSTAL) {
-        rc = legacy_bitmap(ctx, true, comp_crystal, f_crystal, slot.bm_crystal);
+        rc = legacy_bitmap(ctx, true, comp_crystal, f_crystal, slot.bm_crystal, slot.staging);
         if (rc) return rc;
         rc = slot.pe.ensure(sizeof(float) * nel);
         if (rc) return rc;
         CUDA_TRY(cudaMemcpy(slot.pe.p, pe, sizeof(float) * nel, cudaMemcpyHostToDevice));
     }
     if (parts & SYSMAT_SCATTER_COLLIMATOR) {
-        rc = legacy_bitmap(ctx, false, comp_collimator, f_collimator, slot.bm_collimator);
+        rc = legacy_bitmap(ctx, false, comp_collimator, f_collimator, slot.bm_collimator, slot.staging);
         if (rc) return rc;
     }
     rc = legacy_out(slot, nel);

@@ -190,11 +190,6 @@ __global__ void bitmap_collimator_kernel(const float* __restrict__ det, const fl
 
 // ---- pair tables ----
 
-__device__ __forceinline__ bool test_bit(const uint32_t* bm, long long bit)
-{
-    return (__ldg(&bm[bit >> 5]) >> (bit & 31)) & 1u;
-}
-
 // Scatter point of scatterer s: crystal centre (y + FOV) or hole centre
 // ((y1 + y2) / 2 + FOV), scatter.cu:1221-1223, :1707-1709.
 __device__ __forceinline__ void scatter_point(const DevGeom& g, int s, float& xs, float& ys, float& zs)
@@ -226,14 +221,7 @@ __device__ void for_each_attenuator(const DevGeom& g, const uint32_t* bm_cry, co
         base = ((long long)(s - n) * n + d) * n;
     }
     const uint32_t* bm = s < n ? bm_cry : bm_col;
-    const float4 hr = (NATIVE && s >= n) ? __ldg(&g.hole.raw[s - n]) : make_float4(0.f, 0.f, 0.f, 0.f);
-    for (int a = 0; a < n; ++a) {
-        if (a == d || (s < n && a == s)) continue;
-        if (NATIVE && s >= n) {
-            if (!collimator_related(g.raw_det, hr, d, a)) continue;
-        } else if (!test_bit(bm, base + a)) {
-            continue;
-        }
+    auto visit = [&](int a) {
         const float4 pa = __ldg(&g.cry.pos[a]);
         const float4 sa = __ldg(&g.cry.size[a]);
         const float4 ta = __ldg(&g.cry.trig[a]);
@@ -243,6 +231,27 @@ __device__ void for_each_attenuator(const DevGeom& g, const uint32_t* bm_cry, co
         const float len = box_chord(xa, ya, za, xb, yb, zb, -0.5f * sa.x, -0.5f * sa.y, -0.5f * sa.z,
                                     0.5f * sa.x, 0.5f * sa.y, 0.5f * sa.z);
         if (len != 0.0f) f(a, len);
+    };
+    if (NATIVE && s >= n) {
+        const float4 hr = __ldg(&g.hole.raw[s - n]);
+        for (int a = 0; a < n; ++a)
+            if (a != d && collimator_related(g.raw_det, hr, d, a)) visit(a);
+        return;
+    }
+    // The pair's n bits start at bit `base`: visit the set ones word by word, lowest first
+    // (ascending a), so a sparse row costs one load per 32 crystals.
+    const long long end = base + n;
+    for (long long w = base >> 5; w < (end + 31) >> 5; ++w) {
+        const long long b0 = w << 5;
+        uint32_t word = __ldg(&bm[w]);
+        if (b0 < base) word &= ~0u << (int)(base - b0);
+        if (b0 + 32 > end) word &= (1u << (int)(end - b0)) - 1u;
+        while (word) {
+            const int a = (int)(b0 + (__ffs(word) - 1) - base);
+            word &= word - 1u;
+            if (a == d || (s < n && a == s)) continue;
+            visit(a);
+        }
     }
 }
 

@@ -164,6 +164,43 @@ def test_legacy_scatter_programs_and_bitmap_files(gpu):
         assert ei.value.code == -4                        # SYSMAT_ERR_IO, not exit(0)
 
 
+def test_legacy_scatter_reads_large_and_short_bitmap_files(gpu):
+    """The file reader streams a bitmap through several reader threads and pinned pieces; a
+    file of 200 MB of bitmaps must reproduce the computing call bit for bit, and a short file
+    (cut inside a word) reads its missing words as 0, as the reference's zero-filled buffer
+    does (scatter.cu:2156-2159)."""
+    torch = gpu
+    geo, z = golden("config3_z8")
+    ctx = sysmat.Context(geo)
+    pe_t = _pe(torch, ctx, geo)
+    pe = pe_t.cpu().numpy().reshape(-1)
+    n = geo.n_det * geo.n_vox
+    with tempfile.TemporaryDirectory() as tmp:
+        fc, fh = os.path.join(tmp, "GeoCrystal"), os.path.join(tmp, "GeoCollimator")
+        dst = np.zeros(n, np.float32)
+        sysmat.scatter(geo.collimator, geo.detector, geo.image, geo.physics, pe, fc, fh, dst)
+        for f, key in ((fc, "crystal"), (fh, "collimator")):
+            assert hashlib.sha256(np.fromfile(f, np.uint8).tobytes()).digest() == bytes(z[f"bitmap_{key}_sha256"])
+        phys = geo.physics.copy()
+        phys[8] = phys[9] = 0
+        dst2 = np.zeros(n, np.float32)
+        sysmat.scatter(geo.collimator, geo.detector, geo.image, phys, pe, fc, fh, dst2)
+        assert np.array_equal(dst, dst2)
+        words = np.fromfile(fh, np.uint32)
+        keep = int(words.size * 0.6)
+        with open(fh, "r+b") as f:
+            f.truncate(4 * keep + 3)                      # a partial last word reads as 0 too
+        short = np.zeros(n, np.float32)
+        sysmat.scatter(geo.collimator, geo.detector, geo.image, phys, pe, fc, fh, short)
+    cut = words.copy()
+    cut[keep:] = 0
+    ctx.scatter_prepare(ctx.bitmap_crystal(), torch.from_numpy(cut.view(np.int32)).cuda())
+    exp = torch.empty((geo.n_det, geo.n_vox), dtype=torch.float32, device="cuda")
+    ctx.scatter(exp, pe_t, rotation=float(geo.image[20]))
+    assert np.array_equal(short, exp.cpu().numpy().reshape(-1))
+    assert not np.array_equal(short, dst)
+
+
 def test_scatter_argument_errors(gpu):
     geo, z = golden("mini0")
     ctx = sysmat.Context(geo)
