@@ -23,6 +23,7 @@
 //  * one thread per matrix element (d, v); a block shares d, so pair records are staged in
 //    shared memory and attenuator lists are broadcast loads; each element sums its items in
 //    FP64 (the reference adds float items with atomicAdd in an unspecified order).
+#include <algorithm>
 #include <cmath>
 
 #include <cub/cub.cuh>
@@ -205,53 +206,103 @@ __device__ __forceinline__ void scatter_point(const DevGeom& g, int s, float& xs
     }
 }
 
-// Visit the attenuators of pair (s, d) with non-zero chords, in ascending crystal order.
-// NATIVE: hole scatterers s >= D are holes of any layer, their attenuators given by the
-// relationship predicate evaluated here instead of the layer-0 bitmap.
-template <bool NATIVE, typename F>
-__device__ void for_each_attenuator(const DevGeom& g, const uint32_t* bm_cry, const uint32_t* bm_col,
-                                    int s, int d, float xs, float ys, float zs, const DetPoint& q, F&& f)
+// Pair-table kernels: one warp per (detector d, scatterer s) pair.  The pair's candidate
+// attenuators (its bitmap row, or the relationship predicate) are compacted into a per-warp
+// list in ascending crystal order, then the lanes take 32 list entries at a time, so every
+// lane evaluates a chord instead of waiting on the lane with the most set bits.
+constexpr int kPairWarps = 8;          // warps per block
+constexpr int kPairSpan = 1024;        // candidates compacted per pass (32 per lane)
+
+// Bit start of the n-bit row of pair (s, d): crystal pairs in the upper triangle (i < j),
+// hole pairs by (hole, detector).
+__device__ __forceinline__ long long pair_row_bit(int n, int s, int d)
 {
-    const int n = g.n_det;
-    long long base;
     if (s < n) {
         const long long i = s < d ? s : d, j = s < d ? d : s;
-        base = (i * n - (i * (i + 1)) / 2 + j) * n;
-    } else {
-        base = ((long long)(s - n) * n + d) * n;
+        return (i * n - (i * (i + 1)) / 2 + j) * n;
     }
-    const uint32_t* bm = s < n ? bm_cry : bm_col;
-    auto visit = [&](int a) {
-        const float4 pa = __ldg(&g.cry.pos[a]);
-        const float4 sa = __ldg(&g.cry.size[a]);
-        const float4 ta = __ldg(&g.cry.trig[a]);
-        float xa, ya, za, xb, yb, zb;                            // :1377-1394
-        to_crystal_frame(pa.x, pa.y, pa.z, ta.z, ta.w, xs, ys, zs, xa, ya, za);
-        to_crystal_frame(pa.x, pa.y, pa.z, ta.z, ta.w, q.xD, q.yD, q.zD, xb, yb, zb);
-        const float len = box_chord(xa, ya, za, xb, yb, zb, -0.5f * sa.x, -0.5f * sa.y, -0.5f * sa.z,
-                                    0.5f * sa.x, 0.5f * sa.y, 0.5f * sa.z);
-        if (len != 0.0f) f(a, len);
-    };
+    return ((long long)(s - n) * n + d) * n;
+}
+
+// Candidates a0 .. a0+31 of pair (s, d) as a bit mask (bit k: crystal a0 + k), without
+// crystal d and scatter crystal s.  NATIVE hole scatterers evaluate the predicate instead of
+// reading a bitmap.
+template <bool NATIVE>
+__device__ __forceinline__ uint32_t candidate_mask(const DevGeom& g, const uint32_t* bm, long long base,
+                                                   float4 hr, int s, int d, int a0)
+{
+    const int n = g.n_det;
+    if (a0 >= n) return 0u;
+    const int span = n - a0 < 32 ? n - a0 : 32;
+    uint32_t m = 0u;
     if (NATIVE && s >= n) {
-        const float4 hr = __ldg(&g.hole.raw[s - n]);
-        for (int a = 0; a < n; ++a)
-            if (a != d && collimator_related(g.raw_det, hr, d, a)) visit(a);
-        return;
+        for (int k = 0; k < span; ++k)
+            if (collimator_related(g.raw_det, hr, d, a0 + k)) m |= 1u << k;
+    } else {
+        const long long b = base + a0, w = b >> 5;
+        const int sh = (int)(b & 31);
+        const uint32_t lo = __ldg(&bm[w]);
+        // the next word only when the row continues into it
+        const uint32_t hi = (sh != 0 && w + 1 <= ((base + n - 1) >> 5)) ? __ldg(&bm[w + 1]) : 0u;
+        m = __funnelshift_r(lo, hi, sh);
+        if (span < 32) m &= (1u << span) - 1u;
     }
-    // The pair's n bits start at bit `base`: visit the set ones word by word, lowest first
-    // (ascending a), so a sparse row costs one load per 32 crystals.
-    const long long end = base + n;
-    for (long long w = base >> 5; w < (end + 31) >> 5; ++w) {
-        const long long b0 = w << 5;
-        uint32_t word = __ldg(&bm[w]);
-        if (b0 < base) word &= ~0u << (int)(base - b0);
-        if (b0 + 32 > end) word &= (1u << (int)(end - b0)) - 1u;
-        while (word) {
-            const int a = (int)(b0 + (__ffs(word) - 1) - base);
-            word &= word - 1u;
-            if (a == d || (s < n && a == s)) continue;
-            visit(a);
+    if (d >= a0 && d - a0 < 32) m &= ~(1u << (d - a0));
+    if (s < n && s >= a0 && s - a0 < 32) m &= ~(1u << (s - a0));
+    return m;
+}
+
+// Chord of the scatter point -> detector point segment inside attenuating crystal a
+// (scatter.cu:1377-1394).
+__device__ __forceinline__ float attenuator_chord(const DevGeom& g, int a, float xs, float ys, float zs,
+                                                  const DetPoint& q)
+{
+    const float4 pa = __ldg(&g.cry.pos[a]);
+    const float4 sa = __ldg(&g.cry.size[a]);
+    const float4 ta = __ldg(&g.cry.trig[a]);
+    float xa, ya, za, xb, yb, zb;
+    to_crystal_frame(pa.x, pa.y, pa.z, ta.z, ta.w, xs, ys, zs, xa, ya, za);
+    to_crystal_frame(pa.x, pa.y, pa.z, ta.z, ta.w, q.xD, q.yD, q.zD, xb, yb, zb);
+    return box_chord(xa, ya, za, xb, yb, zb, -0.5f * sa.x, -0.5f * sa.y, -0.5f * sa.z, 0.5f * sa.x,
+                     0.5f * sa.y, 0.5f * sa.z);
+}
+
+// Warp-collective walk over the attenuators of pair (s, d) in ascending crystal order: f(a,
+// len, ok) is called by every lane for each group of 32 candidates (ok false on lanes past
+// the group's end).  list: the warp's kPairSpan-entry shared buffer.
+template <bool NATIVE, typename F>
+__device__ __forceinline__ void warp_attenuators(const DevGeom& g, const uint32_t* bm_cry, const uint32_t* bm_col,
+                                                 int s, int d, float xs, float ys, float zs, const DetPoint& q,
+                                                 int lane, int* list, F&& f)
+{
+    const int n = g.n_det;
+    const long long base = (NATIVE && s >= n) ? 0 : pair_row_bit(n, s, d);
+    const uint32_t* bm = s < n ? bm_cry : bm_col;
+    const float4 hr = (NATIVE && s >= n) ? __ldg(&g.hole.raw[s - n]) : make_float4(0.f, 0.f, 0.f, 0.f);
+    for (int c0 = 0; c0 < n; c0 += kPairSpan) {
+        const int a0 = c0 + 32 * lane;
+        uint32_t m = candidate_mask<NATIVE>(g, bm, base, hr, s, d, a0);
+        const int cnt = __popc(m);
+        int incl = cnt;
+#pragma unroll
+        for (int off = 1; off < 32; off <<= 1) {
+            const int v = __shfl_up_sync(0xffffffffu, incl, off);
+            if (lane >= off) incl += v;
         }
+        const int total = __shfl_sync(0xffffffffu, incl, 31);
+        int pos = incl - cnt;
+        while (m) {
+            list[pos++] = a0 + __ffs(m) - 1;
+            m &= m - 1u;
+        }
+        __syncwarp();
+        for (int b = 0; b < total; b += 32) {
+            const bool ok = b + lane < total;
+            const int a = ok ? list[b + lane] : 0;
+            const float len = ok ? attenuator_chord(g, a, xs, ys, zs, q) : 0.0f;
+            f(a, len, ok);
+        }
+        __syncwarp();
     }
 }
 
@@ -323,73 +374,96 @@ __device__ void tungsten_path(const DevGeom& g, int h, float sx, float sy, float
 }
 
 template <bool NATIVE>
-__global__ void pair_count_kernel(DevGeom g, int parts, const uint32_t* bm_cry, const uint32_t* bm_col,
-                                  long long* counts)
+__global__ void __launch_bounds__(32 * kPairWarps) pair_count_kernel(DevGeom g, int parts, const uint32_t* bm_cry,
+                                                                     const uint32_t* bm_col, long long* counts)
 {
+    __shared__ int list[kPairWarps][kPairSpan];
     const int ns = g.n_det + (NATIVE ? g.n_holes : g.n_holes0);
-    const long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (p >= (long long)g.n_det * ns) return;
-    const int d = (int)(p / ns), s = (int)(p - (long long)d * ns);
-    int c = 0;
-    if (pair_enabled(g, parts, s, d)) {
-        float xs, ys, zs;
-        scatter_point(g, s, xs, ys, zs);
-        const DetPoint q = det_point(__ldg(&g.cry.pos[d]), __ldg(&g.cry.size[d]), __ldg(&g.cry.trig[d]));
-        for_each_attenuator<NATIVE>(g, bm_cry, bm_col, s, d, xs, ys, zs, q, [&](int, float) { ++c; });
+    const long long np = (long long)g.n_det * ns;
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    for (long long p = (long long)blockIdx.x * kPairWarps + wid; p < np; p += (long long)gridDim.x * kPairWarps) {
+        const int d = (int)(p / ns), s = (int)(p - (long long)d * ns);
+        int c = 0;
+        if (pair_enabled(g, parts, s, d)) {
+            float xs, ys, zs;
+            scatter_point(g, s, xs, ys, zs);
+            const DetPoint q = det_point(__ldg(&g.cry.pos[d]), __ldg(&g.cry.size[d]), __ldg(&g.cry.trig[d]));
+            warp_attenuators<NATIVE>(g, bm_cry, bm_col, s, d, xs, ys, zs, q, lane, list[wid],
+                                     [&](int, float len, bool ok) {
+                                         c += __popc(__ballot_sync(0xffffffffu, ok && len != 0.0f));
+                                     });
+        }
+        if (lane == 0) counts[p] = c;
     }
-    counts[p] = c;
 }
 
 template <bool NATIVE>
-__global__ void pair_fill_kernel(DevGeom g, int parts, const uint32_t* bm_cry, const uint32_t* bm_col,
-                                 const long long* offsets, PairRec* pairs, PairNative* nat, AttEntry* att)
+__global__ void __launch_bounds__(32 * kPairWarps) pair_fill_kernel(DevGeom g, int parts, const uint32_t* bm_cry,
+                                                                    const uint32_t* bm_col, const long long* offsets,
+                                                                    PairRec* pairs, AttEntry* att)
 {
+    __shared__ int list[kPairWarps][kPairSpan];
     const int ns = g.n_det + (NATIVE ? g.n_holes : g.n_holes0);
+    const long long np = (long long)g.n_det * ns;
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    for (long long p = (long long)blockIdx.x * kPairWarps + wid; p < np; p += (long long)gridDim.x * kPairWarps) {
+        const int d = (int)(p / ns), s = (int)(p - (long long)d * ns);
+        PairRec r{};
+        r.valid = pair_enabled(g, parts, s, d);
+        if (r.valid) {
+            float xs, ys, zs;
+            scatter_point(g, s, xs, ys, zs);
+            const float4 P = __ldg(&g.cry.pos[d]), S = __ldg(&g.cry.size[d]), T = __ldg(&g.cry.trig[d]);
+            const DetPoint q = det_point(P, S, T);
+            to_crystal_frame(P.x, P.y, P.z, T.z, T.w, xs, ys, zs, r.xss, r.yss, r.zss);   // :1290-1292
+            r.lsd = dist3(xs, ys, zs, q.xD, q.yD, q.zD);                                   // :1275
+            // absorption chord along the extended scatter->detector ray (:1420-1424)
+            const float ux1 = ((float)0 / (float)1 - 0.5f) * S.x, ux2 = (((float)0 + 1.0f) / (float)1 - 0.5f) * S.x;
+            const float uy1 = ((float)0 / (float)1 - 0.5f) * S.y, uy2 = (((float)0 + 1.0f) / (float)1 - 0.5f) * S.y;
+            const float uz1 = ((float)0 / (float)1 - 0.5f) * S.z, uz2 = (((float)0 + 1.0f) / (float)1 - 0.5f) * S.z;
+            const float xt = q.xDs + 1000.0f * (q.xDs - r.xss) / r.lsd;
+            const float yt = q.yDs + 1000.0f * (q.yDs - r.yss) / r.lsd;
+            const float zt = q.zDs + 1000.0f * (q.zDs - r.zss) / r.lsd;
+            r.labs = box_chord(r.xss, r.yss, r.zss, xt, yt, zt, ux1, uy1, uz1, ux2, uy2, uz2);
+            // row-relative start: a row holds at most ns * D entries, which fits an int
+            r.att_begin = (int)(offsets[p] - offsets[(long long)d * ns]);
+            AttEntry* dst = att + offsets[p];
+            int k = 0;
+            warp_attenuators<NATIVE>(g, bm_cry, bm_col, s, d, xs, ys, zs, q, lane, list[wid],
+                                     [&](int a, float len, bool ok) {
+                                         const bool nz = ok && len != 0.0f;
+                                         const unsigned m = __ballot_sync(0xffffffffu, nz);
+                                         if (nz) {
+                                             const float4 mu = __ldg(&g.cry.mu[a]);
+                                             dst[k + __popc(m & ((1u << lane) - 1u))] = AttEntry{len, mu.y, mu.z};
+                                         }
+                                         k += __popc(m);
+                                     });
+            r.att_count = k;
+        }
+        if (lane == 0) pairs[p] = r;
+    }
+}
+
+// Native model: the tungsten terms of each pair, one thread per pair.
+__global__ void pair_native_kernel(DevGeom g, int parts, PairNative* nat)
+{
+    const int ns = g.n_det + g.n_holes;
     const long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (p >= (long long)g.n_det * ns) return;
     const int d = (int)(p / ns), s = (int)(p - (long long)d * ns);
-    PairRec r{};
-    r.valid = pair_enabled(g, parts, s, d);
-    if (r.valid) {
+    PairNative n{};
+    if (s >= g.n_det && pair_enabled(g, parts, s, d)) {
         float xs, ys, zs;
         scatter_point(g, s, xs, ys, zs);
-        const float4 P = __ldg(&g.cry.pos[d]), S = __ldg(&g.cry.size[d]), T = __ldg(&g.cry.trig[d]);
-        const DetPoint q = det_point(P, S, T);
-        to_crystal_frame(P.x, P.y, P.z, T.z, T.w, xs, ys, zs, r.xss, r.yss, r.zss);   // :1290-1292
-        r.lsd = dist3(xs, ys, zs, q.xD, q.yD, q.zD);                                   // :1275
-        // absorption chord along the extended scatter->detector ray (:1420-1424)
-        const float ux1 = ((float)0 / (float)1 - 0.5f) * S.x, ux2 = (((float)0 + 1.0f) / (float)1 - 0.5f) * S.x;
-        const float uy1 = ((float)0 / (float)1 - 0.5f) * S.y, uy2 = (((float)0 + 1.0f) / (float)1 - 0.5f) * S.y;
-        const float uz1 = ((float)0 / (float)1 - 0.5f) * S.z, uz2 = (((float)0 + 1.0f) / (float)1 - 0.5f) * S.z;
-        const float xt = q.xDs + 1000.0f * (q.xDs - r.xss) / r.lsd;
-        const float yt = q.yDs + 1000.0f * (q.yDs - r.yss) / r.lsd;
-        const float zt = q.zDs + 1000.0f * (q.zDs - r.zss) / r.lsd;
-        r.labs = box_chord(r.xss, r.yss, r.zss, xt, yt, zt, ux1, uy1, uz1, ux2, uy2, uz2);
-        // row-relative start: a row holds at most ns * D entries, which fits an int
-        r.att_begin = (int)(offsets[p] - offsets[(long long)d * ns]);
-        AttEntry* dst = att + offsets[p];
-        int k = 0;
-        for_each_attenuator<NATIVE>(g, bm_cry, bm_col, s, d, xs, ys, zs, q, [&](int a, float len) {
-            const float4 mu = __ldg(&g.cry.mu[a]);
-            dst[k] = AttEntry{len, mu.y, mu.z};
-            ++k;
-        });
-        r.att_count = k;
-        if (NATIVE && s >= g.n_det) {
-            const int h = s - g.n_det;
-            PairNative n{};
-            tungsten_path(g, h, xs, ys, zs, q.xD, q.yD, q.zD, n.w_pe, n.w_c);
-            const LayerInfo& Ly = g.layer[hole_layer(g, h)];
-            n.mu_tot_h = Ly.mu_total;
-            n.mu_c_h = Ly.mu_c;
-            nat[p] = n;
-        } else if (NATIVE) {
-            nat[p] = PairNative{};
-        }
-    } else if (NATIVE) {
-        nat[p] = PairNative{};
+        const DetPoint q = det_point(__ldg(&g.cry.pos[d]), __ldg(&g.cry.size[d]), __ldg(&g.cry.trig[d]));
+        const int h = s - g.n_det;
+        tungsten_path(g, h, xs, ys, zs, q.xD, q.yD, q.zD, n.w_pe, n.w_c);
+        const LayerInfo& Ly = g.layer[hole_layer(g, h)];
+        n.mu_tot_h = Ly.mu_total;
+        n.mu_c_h = Ly.mu_c;
     }
-    pairs[p] = r;
+    nat[p] = n;
 }
 
 // ---- scatter items ----
@@ -688,7 +762,8 @@ static int build_pairs(const DevGeom& g, int parts, const uint32_t* bm_cry, cons
     long long* counts = (long long*)(base + off_counts);
     long long* offsets = (long long*)(base + off_offsets);
     const unsigned blocks = (unsigned)((np + 255) / 256);
-    pair_count_kernel<NATIVE><<<blocks, 256, 0, s>>>(g, parts, bm_cry, bm_col, counts);
+    const unsigned warp_blocks = (unsigned)std::min<long long>((np + kPairWarps - 1) / kPairWarps, 148LL * 64);
+    pair_count_kernel<NATIVE><<<warp_blocks, 32 * kPairWarps, 0, s>>>(g, parts, bm_cry, bm_col, counts);
     if (cudaMemsetAsync(counts + np, 0, sizeof(long long), s) != cudaSuccess) return -1;
     cub::DeviceScan::ExclusiveSum(base + off_temp, temp_bytes, counts, offsets, np + 1, s);
     long long total = 0;
@@ -704,7 +779,7 @@ static int build_pairs(const DevGeom& g, int parts, const uint32_t* bm_cry, cons
         base = (char*)scratch.base;
         counts = (long long*)(base + off_counts);
         offsets = (long long*)(base + off_offsets);
-        pair_count_kernel<NATIVE><<<blocks, 256, 0, s>>>(g, parts, bm_cry, bm_col, counts);
+        pair_count_kernel<NATIVE><<<warp_blocks, 32 * kPairWarps, 0, s>>>(g, parts, bm_cry, bm_col, counts);
         if (cudaMemsetAsync(counts + np, 0, sizeof(long long), s) != cudaSuccess) return -1;
         cub::DeviceScan::ExclusiveSum(base + off_temp, temp_bytes, counts, offsets, np + 1, s);
     }
@@ -713,7 +788,8 @@ static int build_pairs(const DevGeom& g, int parts, const uint32_t* bm_cry, cons
     if (native) *native = nat;
     *att = (AttEntry*)(base + fixed);
     *att_offsets = offsets;
-    pair_fill_kernel<NATIVE><<<blocks, 256, 0, s>>>(g, parts, bm_cry, bm_col, offsets, *pairs, nat, *att);
+    pair_fill_kernel<NATIVE><<<warp_blocks, 32 * kPairWarps, 0, s>>>(g, parts, bm_cry, bm_col, offsets, *pairs, *att);
+    if (NATIVE) pair_native_kernel<<<blocks, 256, 0, s>>>(g, parts, nat);
     return cudaGetLastError() == cudaSuccess ? 0 : -1;
 }
 
