@@ -85,7 +85,7 @@ __device__ __forceinline__ void kn_tab_eval(const double* __restrict__ tab, doub
                                             double& F, double& Fp)
 {
     const double hc = 3.14159265358979323846 / kKnTable;
-    double x = th / hc;
+    double x = th * (kKnTable / 3.14159265358979323846);   // cell coordinate (no double division)
     int i = (int)x;
     i = i < 0 ? 0 : (i > kKnTable - 1 ? kKnTable - 1 : i);
     const double t = x - (double)i;
