@@ -545,7 +545,7 @@ __device__ float scatter_item(const ElemConst& e, const PairRec& pr, const PairN
     const float mpe_s = e.mu_pe * e0 * e0 * e0 / es / es / es;              // :1411-1417
     const float mc_s = e.mu_c * e0 / es;
     const float mt_s = mpe_s + mc_s;
-    const double c = (double)(w_s * phi / 2.0f) / 3.14159265358979323846 * (double)ratio *
+    const double c = (double)(w_s * phi / 2.0f) * (1.0 / 3.14159265358979323846) * (double)ratio *
                      (double)pwin * (double)expf(-a_sum) *
                      (double)(1.0f - expf(-pr.labs * mt_s)) * (double)mpe_s / (double)mt_s;
     return (float)c;
@@ -619,9 +619,10 @@ __device__ __forceinline__ void scatter_rows(const DevGeom& g, const ScatterPhys
                 float sa;
                 if (L.hole_model != 1) {                                  // :1711-1715
                     const float vr = 0.1f;
-                    sa = (float)(((double)(vr * vr) * 3.14159265358979323846 + (double)((hr.z - hr.y) * vr)) /
-                                 (4.0f * 3.14159265358979323846 * (double)lih * (double)lih) *
-                                 (double)fabsf(ys - e.yI) / (double)lih);
+                    // (pi vr^2 + h vr) / (4 pi lih^2) * |dy| / lih, with one double reciprocal
+                    const double rl = 1.0 / (double)lih;
+                    sa = (float)(((double)(vr * vr) * 3.14159265358979323846 + (double)((hr.z - hr.y) * vr)) *
+                                 (1.0 / (4.0 * 3.14159265358979323846)) * rl * rl * (double)fabsf(ys - e.yI) * rl);
                 } else {                                                  // ScatterGen_Collimator :1212-1215
                     const float vr = 0.2f;
                     sa = (vr * vr + (hr.z - hr.y) * vr) / (4.0f * lih * lih);
