@@ -763,6 +763,7 @@ static int build_pairs(const DevGeom& g, int parts, const uint32_t* bm_cry, cons
     long long* counts = (long long*)(base + off_counts);
     long long* offsets = (long long*)(base + off_offsets);
     const unsigned blocks = (unsigned)((np + 255) / 256);
+    // one warp per pair, grid-stride beyond 148 x 64 blocks (64 per SM of a B200)
     const unsigned warp_blocks = (unsigned)std::min<long long>((np + kPairWarps - 1) / kPairWarps, 148LL * 64);
     pair_count_kernel<NATIVE><<<warp_blocks, 32 * kPairWarps, 0, s>>>(g, parts, bm_cry, bm_col, counts);
     if (cudaMemsetAsync(counts + np, 0, sizeof(long long), s) != cudaSuccess) return -1;

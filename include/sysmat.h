@@ -81,8 +81,12 @@ SYSMAT_API int PESysMatGen(float* parameter_Collimator, float* parameter_Detecto
 /* Replaces scatter of the combined program (ScatterGen_RayTracing_CircularHole/scatter.h:4-5,
  * scatter.cu:2013).  PE_SysMat: the D*V photoelectric matrix read from offset 0.  The
  * bitmaps are computed and written to the named files when parameter_Physics[8] / [9]
- * equal 1, else read from them (scatter.cu:2116-2164, :2246-2296).  Writes D*V floats =
- * collimator scatter + crystal scatter.  Returns V or a SYSMAT_ERR_* code. */
+ * equal 1, else read from them (scatter.cu:2116-2164, :2246-2296).  A file shorter than
+ * its bitmap reads its missing words as 0, with a warning on stderr, as the reference's
+ * zero-filled buffer does.  Files are read by up to 12 threads through pinned staging
+ * memory (32 MB per thread), allocated on the first read on a device and kept for the
+ * process.  Writes D*V floats = collimator scatter + crystal scatter.  Returns V or a
+ * SYSMAT_ERR_* code. */
 SYSMAT_API int scatter(float* parameter_Collimator, float* parameter_Detector, float* parameter_Image,
             float* parameter_Physics, float* PE_SysMat, const char* FnameGeoCrystal,
             const char* FnameGeoCollimator, float* dst, int cuda_id);
